@@ -1,0 +1,228 @@
+/*
+ * polfed_b200.h -- C ABI of the B200 (sm_100a) POLFED filter-and-Lanczos library.
+ *
+ * Every entry point returns an int status (PF_OK == 0).  On failure
+ * pf_last_error() returns a thread-local message.  No C++ exception and no
+ * torch type crosses this boundary; arrays are plain pointers plus sizes.
+ * A handle owns one CUDA stream plus workspaces; handles are independent and
+ * may be used from different host threads, but one handle is not re-entrant.
+ *
+ * Matrix-shaped arguments are column-major with a leading dimension, like a
+ * Julia CuArray / Array.  "device" pointers are CUDA global memory on the
+ * handle's device; "host" pointers are ordinary (pageable or pinned) memory.
+ *
+ * Reference interfaces replaced (Polfed.jl, file:line within that project):
+ *   operators          Models/SpinHalfChains.jl:74-99 (xxz_hamiltonian),
+ *                      :189-220 (j1j2_hamiltonian), :267-315 (matrix elements);
+ *                      QSun/QuantumSun.jl:1-102 (qsun_hamiltonian, S = 1/2)
+ *   pf_apply           MappingConfig.f!_rescaled, Polfed/Plan/Plan.jl:173-177
+ *                      and the plain operator f!, PolfedCore.jl:172
+ *   pf_clenshaw_*      MappingConfig.clenshaw_recurrence / clenshaw_finalsum,
+ *                      Polfed/Structs/MappingConfig.jl:35-45; the CUDA.jl
+ *                      kernels of Optimization/gpu/vector_dispatch.jl:113-139
+ *   pf_filter          the whole Clenshaw loop, Clenshaw/Algorithm/ClenshawAlgorithm.jl:12-29
+ *   pf_kpm_moments     dos_moments, DensetiesOfStates/Moments.jl:42-140
+ *   pf_solve           polfed(f!, x0, howmany, target; ...), Polfed/PolfedCore.jl:194-263
+ *   pf_lanczos_extrema lanczos_extrema, Lanczos/Lanczos.jl:183-212
+ */
+#ifndef POLFED_B200_H
+#define POLFED_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF_ABI_VERSION 1
+
+/* status codes */
+#define PF_OK              0
+#define PF_ERR_INVALID     1  /* bad argument (ArgumentError / DimensionMismatch) */
+#define PF_ERR_CUDA        2  /* CUDA runtime / cuBLAS / cuSOLVER failure */
+#define PF_ERR_NOMEM       3  /* device allocation failed */
+#define PF_ERR_NUMERIC     4  /* non-finite values, failed bisection bracket, ... */
+#define PF_ERR_UNSUPPORTED 5
+
+/* element types */
+#define PF_F64 0
+#define PF_F32 1
+
+/* memory spaces */
+#define PF_MEM_HOST   0
+#define PF_MEM_DEVICE 1
+
+/* target kinds (Polfed/Structs/TargetSpec.jl:26-58) */
+#define PF_TARGET_MAXDOS     0  /* :maxdos */
+#define PF_TARGET_MIDDLE     1  /* :middle */
+#define PF_TARGET_OFFSET     2  /* (:offset, eta) */
+#define PF_TARGET_UNRESCALED 3  /* (:unrescaled, E) or a plain number */
+#define PF_TARGET_RESCALED   4  /* (:rescaled, eps) */
+
+/* eigenvalue selection (Lanczos/Convergence/EigSorter.jl) */
+#define PF_WHICH_SR 0
+#define PF_WHICH_LR 1
+
+/* DoS damping kernels (DensetiesOfStates/Kernels.jl:33-72) */
+#define PF_KERNEL_JACKSON    0
+#define PF_KERNEL_LORENTZ    1
+#define PF_KERNEL_FEJER      2
+#define PF_KERNEL_LANCZOS    3
+#define PF_KERNEL_WANGZUNGER 4
+#define PF_KERNEL_DIRICHLET  5
+
+/* KPM probe vectors */
+#define PF_PROBE_GAUSSIAN   0  /* randn, normalised per column (Moments.jl:101-102) */
+#define PF_PROBE_RADEMACHER 1  /* +-1/sqrt(D) */
+
+/* solve precision */
+#define PF_PREC_FP64  0  /* FP64 throughout (the reference's arithmetic) */
+#define PF_PREC_MIXED 1  /* FP32 filter and KPM; FP64 Ritz, residual, refinement */
+
+typedef struct pf_handle pf_handle;
+typedef struct pf_op pf_op;
+
+/* ------------------------------------------------------------ library */
+int         pf_abi_version(void);
+const char *pf_last_error(void);
+
+int pf_handle_create(int device, pf_handle **out);
+int pf_handle_destroy(pf_handle *h);
+/* The handle's cudaStream_t, for callers that order their own work with it. */
+int pf_handle_stream(pf_handle *h, void **stream);
+int pf_handle_synchronize(pf_handle *h);
+
+/* ---------------------------------------------------------- operators */
+/* Spin-1/2 chain  H = sum_b J_b (S+_i S-_j + h.c.)/2 + J_b Delta_b Sz_i Sz_j
+ *                   + sum_i h_i Sz_i
+ * on the sector of states with Lup up spins (Lup < 0: the full 2^L space).
+ * bonds holds 2*nbonds 0-based sites (i0, j0, i1, j1, ...), as returned by
+ * _chain_bonds with 1 subtracted.  Host arrays are copied.  L <= 32, nbonds <= 64.
+ * Replaces SpinHalfChains.jl:267-315 (_spin_half_hamiltonian). */
+int pf_op_spin_chain_create(pf_handle *h, int L, int Lup, int nbonds, const int32_t *bonds,
+                            const double *J, const double *Delta, const double *fields,
+                            pf_op **out);
+/* Quantum Sun (S = 1/2, full space of L_loc + L_grain spins), QuantumSun.jl:1-102:
+ * coup[j] = g0-free couplings alpha^{u_j}, nbr[j] in [0, L_grain), fields[j] = h_j,
+ * grain = the dg x dg grain block (row-major, dg = 2^L_grain <= 16), already
+ * scaled by gamma / sqrt(dg + 1). */
+int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup,
+                      const int32_t *nbr, const double *fields, const double *grain,
+                      pf_op **out);
+int     pf_op_destroy(pf_op *op);
+int64_t pf_op_dim(const pf_op *op);
+
+/* Bit-exact basis work (device pointers).  unrank: idx -> basis state;
+ * rank: state -> index, or -1 for a state outside the basis. */
+int pf_basis_unrank(pf_op *op, int64_t n, const int64_t *idx, uint64_t *states);
+int pf_basis_rank(pf_op *op, int64_t n, const uint64_t *states, int64_t *idx);
+
+/* ------------------------------------------- operator-level drop-ins */
+/* All block arguments are device pointers, column-major D x s with leading
+ * dimension ld >= D, element type dtype (PF_F64 / PF_F32).  Htilde = (H - b)/a;
+ * a = 1, b = 0 gives the plain H.  Results are ordered on the handle's stream. */
+
+/* Y = Htilde X                                  (f!_rescaled, Plan.jl:173-177) */
+int pf_apply(pf_op *op, int dtype, double a, double b, int s,
+             const void *X, int64_t ldx, void *Y, int64_t ldy);
+/* b1 = c X + 2 Htilde b2 - b3       (clenshaw_recurrence, vector_dispatch.jl:120-124) */
+int pf_clenshaw_recurrence(pf_op *op, int dtype, double a, double b, double c, int s,
+                           void *b1, const void *b2, const void *b3, const void *X, int64_t ld);
+/* Y = c0 X + Htilde b1 - b2        (clenshaw_finalsum, vector_dispatch.jl:134-137) */
+int pf_clenshaw_finalsum(pf_op *op, int dtype, double a, double b, double c0, int s,
+                         const void *b1, const void *b2, void *Y, const void *X, int64_t ld);
+/* Y = sum_{k=0}^{K} coeffs[k] T_k(Htilde) X  (ClenshawAlgorithm.jl:12-29); coeffs on host. */
+int pf_filter(pf_op *op, int dtype, double a, double b, int K, const double *coeffs,
+              int s, const void *X, int64_t ldx, void *Y, int64_t ldy);
+/* KPM moments mu[0..N-1] = (D/R) sum_r <r|T_n(Htilde)|r> (Moments.jl:42-140).
+ * probes: device D x R column-major with normalised columns, or NULL to draw
+ * R probes of probe_kind from seed on the device.  mu is a host array. */
+int pf_kpm_moments(pf_op *op, int dtype, double a, double b, int N, int R,
+                   const void *probes, int64_t ldp, int probe_kind, uint64_t seed,
+                   double *mu);
+
+/* Autotuner (no reference counterpart: the reference has no kernel variants).
+ * Times every columns-per-thread width of the Clenshaw step kernel for block
+ * width s and dtype on scratch blocks, keeps the fastest for this operator and
+ * returns it in *width; times_ms[i] (optional, 5 entries) receives the
+ * measured milliseconds per launch of widths 1, 2, 4, 8, 16 (0 if invalid). */
+int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms);
+
+/* ----------------------------------------------------------- solving */
+typedef struct pf_params {
+    int    target_kind;          /* PF_TARGET_* */
+    double target_value;         /* eta, E or eps depending on target_kind */
+    int    has_Emin, has_Emax;   /* MappingConfig.Emin / Emax given? */
+    double Emin, Emax;
+    int    has_left, has_right;  /* TransformConfig.left / right (unrescaled) */
+    double left, right;
+    int    order;                /* TransformConfig.order, 0 = automatic */
+    double cutoff;               /* 0.17 */
+    double normalization;        /* 1.0 */
+    double order_safety_factor;  /* 0.97 */
+    double tol;                  /* 1e-14 */
+    double eigentol;             /* 1e-9 */
+    double overestimate_iters;   /* 1.25 */
+    int    which;                /* PF_WHICH_LR */
+    int    dos_N;                /* 250 */
+    int    dos_R;                /* 300 */
+    int    dos_kernel;           /* PF_KERNEL_JACKSON */
+    int    probe_kind;           /* PF_PROBE_GAUSSIAN */
+    uint64_t seed;               /* probe seed */
+    const double *probes;        /* optional host D x R normalised probes (overrides seed) */
+    int    precision;            /* PF_PREC_FP64 */
+    int    reorth_passes;        /* 1 = FullRO of the reference; 2 = CGS2 */
+    int    extrema_maxdim;       /* 1000 (Plan.jl:143,160) */
+    int    refine;               /* MIXED only: FP64 refinement passes for unconverged pairs */
+    int    autotune;             /* 1: time the step-kernel variants once per (op, s, dtype) */
+} pf_params;
+
+#define PF_REPORT_MAX_CHECKS 128
+
+/* Mirrors SpectralTransformReport, FactorizationReport and BenchmarkReport
+ * (SpectralTransformReport.jl:30-71, FactorizationReport.jl:48-143,
+ * BenchmarkReport.jl:68-129). Times are seconds measured with CUDA events. */
+typedef struct pf_report {
+    double  Emin, Emax, a, b;
+    double  target, left, right;        /* rescaled units */
+    int     order;
+    double  order_safety_factor;
+    int64_t matvecs;                    /* K * s * iters + howmany */
+    int64_t kpm_block_matvecs;          /* column-matvecs spent in KPM */
+    int     blocksize, howmany;
+    int     iters_needed, iters_reserved, krylovdim;
+    double  tol, residual;
+    int     converged_tol;
+    double  eigentol, eigenresidual;
+    int     converged_eigentol;
+    int     refined;                    /* pairs repaired by FP64 refinement */
+    int     numofchecks;
+    int     converged_history[PF_REPORT_MAX_CHECKS];
+    int     krylovdim_history[PF_REPORT_MAX_CHECKS];
+    double  maxresidual_history[PF_REPORT_MAX_CHECKS];
+    /* stage times: 0 tridiagonalization, 1 mapping (filter), 2 overlap,
+     * 3 orthogonalization, 4 reorthogonalization, 5 convergence check,
+     * 6 Emin/Emax probes, 7 KPM DoS, 8 bounds+order, 9 total */
+    double  stage_seconds[10];
+    double  basis_bytes_reserved, basis_bytes_used;
+} pf_report;
+
+void pf_params_default(pf_params *p);
+
+/* POLFED solve on operator op (PolfedCore.jl:194-263).  x0 is D x s
+ * (s == 1: scalar Lanczos), in host or device memory per x0_mem.  Outputs:
+ * vals[nev] (host), vecs D x nev column-major (host or device per vecs_mem;
+ * may be NULL), report (may be NULL), *nconv = number of returned pairs,
+ * sorted ascending (LanczosMethod.jl:74-82). */
+int pf_solve(pf_op *op, const pf_params *params, int s, int nev,
+             const double *x0, int x0_mem, double *vals, double *vecs, int vecs_mem,
+             pf_report *report, int *nconv);
+
+/* (Emin, Emax) from two Lanczos probes on H (Lanczos.jl:183-212); x0 length D (host). */
+int pf_lanczos_extrema(pf_op *op, const double *x0, int maxdim, double tol, double eigentol,
+                       double *Emin, double *Emax);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POLFED_B200_H */

@@ -1,0 +1,452 @@
+"""``polfed`` and its configuration / report types, mirroring Polfed.jl's API.
+
+* ``polfed(op, x0, howmany, target; mapping, transform, fact, dos, produce_report)``
+  -- PolfedCore.jl:194-263 (operator-callback overload; the operator is a
+  matrix-free model from :mod:`models`).
+* ``MappingConfig``, ``TransformConfig``, ``FactorizationConfig``,
+  ``DoSConfig`` -- Polfed/Structs/*.jl with the PolfedDefaults.jl defaults.
+* target specs -- Polfed/Structs/TargetSpec.jl:26-58.
+* ``Report`` -- Report.jl:16-62 (SpectralTransformReport, FactorizationReport,
+  BenchmarkReport fields).
+* ``lanczos_extrema`` -- Lanczos.jl:183-212.
+* operator-level drop-ins ``apply`` / ``clenshaw_recurrence`` /
+  ``clenshaw_finalsum`` / ``chebyshev_filter`` / ``kpm_moments`` -- the
+  ``MappingConfig`` callbacks (MappingConfig.jl:28-45) and ``dos_moments``
+  (Moments.jl:42-46), on CUDA tensors.
+
+Everything runs in libpolfed_b200.so; this module only marshals arguments.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .models import Operator
+
+# ------------------------------------------------------------------ configs
+
+
+@dataclass
+class MappingConfig:
+    """MappingConfig.jl:82-103.  On the GPU the strategy is always NoParallel
+    (Plan.jl:64-67); ``Emin``/``Emax`` skip the Lanczos probes when given."""
+    Emin: Optional[float] = None
+    Emax: Optional[float] = None
+    parallel_strategy: Optional[str] = None
+    optimize_mapping: bool = False
+
+
+@dataclass
+class TransformConfig:
+    """TransformConfig.jl:77-100 (PolfedDefaults.jl:104-133)."""
+    normalization: float = 1.0
+    cutoff: float = 0.17
+    left: Optional[float] = None
+    right: Optional[float] = None
+    order: Optional[int] = None
+    order_safety_factor: float = 0.97
+    polynomialtype: str = "Chebyshev"
+
+
+@dataclass
+class FactorizationConfig:
+    """FactorizationConfig.jl:49-70 (PolfedDefaults.jl:151-191).
+    ``reorth_passes`` 1 is the reference's FullRO; 2 is CGS2."""
+    which: str = "LR"
+    tol: float = 1e-14
+    eigentol: float = 1e-9
+    overestimate_iters: float = 1.25
+    reorth_passes: int = 1
+
+
+@dataclass
+class DoSConfig:
+    """DensitiesOfStatesConfig.jl:39-51 (PolfedDefaults.jl:203-217).
+    ``probes`` (D x R, normalised columns) pins the otherwise random KPM probes."""
+    N: int = 250
+    R: int = 300
+    kernel: str = "Jackson"
+    probe_kind: str = "gaussian"
+    seed: Optional[int] = None
+    probes: Optional[np.ndarray] = None
+
+
+def normalize_target_spec(target):
+    """TargetSpec.jl:26-58 -> (kind id, value)."""
+    if isinstance(target, str):
+        if target == "maxdos":
+            return _lib.PF_TARGET_MAXDOS, 0.0
+        if target == "middle":
+            return _lib.PF_TARGET_MIDDLE, 0.0
+        raise ValueError(f"Unknown target symbol: {target}")
+    if isinstance(target, tuple) and len(target) == 2 and isinstance(target[0], str):
+        tag, val = target
+        if isinstance(val, bool) or not isinstance(val, (int, float, np.integer, np.floating)):
+            raise ValueError(f"Target tuple value must be Real, got {type(val)}")
+        if tag == "absolute":
+            raise ValueError("`(:absolute, value)` is no longer supported. Use `(:unrescaled, value)` instead.")
+        if tag == "quantile":
+            raise ValueError("`(:quantile, q)` is no longer supported.")
+        if tag == "offset":
+            if not (-1 <= val <= 1):
+                raise ValueError(f"Offset target requires `eta in [-1, 1]`, got {val}")
+            return _lib.PF_TARGET_OFFSET, float(val)
+        if tag == "unrescaled":
+            return _lib.PF_TARGET_UNRESCALED, float(val)
+        if tag == "rescaled":
+            return _lib.PF_TARGET_RESCALED, float(val)
+        raise ValueError(f"Unknown target tuple tag: {tag}")
+    if isinstance(target, (int, float, np.integer, np.floating)) and not isinstance(target, bool):
+        return _lib.PF_TARGET_UNRESCALED, float(target)
+    raise ValueError(f"Unsupported target specification: {target}")
+
+
+def expectedkrylovdim(howmany: int, blocksize: int, eta: float) -> int:
+    """PolfedDefaults.jl:61-62."""
+    return int(math.ceil((20.427 * blocksize + 1.696 * howmany) * eta))
+
+
+# ------------------------------------------------------------------ reports
+
+STAGES = ("tridiagonalization", "mapping", "overlap", "orthogonalization", "reorthogonalization",
+          "convergence", "extrema", "dos", "bounds_order", "total")
+
+
+@dataclass
+class SpectralTransformReport:
+    target: float
+    target_strategy: str
+    left: float
+    right: float
+    polynomialtype: str
+    order: int
+    order_safety_factor: float
+    howmany: int
+    matrixvec_muls: int
+    Emin: float
+    Emax: float
+    a: float
+    b: float
+
+
+@dataclass
+class FactorizationReport:
+    factorizationtype: str
+    blocksize: int
+    howmany: int
+    itersneeded: int
+    itersreserved: int
+    krylovdim: int
+    tol: float
+    residual: float
+    converged_tol: int
+    eigentol: float
+    eigenresidual: float
+    converged_eigentol: int
+    numofchecks: int
+    converged_history: list
+    krylovbasisdim_history: list
+    maxresidual_history: list
+
+
+@dataclass
+class BenchmarkReport:
+    stage_seconds: dict
+    basis_bytes_reserved: float
+    basis_bytes_used: float
+    kpm_block_matvecs: int
+
+
+@dataclass
+class Report:
+    spectral: SpectralTransformReport
+    factorization: FactorizationReport
+    benchmark: BenchmarkReport
+
+
+def _target_strategy(kind: int, value: float) -> str:
+    return {0: ":maxdos", 1: ":middle", 2: f"(:offset, {value:.6g})", 3: f"(:unrescaled, {value:.6g})",
+            4: f"(:rescaled, {value:.6g})"}[kind]
+
+
+def _make_report(r: _lib.pf_report, kind: int, value: float) -> Report:
+    n = r.numofchecks
+    spec = SpectralTransformReport(r.target, _target_strategy(kind, value), r.left, r.right, "Chebyshev", r.order,
+                                   r.order_safety_factor, r.howmany, int(r.matvecs), r.Emin, r.Emax, r.a, r.b)
+    fac = FactorizationReport("LanczosFactorization" if r.blocksize == 1 else "BlockLanczosFactorization",
+                              r.blocksize, r.howmany, r.iters_needed, r.iters_reserved, r.krylovdim, r.tol,
+                              r.residual, r.converged_tol, r.eigentol, r.eigenresidual, r.converged_eigentol,
+                              r.numofchecks, list(r.converged_history[:n]), list(r.krylovdim_history[:n]),
+                              list(r.maxresidual_history[:n]))
+    bench = BenchmarkReport({k: r.stage_seconds[i] for i, k in enumerate(STAGES)}, r.basis_bytes_reserved,
+                            r.basis_bytes_used, int(r.kpm_block_matvecs))
+    return Report(spec, fac, bench)
+
+
+def display_report(report: Report) -> str:
+    """Plain-text summary in the layout of Report.jl:47-62 (no colours)."""
+    s, f, b = report.spectral, report.factorization, report.benchmark
+    lines = [
+        "Spectral Transformation Report:",
+        f"- Targeted {s.howmany} eigenpairs with strategy {s.target_strategy} at rescaled energy {s.target:.6f}",
+        f"- Exposing ev's in the rescaled interval [{s.left:.2e}, {s.right:.2e}], with width "
+        f"δ = {s.right - s.left:.2e}",
+        f"- Performing '{s.polynomialtype}' spectral transformation of order K = {s.order} "
+        f"(and order safety factor {s.order_safety_factor})",
+        f"- Matrix multiplication performed {s.matrixvec_muls} times!",
+        f"Factorization Report: ({f.factorizationtype} with blocksize {f.blocksize})",
+        f"- Number of converged eigenpairs:   {min(f.converged_tol, f.converged_eigentol)} (out of {f.howmany} requested)",
+        f"- Lanczos convergence satisfied by: {f.converged_tol} (with tolerance {f.tol:.2e}, max residual {f.residual:.2e})",
+        f"- Eigen convergence satisfied by:   {f.converged_eigentol} (with tolerance {f.eigentol:.2e}, "
+        f"max residual {f.eigenresidual:.2e})",
+        f"- Iterations needed: {f.itersneeded} (out of {f.itersreserved} reserved)",
+        "Timings (CUDA events, seconds): " + ", ".join(f"{k}={v:.4f}" for k, v in b.stage_seconds.items()),
+    ]
+    text = "\n".join(lines)
+    print(text)
+    return text
+
+
+# ------------------------------------------------------------------ solving
+
+def _params(op: Operator, howmany: int, target, mapping: MappingConfig, transform: TransformConfig,
+            fact: FactorizationConfig, dos: DoSConfig, precision: str):
+    p = _lib.pf_params()
+    _lib.load().pf_params_default(ctypes.byref(p))
+    kind, val = normalize_target_spec(target)
+    p.target_kind, p.target_value = kind, val
+    if mapping.Emin is not None:
+        p.has_Emin, p.Emin = 1, float(mapping.Emin)
+    if mapping.Emax is not None:
+        p.has_Emax, p.Emax = 1, float(mapping.Emax)
+    if transform.polynomialtype != "Chebyshev":
+        raise NotImplementedError("only the Chebyshev filter is implemented")
+    if transform.left is not None:
+        p.has_left, p.left = 1, float(transform.left)
+    if transform.right is not None:
+        p.has_right, p.right = 1, float(transform.right)
+    p.order = 0 if transform.order is None else int(transform.order)
+    if transform.order is not None and transform.order <= 0:
+        raise ValueError("order must be positive")
+    p.cutoff = transform.cutoff
+    p.normalization = transform.normalization
+    p.order_safety_factor = transform.order_safety_factor
+    if fact.which not in ("LR", "SR"):
+        raise ValueError(f"Unknown sorting mode: {fact.which}")
+    p.which = _lib.PF_WHICH_LR if fact.which == "LR" else _lib.PF_WHICH_SR
+    p.tol = fact.tol
+    p.eigentol = fact.eigentol
+    p.overestimate_iters = fact.overestimate_iters
+    p.reorth_passes = int(fact.reorth_passes)
+    p.dos_N, p.dos_R = int(dos.N), int(dos.R)
+    if dos.kernel not in _lib.KERNEL_IDS:
+        raise ValueError(f"Unknown kernel: {dos.kernel}. Available: {list(_lib.KERNEL_IDS)}")
+    p.dos_kernel = _lib.KERNEL_IDS[dos.kernel]
+    p.probe_kind = {"gaussian": _lib.PF_PROBE_GAUSSIAN, "rademacher": _lib.PF_PROBE_RADEMACHER}[dos.probe_kind]
+    p.seed = int(dos.seed) if dos.seed is not None else int(np.random.default_rng().integers(0, 2 ** 63))
+    p.precision = {"fp64": _lib.PF_PREC_FP64, "mixed": _lib.PF_PREC_MIXED}[precision]
+    keep = None
+    if dos.probes is not None:
+        keep = np.asfortranarray(dos.probes, dtype=np.float64)
+        if keep.shape != (op.dim, dos.R):
+            raise ValueError(f"probes must be D x R = {op.dim} x {dos.R}")
+        p.probes = keep.ctypes.data
+    return p, keep, kind, val
+
+
+def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = False,
+           mapping: Optional[MappingConfig] = None, transform: Optional[TransformConfig] = None,
+           fact: Optional[FactorizationConfig] = None, dos: Optional[DoSConfig] = None,
+           precision: str = "fp64", vecs: bool = True):
+    """POLFED on the B200 (PolfedCore.jl:194-263).
+
+    ``x0`` is a host array, D (scalar Lanczos) or D x s (block Lanczos); a
+    non-normalised / non-orthonormal start is replaced by a normalised copy,
+    as the reference does.  Returns ``(vals, vecs)`` or
+    ``(vals, vecs, report)``: the converged eigenpairs, ascending."""
+    mapping = mapping or MappingConfig()
+    transform = transform or TransformConfig()
+    fact = fact or FactorizationConfig()
+    dos = dos or DoSConfig()
+    if howmany < 1:
+        raise ValueError("howmany must be positive")
+    x = np.asarray(x0, dtype=np.float64)
+    if x.ndim not in (1, 2):
+        raise ValueError("x0 must be a vector or a matrix")
+    D = op.dim
+    if x.shape[0] != D:
+        raise ValueError(f"x0 has {x.shape[0]} rows; the operator dimension is {D}")
+    if x.size == 0:
+        raise ValueError("POLFED initial vector must not be empty.")
+    s = 1 if x.ndim == 1 else x.shape[1]
+    xf = np.asfortranarray(x.reshape(D, s))
+    p, keep, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
+    vals = np.zeros(howmany)
+    V = np.zeros((D, howmany), order="F") if vecs else None
+    rep = _lib.pf_report()
+    n = ctypes.c_int(0)
+    _lib.check(_lib.load().pf_solve(op.op, ctypes.byref(p), s, howmany, xf.ctypes.data, _lib.PF_MEM_HOST,
+                                    vals.ctypes.data, V.ctypes.data if vecs else None, _lib.PF_MEM_HOST,
+                                    ctypes.byref(rep), ctypes.byref(n)))
+    del keep
+    k = n.value
+    out_vals = vals[:k].copy()
+    out_vecs = V[:, :k].copy() if vecs else None
+    if produce_report:
+        return out_vals, out_vecs, _make_report(rep, kind, val)
+    return out_vals, out_vecs
+
+
+def lanczos_extrema(op: Operator, x0, maxdim: int = 1000, tol: float = 1e-14, eigentol: float = 1e-8):
+    """(Emin, Emax) by two Lanczos probes (Lanczos.jl:183-212)."""
+    x = np.ascontiguousarray(x0, dtype=np.float64).ravel()
+    if len(x) != op.dim:
+        raise ValueError("x0 length must match the matrix dimension.")
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.load().pf_lanczos_extrema(op.op, x.ctypes.data, maxdim, tol, eigentol,
+                                              ctypes.byref(lo), ctypes.byref(hi)))
+    return lo.value, hi.value
+
+
+# ---------------------------------------------------- operator-level drop-ins
+
+def _cm(t, D):
+    """(pointer, s, ld, dtype id) of a CUDA tensor holding a column-major D x s block."""
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda):
+        raise ValueError("operator-level calls take CUDA tensors")
+    if t.dtype == torch.float64:
+        dt = _lib.PF_F64
+    elif t.dtype == torch.float32:
+        dt = _lib.PF_F32
+    else:
+        raise ValueError("dtype must be float64 or float32")
+    if t.dim() == 1:
+        if t.shape[0] != D or t.stride(0) != 1:
+            raise ValueError("vector length must equal the operator dimension and be contiguous")
+        return t.data_ptr(), 1, D, dt
+    if t.dim() != 2 or t.shape[0] != D or t.stride(0) != 1:
+        raise ValueError("blocks must be column-major D x s (stride(0) == 1)")
+    return t.data_ptr(), t.shape[1], max(t.stride(1), D), dt
+
+
+def col_major(D: int, s: int, dtype=None, device: int = 0):
+    """An uninitialised column-major D x s CUDA tensor."""
+    import torch
+    dtype = torch.float64 if dtype is None else dtype
+    return torch.empty((s, D), dtype=dtype, device=f"cuda:{device}").t()
+
+
+def _sync_in(op):
+    import torch
+    torch.cuda.synchronize(op.device)
+
+
+def _sync_out(op):
+    _lib.synchronize(op.handle)
+
+
+def apply(op: Operator, Y, X, a: float = 1.0, b: float = 0.0):
+    """Y = (H X - b X)/a  (f!_rescaled of Plan.jl:173-177; a=1, b=0: f!)."""
+    D = op.dim
+    px, s, ldx, dt = _cm(X, D)
+    py, s2, ldy, dt2 = _cm(Y, D)
+    if s != s2 or dt != dt2:
+        raise ValueError("X and Y must have the same shape and dtype")
+    _sync_in(op)
+    _lib.check(_lib.load().pf_apply(op.op, dt, a, b, s, px, ldx, py, ldy))
+    _sync_out(op)
+    return Y
+
+
+def clenshaw_recurrence(op: Operator, b1, b2, b3, c: float, X, a: float = 1.0, b: float = 0.0):
+    """b1 = c X + 2 Htilde b2 - b3 (vector_dispatch.jl:113-125)."""
+    D = op.dim
+    p1, s, ld, dt = _cm(b1, D)
+    ptrs = [_cm(t, D) for t in (b2, b3, X)]
+    if any(q[1] != s or q[2] != ld or q[3] != dt for q in ptrs):
+        raise ValueError("all blocks must share shape, leading dimension and dtype")
+    _sync_in(op)
+    _lib.check(_lib.load().pf_clenshaw_recurrence(op.op, dt, a, b, c, s, p1, ptrs[0][0], ptrs[1][0], ptrs[2][0], ld))
+    _sync_out(op)
+    return b1
+
+
+def clenshaw_finalsum(op: Operator, b1, b2, c0: float, Y, X, a: float = 1.0, b: float = 0.0):
+    """Y = c0 X + Htilde b1 - b2 (vector_dispatch.jl:127-139)."""
+    D = op.dim
+    py, s, ld, dt = _cm(Y, D)
+    ptrs = [_cm(t, D) for t in (b1, b2, X)]
+    if any(q[1] != s or q[2] != ld or q[3] != dt for q in ptrs):
+        raise ValueError("all blocks must share shape, leading dimension and dtype")
+    _sync_in(op)
+    _lib.check(_lib.load().pf_clenshaw_finalsum(op.op, dt, a, b, c0, s, ptrs[0][0], ptrs[1][0], py, ptrs[2][0], ld))
+    _sync_out(op)
+    return Y
+
+
+def chebyshev_filter(op: Operator, Y, X, coeffs, a: float = 1.0, b: float = 0.0):
+    """Y = sum_k coeffs[k] T_k(Htilde) X (ClenshawAlgorithm.jl:12-29)."""
+    D = op.dim
+    px, s, ldx, dt = _cm(X, D)
+    py, s2, ldy, dt2 = _cm(Y, D)
+    if s != s2 or dt != dt2:
+        raise ValueError("X and Y must have the same shape and dtype")
+    c = np.ascontiguousarray(coeffs, dtype=np.float64)
+    _sync_in(op)
+    _lib.check(_lib.load().pf_filter(op.op, dt, a, b, len(c) - 1, c.ctypes.data, s, px, ldx, py, ldy))
+    _sync_out(op)
+    return Y
+
+
+def kpm_moments(op: Operator, N: int, R: int, a: float = 1.0, b: float = 0.0, probes=None,
+                probe_kind: str = "gaussian", seed: int = 0, dtype: str = "fp64"):
+    """KPM moments (Moments.jl:42-140); ``probes`` a column-major D x R CUDA tensor."""
+    mu = np.zeros(N)
+    if probes is not None:
+        pp, R2, ldp, dt = _cm(probes, op.dim)
+        if R2 != R:
+            raise ValueError("probes must have R columns")
+    else:
+        pp, ldp = None, op.dim
+        dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
+    kind = {"gaussian": _lib.PF_PROBE_GAUSSIAN, "rademacher": _lib.PF_PROBE_RADEMACHER}[probe_kind]
+    _sync_in(op)
+    _lib.check(_lib.load().pf_kpm_moments(op.op, dt, a, b, N, R, pp, ldp, kind, seed, mu.ctypes.data))
+    _sync_out(op)
+    return mu
+
+
+def autotune(op: Operator, s: int, dtype: str = "fp64"):
+    """Time every columns-per-thread width of the step kernel for block width
+    ``s``; the fastest is kept on the operator.  Returns (width, {width: ms})."""
+    w = ctypes.c_int(0)
+    t = (ctypes.c_float * 5)()
+    dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
+    _lib.check(_lib.load().pf_autotune(op.op, dt, int(s), ctypes.byref(w), ctypes.addressof(t)))
+    return w.value, {1 << i: t[i] for i in range(5) if t[i] > 0}
+
+
+def basis_states(op: Operator, idx):
+    """Basis states of indices ``idx`` (CUDA int64 tensor) -> CUDA uint64-as-int64 tensor."""
+    import torch
+    out = torch.empty_like(idx)
+    _sync_in(op)
+    _lib.check(_lib.load().pf_basis_unrank(op.op, idx.numel(), idx.data_ptr(), out.data_ptr()))
+    _sync_out(op)
+    return out
+
+
+def basis_index(op: Operator, states):
+    """Indices of basis ``states`` (CUDA int64 tensor), -1 when outside the sector."""
+    import torch
+    out = torch.empty_like(states)
+    _sync_in(op)
+    _lib.check(_lib.load().pf_basis_rank(op.op, states.numel(), states.data_ptr(), out.data_ptr()))
+    _sync_out(op)
+    return out

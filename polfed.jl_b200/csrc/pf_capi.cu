@@ -1,0 +1,240 @@
+// pf_capi.cu -- the extern "C" boundary of libpolfed_b200.so.
+// Every entry point converts C++ exceptions into a status code plus a
+// thread-local message (pf_last_error), so nothing but ints and plain
+// pointers crosses the ABI.
+#include "pf_internal.h"
+#include "pf_solver.h"
+
+#include <cstring>
+#include <string>
+
+namespace pf {
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace pf
+
+#define PF_API_BEGIN try {
+#define PF_API_END                                              \
+    return PF_OK;                                               \
+    }                                                           \
+    catch (const pf::Error &e) {                                \
+        pf::set_last_error(e.what());                           \
+        return e.code;                                          \
+    }                                                           \
+    catch (const std::bad_alloc &) {                            \
+        pf::set_last_error("host allocation failed");           \
+        return PF_ERR_NOMEM;                                    \
+    }                                                           \
+    catch (const std::exception &e) {                           \
+        pf::set_last_error(e.what());                           \
+        return PF_ERR_CUDA;                                     \
+    }
+
+extern "C" {
+
+int pf_abi_version(void) { return PF_ABI_VERSION; }
+
+const char *pf_last_error(void) { return pf::g_last_error.c_str(); }
+
+int pf_handle_create(int device, pf_handle **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    int ndev = 0;
+    PF_CUDA(cudaGetDeviceCount(&ndev));
+    PF_CHECK(device >= 0 && device < ndev, PF_ERR_INVALID, "no such CUDA device");
+    PF_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    PF_CUDA(cudaGetDeviceProperties(&prop, device));
+    PF_CHECK(prop.major >= 10, PF_ERR_UNSUPPORTED, "libpolfed_b200 is built for sm_100a (B200) only");
+    pf_handle *h = new pf_handle();
+    h->device = device;
+    h->num_sms = prop.multiProcessorCount;
+    try {
+        PF_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        PF_CUBLAS(cublasCreate(&h->blas));
+        PF_CUBLAS(cublasSetStream(h->blas, h->stream));
+        PF_CUSOLVER(cusolverDnCreate(&h->solver));
+        PF_CUSOLVER(cusolverDnSetStream(h->solver, h->stream));
+        PF_CUDA(cudaMalloc(&h->red_counter, 64 * sizeof(unsigned int)));
+        PF_CUDA(cudaMemset(h->red_counter, 0, 64 * sizeof(unsigned int)));
+    } catch (...) {
+        if (h->blas) cublasDestroy(h->blas);
+        if (h->solver) cusolverDnDestroy(h->solver);
+        if (h->stream) cudaStreamDestroy(h->stream);
+        delete h;
+        throw;
+    }
+    *out = h;
+    PF_API_END
+}
+
+int pf_handle_destroy(pf_handle *h) {
+    PF_API_BEGIN
+    if (!h) return PF_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->blas) cublasDestroy(h->blas);
+    if (h->solver) cusolverDnDestroy(h->solver);
+    if (h->scratch) cudaFree(h->scratch);
+    if (h->red_partials) cudaFree(h->red_partials);
+    if (h->red_counter) cudaFree(h->red_counter);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    PF_API_END
+}
+
+int pf_handle_stream(pf_handle *h, void **stream) {
+    PF_API_BEGIN
+    PF_CHECK(h && stream, PF_ERR_INVALID, "null argument");
+    *stream = (void *)h->stream;
+    PF_API_END
+}
+
+int pf_handle_synchronize(pf_handle *h) {
+    PF_API_BEGIN
+    PF_CHECK(h, PF_ERR_INVALID, "null handle");
+    PF_CUDA(cudaSetDevice(h->device));
+    PF_CUDA(cudaStreamSynchronize(h->stream));
+    PF_API_END
+}
+
+int pf_op_spin_chain_create(pf_handle *h, int L, int Lup, int nbonds, const int32_t *bonds, const double *J,
+                            const double *Delta, const double *fields, pf_op **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    *out = pf::create_spin_chain(h, L, Lup, nbonds, bonds, J, Delta, fields);
+    PF_API_END
+}
+
+int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup, const int32_t *nbr,
+                      const double *fields, const double *grain, pf_op **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    *out = pf::create_qsun(h, L_loc, L_grain, g0, coup, nbr, fields, grain);
+    PF_API_END
+}
+
+int pf_op_destroy(pf_op *op) {
+    PF_API_BEGIN
+    pf::destroy_op(op);
+    PF_API_END
+}
+
+int64_t pf_op_dim(const pf_op *op) { return op ? op->dim : -1; }
+
+int pf_basis_unrank(pf_op *op, int64_t n, const int64_t *idx, uint64_t *states) {
+    PF_API_BEGIN
+    PF_CHECK(op && (n == 0 || (idx && states)), PF_ERR_INVALID, "null argument");
+    PF_CHECK(op->kind == pf::OP_CHAIN, PF_ERR_UNSUPPORTED, "basis rank/unrank applies to spin-chain operators");
+    PF_CUDA(cudaSetDevice(op->h->device));
+    pf::launch_unrank(op, op->h->stream, n, idx, states);
+    PF_API_END
+}
+
+int pf_basis_rank(pf_op *op, int64_t n, const uint64_t *states, int64_t *idx) {
+    PF_API_BEGIN
+    PF_CHECK(op && (n == 0 || (idx && states)), PF_ERR_INVALID, "null argument");
+    PF_CHECK(op->kind == pf::OP_CHAIN, PF_ERR_UNSUPPORTED, "basis rank/unrank applies to spin-chain operators");
+    PF_CUDA(cudaSetDevice(op->h->device));
+    pf::launch_rank(op, op->h->stream, n, states, idx);
+    PF_API_END
+}
+
+int pf_apply(pf_op *op, int dtype, double a, double b, int s, const void *X, int64_t ldx, void *Y, int64_t ldy) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::op_apply(op, dtype, a, b, s, X, ldx, Y, ldy);
+    PF_API_END
+}
+
+int pf_clenshaw_recurrence(pf_op *op, int dtype, double a, double b, double c, int s, void *b1, const void *b2,
+                           const void *b3, const void *X, int64_t ld) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::op_recurrence(op, dtype, a, b, c, s, b1, b2, b3, X, ld);
+    PF_API_END
+}
+
+int pf_clenshaw_finalsum(pf_op *op, int dtype, double a, double b, double c0, int s, const void *b1, const void *b2,
+                         void *Y, const void *X, int64_t ld) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::op_finalsum(op, dtype, a, b, c0, s, b1, b2, Y, X, ld);
+    PF_API_END
+}
+
+int pf_filter(pf_op *op, int dtype, double a, double b, int K, const double *coeffs, int s, const void *X,
+              int64_t ldx, void *Y, int64_t ldy) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::op_filter(op, dtype, a, b, K, coeffs, s, X, ldx, Y, ldy);
+    PF_API_END
+}
+
+int pf_kpm_moments(pf_op *op, int dtype, double a, double b, int N, int R, const void *probes, int64_t ldp,
+                   int probe_kind, uint64_t seed, double *mu) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::op_kpm(op, dtype, a, b, N, R, probes, ldp, probe_kind, seed, mu);
+    PF_API_END
+}
+
+int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms) {
+    PF_API_BEGIN
+    PF_CHECK(op && width, PF_ERR_INVALID, "null argument");
+    std::vector<std::pair<int, float>> t;
+    *width = pf::autotune_step(op, s, dtype, &t);
+    if (times_ms) {
+        for (int i = 0; i < 5; ++i) times_ms[i] = 0.f;
+        for (auto &pr : t) {
+            int idx = 0;
+            while ((1 << idx) < pr.first) ++idx;
+            if (idx < 5) times_ms[idx] = pr.second;
+        }
+    }
+    PF_API_END
+}
+
+void pf_params_default(pf_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->target_kind = PF_TARGET_MAXDOS;
+    p->target_value = 0.0;
+    p->order = 0;
+    p->cutoff = 0.17;               // PolfedDefaults.jl:119
+    p->normalization = 1.0;         // :126
+    p->order_safety_factor = 0.97;  // :133
+    p->tol = 1e-14;                 // :177
+    p->eigentol = 1e-9;             // :184
+    p->overestimate_iters = 1.25;   // :151
+    p->which = PF_WHICH_LR;         // :191
+    p->dos_N = 250;                 // :210
+    p->dos_R = 300;                 // :217
+    p->dos_kernel = PF_KERNEL_JACKSON;
+    p->probe_kind = PF_PROBE_GAUSSIAN;
+    p->seed = 0x5eed5eedULL;
+    p->probes = nullptr;
+    p->precision = PF_PREC_FP64;
+    p->reorth_passes = 1;
+    p->extrema_maxdim = 1000;       // Plan.jl:143,160
+    p->refine = 1;
+    p->autotune = 1;
+}
+
+int pf_solve(pf_op *op, const pf_params *params, int s, int nev, const double *x0, int x0_mem, double *vals,
+             double *vecs, int vecs_mem, pf_report *report, int *nconv) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::solve(op, params, s, nev, x0, x0_mem, vals, vecs, vecs_mem, report, nconv);
+    PF_API_END
+}
+
+int pf_lanczos_extrema(pf_op *op, const double *x0, int maxdim, double tol, double eigentol, double *Emin,
+                       double *Emax) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::lanczos_extrema(op, x0, maxdim, tol, eigentol, Emin, Emax);
+    PF_API_END
+}
+
+}  // extern "C"

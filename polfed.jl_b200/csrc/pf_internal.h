@@ -1,0 +1,197 @@
+// pf_internal.h -- internal types shared by the kernels, the solver and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+#include <stdint.h>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <stdexcept>
+
+#include "../../include/polfed_b200.h"
+
+#define PF_MAX_BONDS 64
+#define PF_MAX_SITES 32
+#define PF_MAX_GRAIN 16   // dg = 2^L_grain <= 16
+#define PF_MAX_LOC   32
+
+namespace pf {
+
+// ---------------------------------------------------------------- errors
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void set_last_error(const std::string &msg);
+
+#define PF_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            throw ::pf::Error(e_ == cudaErrorMemoryAllocation ? PF_ERR_NOMEM : PF_ERR_CUDA, \
+                              std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+#define PF_CUBLAS(call)                                                                 \
+    do {                                                                                \
+        cublasStatus_t e_ = (call);                                                     \
+        if (e_ != CUBLAS_STATUS_SUCCESS)                                                \
+            throw ::pf::Error(PF_ERR_CUDA, std::string(#call) + ": cublas status " +    \
+                                               std::to_string((int)e_));                \
+    } while (0)
+#define PF_CUSOLVER(call)                                                               \
+    do {                                                                                \
+        cusolverStatus_t e_ = (call);                                                   \
+        if (e_ != CUSOLVER_STATUS_SUCCESS)                                              \
+            throw ::pf::Error(PF_ERR_CUDA, std::string(#call) + ": cusolver status " +  \
+                                               std::to_string((int)e_));                \
+    } while (0)
+#define PF_CHECK(cond, code, msg)                                                       \
+    do {                                                                                \
+        if (!(cond)) throw ::pf::Error((code), (msg));                                  \
+    } while (0)
+
+// ------------------------------------------------------- operator descriptors
+// Both descriptors are passed to kernels by value (kernel parameter space), so
+// every thread of a warp reads the same bond / flip entry at the same time and
+// the access is a broadcast.
+
+// Spin-1/2 chain on an Sz sector (or the full 2^L space when full != 0).
+template <typename T>
+struct ChainDesc {
+    int L, Lup, nb, nchunks, full;
+    uint32_t bmask[PF_MAX_BONDS];  // (1 << i) | (1 << j)
+    uint8_t bi[PF_MAX_BONDS], bj[PF_MAX_BONDS];
+    T jhalf[PF_MAX_BONDS];         // J_b / 2            (off-diagonal element)
+    T jdq[PF_MAX_BONDS];           // J_b * Delta_b / 4  (Sz Sz with Sz = +-1/2)
+    T hhalf[PF_MAX_SITES];         // h_i / 2            (h Sz with Sz = +-1/2)
+    const uint32_t *states;        // D basis states (sector only)
+    const uint32_t *rank_tab;      // chunked rank tables (sector only)
+};
+
+// Spin-1/2 Quantum Sun in the full space; grain = the low L_grain bits.
+template <typename T>
+struct QSunDesc {
+    int L, L_grain, L_loc, dg;
+    uint32_t fmask[PF_MAX_LOC];     // (1 << (L_grain + j)) | (1 << nbr[j])
+    uint8_t site[PF_MAX_LOC];       // L_grain + j
+    T cflip[PF_MAX_LOC];            // g0 * coup[j] / 4
+    T hhalf[PF_MAX_LOC];            // h_j / 2
+    T grain[PF_MAX_GRAIN * PF_MAX_GRAIN];  // row-major dg x dg
+};
+
+enum OpKind { OP_CHAIN = 0, OP_QSUN = 1 };
+
+// Number of entries of the chunked rank table for an L-bit sector:
+// chunk c (bits 8c..8c+7) holds (8c+1) x 256 entries.
+__host__ __device__ inline int rank_table_entries(int nchunks) {
+    int n = 0;
+    for (int c = 0; c < nchunks; ++c) n += (8 * c + 1) * 256;
+    return n;
+}
+__host__ __device__ inline int rank_table_offset(int c) {
+    int n = 0;
+    for (int q = 0; q < c; ++q) n += (8 * q + 1) * 256;
+    return n;
+}
+
+}  // namespace pf
+
+// ------------------------------------------------------------ opaque handles
+struct pf_handle {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cublasHandle_t blas = nullptr;
+    cusolverDnHandle_t solver = nullptr;
+    // per-handle scratch, grown on demand
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    double *red_partials = nullptr;   // deterministic reduction partials
+    size_t red_partials_len = 0;
+    unsigned int *red_counter = nullptr;
+};
+
+struct pf_op {
+    pf_handle *h = nullptr;
+    int kind = 0;
+    int64_t dim = 0;
+    int L = 0, Lup = -1;
+    pf::ChainDesc<double> chain64;
+    pf::ChainDesc<float> chain32;
+    pf::QSunDesc<double> qsun64;
+    pf::QSunDesc<float> qsun32;
+    uint32_t *d_states = nullptr;
+    uint32_t *d_rank_tab = nullptr;
+    int smem_bytes = 0;               // dynamic shared memory of the step kernels
+    // autotuned columns-per-thread of the step kernel, keyed by (element bytes, s)
+    std::mutex tune_mu;
+    std::map<std::pair<int, int>, int> tuned_width;
+    // host copies of the defining parameters (for reports and re-creation)
+    std::vector<int32_t> bonds;
+    std::vector<double> J, Delta, fields, coup, grain;
+    std::vector<int32_t> nbr;
+    double g0 = 0.0;
+    int L_loc = 0, L_grain = 0;
+};
+
+namespace pf {
+
+// ------------------------------------------------------------ kernel API
+// A "block" here is row-interleaved (RI): element (row i, column c) at i*s + c.
+
+struct StepFlags {
+    enum : int { Q = 1, P = 2, X = 4, DOTS = 8 };
+};
+
+// out = cx*X + alpha*Htilde(q) + beta*p   (RI layout, s columns)
+//   Htilde q = (H q - shift q) * inva
+// flags select which of q / p / X take part; DOTS accumulates per column
+// <out,out> and <out,q> into dots[2*s] (deterministic two-stage reduction).
+template <typename T>
+void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p,
+                 const T *x, T *out, double cx, double alpha, double beta, double inva,
+                 double shift, int flags, double *dots);
+
+// Same with an explicit columns-per-thread width V (s % V == 0, V*sizeof(T) <= 64).
+template <typename T>
+void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p, const T *x, T *out,
+                       double cx, double alpha, double beta, double inva, double shift, int flags, double *dots,
+                       int V);
+int default_width(int s, int elem_bytes);
+// Times every columns-per-thread width of the Clenshaw step for (s, dtype) on
+// scratch blocks and records the fastest in op->tuned_width.  Returns it.
+int autotune_step(pf_op *op, int s, int dtype, std::vector<std::pair<int, float>> *timings);
+
+// RI <-> column-major conversion, optional precision change.
+template <typename TS, typename TD>
+void launch_cm_to_ri(cudaStream_t st, int64_t D, int s, const TS *src, int64_t ld, TD *dst);
+template <typename TS, typename TD>
+void launch_ri_to_cm(cudaStream_t st, int64_t D, int s, const TS *src, TD *dst, int64_t ld);
+
+// Per-column dot products of RI blocks: out[c] = sum_i A[i,c] * B[i,c] (FP64 result).
+template <typename T>
+void launch_coldots(pf_handle *h, cudaStream_t st, int64_t D, int s, const T *A, const T *B,
+                    double *out);
+// out[c] = || HA[:,c] - e[c] A[:,c] ||^2  (RI blocks, FP64)
+void launch_colresid(pf_handle *h, cudaStream_t st, int64_t D, int s, const double *HA,
+                     const double *A, const double *e, double *out);
+
+// Probe generation (RI, D x R): Gaussian or Rademacher from a counter hash.
+template <typename T>
+void launch_probes(cudaStream_t st, int64_t D, int R, int kind, uint64_t seed, int col0, T *dst);
+template <typename T>
+void launch_scale_cols(cudaStream_t st, int64_t D, int s, T *A, const double *scale);
+
+void launch_unrank(pf_op *op, cudaStream_t st, int64_t n, const int64_t *idx, uint64_t *out);
+void launch_rank(pf_op *op, cudaStream_t st, int64_t n, const uint64_t *states, int64_t *out);
+
+// grid sizing helper: persistent grid of num_sms * blocks_per_sm CTAs at most
+int grid_for(pf_handle *h, int64_t work_items, int threads, int blocks_per_sm);
+
+void ensure_reduction(pf_handle *h, size_t n);
+
+}  // namespace pf

@@ -1,0 +1,808 @@
+// pf_kernels.cu -- matrix-free Hamiltonian kernels for sm_100a.
+//
+// One fused row kernel serves every operator application of the path:
+//   out = cx*X + alpha*Htilde(q) + beta*p,   Htilde q = (H q)/a - (b/a) q
+// which is
+//   * the Clenshaw recurrence  b_k = c_k X + 2 Htilde b_{k+1} - b_{k+2}
+//     (Clenshaw.jl:69-81, vector_dispatch.jl:120-123) with b_k written in
+//     place over b_{k+2} (each element is read then written by one thread);
+//   * the final sum            Y = c_0 X + Htilde b_1 - b_2 (Clenshaw.jl:104-117);
+//   * the KPM step             v_{n+1} = 2 Htilde v_n - v_{n-1} (Moments.jl:133-139)
+//     with per-column <v_{n+1}, v_{n+1}> and <v_{n+1}, v_n> fused in;
+//   * the plain / rescaled apply (Plan.jl:173-177, PolfedCore.jl:172).
+//
+// Blocks are row-interleaved (element (i, c) at i*s + c), so the s values a
+// Hamiltonian flip gathers from row j are one contiguous 8*s or 4*s byte run.
+// The matrix is never stored: each thread derives its row's basis state,
+// diagonal and flipped neighbours from the operator descriptor.
+//   * spin chain (SpinHalfChains.jl:267-315): diagonal sum_i h_i Sz_i +
+//     sum_b J_b Delta_b Sz_i Sz_j in the reference's summation order (bit-exact
+//     in FP64); one flip per bond with unequal spins, value J_b/2; the flipped
+//     state's index comes from the combinatorial number system
+//     rank(s) = sum_k C(p_k, k) (p_1 < p_2 < ... the set bits) evaluated with
+//     per-byte lookup tables held in shared memory.
+//   * Quantum Sun (QuantumSun.jl:1-102, S=1/2): index == state; L_loc flips
+//     of (outer bit, grain bit) with value g0 c_j / 4, plus the dense grain
+//     block on the low L_grain bits (held in shared memory).
+#include "pf_internal.h"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+namespace pf {
+
+template <typename T, int V>
+struct alignas(sizeof(T) * V) Pack {
+    T v[V];
+};
+
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> ldp(const T *p) {
+    return *reinterpret_cast<const Pack<T, V> *>(p);
+}
+template <typename T, int V>
+__device__ __forceinline__ void stp(T *p, const Pack<T, V> &v) {
+    *reinterpret_cast<Pack<T, V> *>(p) = v;
+}
+
+// ------------------------------------------------------------ sector rank
+__device__ __forceinline__ uint32_t sector_rank(uint32_t st, const uint32_t *tab, int nchunks) {
+    uint32_t r = 0;
+    int p = 0;
+    int off = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (c < nchunks) {
+            uint32_t byte = (st >> (8 * c)) & 0xffu;
+            r += tab[off + p * 256 + (int)byte];
+            p += __popc(byte);
+            off += (8 * c + 1) * 256;
+        }
+    }
+    return r;
+}
+
+// ------------------------------------------------------------ row models
+// Each returns (through acc / diag) the off-diagonal gather sum and the
+// diagonal element of row `row` for columns c0..c0+V-1.
+
+// Gathers are issued in unrolled batches of U independent loads so that each
+// thread keeps several L2/HBM requests in flight (the loop bodies have no
+// load-to-load dependence); accumulation follows the reference's term order.
+// U shrinks as the per-thread column count V grows, to bound registers.
+template <int V>
+struct Batch {
+    static constexpr int U = V >= 16 ? 2 : (V >= 8 ? 4 : 8);
+};
+
+template <typename T, int V, bool HASQ>
+__device__ __forceinline__ void chain_row(const ChainDesc<T> &d, const uint32_t *tab, uint32_t row,
+                                          int s, int c0, const T *__restrict__ q, T (&acc)[V],
+                                          T &diag) {
+    constexpr int U = Batch<V>::U;
+    const uint32_t st = d.full ? row : __ldg(d.states + row);
+    T dg = T(0);
+    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
+    const T *qc = q + c0;
+    for (int b0 = 0; b0 < d.nb; b0 += U) {
+        uint32_t r2[U];
+        bool act[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int b = b0 + u;
+            act[u] = false;
+            r2[u] = 0u;
+            if (b < d.nb) {
+                const uint32_t bm = d.bmask[b];
+                const uint32_t m = st & bm;
+                const bool differ = (m != 0u) && (m != bm);
+                dg += differ ? -d.jdq[b] : d.jdq[b];
+                act[u] = differ;
+                if (HASQ && differ) {
+                    const uint32_t st2 = st ^ bm;
+                    r2[u] = d.full ? st2 : sector_rank(st2, tab, d.nchunks);
+                }
+            }
+        }
+        if constexpr (HASQ) {
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (act[u]) g[u] = ldp<T, V>(qc + (size_t)r2[u] * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (act[u]) {
+                    const T jh = d.jhalf[b0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] += jh * g[u].v[v];
+                }
+        }
+    }
+    diag = dg;
+}
+
+// Quantum Sun shared-memory layout: the grain block with a padded row stride
+// (dg + 1, so the 8 rows of one grain group read different banks), then four
+// 256-entry diagonal tables, one per byte of the outer-spin bits.
+template <typename T>
+struct QSunSmem {
+    static __host__ __device__ int grain_stride(int dg) { return dg + 1; }
+    static __host__ __device__ int bytes(int dg) { return (dg * (dg + 1) + 4 * 256) * (int)sizeof(T); }
+};
+
+template <typename T, int V, bool HASQ>
+__device__ __forceinline__ void qsun_row(const QSunDesc<T> &d, const T *smem_t, uint32_t row,
+                                         int s, int c0, const T *__restrict__ q, T (&acc)[V],
+                                         T &diag) {
+    constexpr int U = Batch<V>::U;
+    const int gs = d.dg + 1;
+    const T *dtab = smem_t + d.dg * gs;
+    const uint32_t outer = row >> d.L_grain;
+    T dg = dtab[outer & 0xffu];
+    if (d.L_loc > 8) dg += dtab[256 + ((outer >> 8) & 0xffu)];
+    if (d.L_loc > 16) dg += dtab[512 + ((outer >> 16) & 0xffu)];
+    if (d.L_loc > 24) dg += dtab[768 + ((outer >> 24) & 0xffu)];
+    diag = dg;
+    if constexpr (HASQ) {
+        const T *qc = q + c0;
+        for (int j0 = 0; j0 < d.L_loc; j0 += U) {
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j0 + u < d.L_loc) g[u] = ldp<T, V>(qc + (size_t)(row ^ d.fmask[j0 + u]) * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j0 + u < d.L_loc) {
+                    const T cf = d.cflip[j0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] += cf * g[u].v[v];
+                }
+        }
+        const uint32_t g = row & ((uint32_t)d.dg - 1u);
+        const uint32_t base = row - g;
+        const T *grow = smem_t + g * gs;
+        for (int h0 = 0; h0 < d.dg; h0 += U) {
+            Pack<T, V> x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (h0 + u < d.dg) x[u] = ldp<T, V>(qc + (size_t)(base + h0 + u) * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (h0 + u < d.dg) {
+                    const T w = grow[h0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] += w * x[u].v[v];
+                }
+        }
+    }
+}
+
+template <typename T>
+struct StepArgs {
+    uint32_t D;
+    int s;
+    int G;          // column groups per row = s / V
+    uint32_t items; // D * G
+    const T *q;
+    const T *p;     // may alias out (in-place update)
+    const T *x;
+    T *out;
+    T cx, alpha, beta, inva, boa;
+    double *partials;
+    unsigned int *counter;
+    double *dots;
+};
+
+template <class Desc>
+struct DescTraits;
+template <typename T>
+struct DescTraits<ChainDesc<T>> {
+    static constexpr int kind = OP_CHAIN;
+};
+template <typename T>
+struct DescTraits<QSunDesc<T>> {
+    static constexpr int kind = OP_QSUN;
+};
+
+constexpr int kThreads = 256;
+
+// Deterministic "last block reduces" epilogue: every block writes its
+// per-column partials, the block that finishes last sums them in block order.
+__device__ void finish_reduction(int nvals, const double *blockvals, double *partials,
+                                 unsigned int *counter, double *out) {
+    __shared__ bool last;
+    for (int c = threadIdx.x; c < nvals; c += blockDim.x)
+        partials[(size_t)blockIdx.x * nvals + c] = blockvals[c];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        for (int c = threadIdx.x; c < nvals; c += blockDim.x) {
+            double acc = 0.0;
+            for (unsigned int b = 0; b < gridDim.x; ++b)
+                acc += ((volatile double *)partials)[(size_t)b * nvals + c];
+            out[c] = acc;
+        }
+        if (threadIdx.x == 0) *counter = 0u;
+    }
+}
+
+template <typename T, int V, class Desc, int FLAGS>
+__global__ void __launch_bounds__(kThreads) k_step(const Desc d, const StepArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool HASQ = (FLAGS & StepFlags::Q) != 0;
+    constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
+    constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
+    constexpr bool DOTS = (FLAGS & StepFlags::DOTS) != 0;
+    const uint32_t *tab = reinterpret_cast<const uint32_t *>(smem_raw);
+    const T *smem_t = reinterpret_cast<const T *>(smem_raw);
+    if constexpr (DescTraits<Desc>::kind == OP_CHAIN) {
+        if (HASQ && !d.full) {
+            const int n = rank_table_entries(d.nchunks);
+            uint32_t *t = reinterpret_cast<uint32_t *>(smem_raw);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) t[i] = __ldg(d.rank_tab + i);
+        }
+    } else {
+        T *sm = reinterpret_cast<T *>(smem_raw);
+        const int gs = d.dg + 1;
+        for (int i = threadIdx.x; i < d.dg * d.dg; i += blockDim.x) sm[(i / d.dg) * gs + (i % d.dg)] = d.grain[i];
+        T *dtab = sm + d.dg * gs;
+        // dtab[c*256 + byte] = sum over the 8 outer spins of chunk c of h_j (bit - 1/2)
+        for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+            const int c = i >> 8, byte = i & 255;
+            T acc = T(0);
+            for (int t = 0; t < 8; ++t) {
+                const int j = 8 * c + t;
+                if (j < d.L_loc) acc += ((byte >> t) & 1) ? d.hhalf[j] : -d.hhalf[j];
+            }
+            dtab[i] = acc;
+        }
+    }
+    __syncthreads();
+
+    double dd1[V], dd2[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) dd1[v] = dd2[v] = 0.0;
+
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t G = (uint32_t)a.G;
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < a.items; it += stride) {
+        const uint32_t row = (G == 1u) ? it : it / G;
+        const int c0 = (G == 1u) ? 0 : (int)(it - row * G) * V;
+        const size_t off = (size_t)row * a.s + c0;
+        T acc[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = T(0);
+        T diag;
+        if constexpr (DescTraits<Desc>::kind == OP_CHAIN)
+            chain_row<T, V, HASQ>(d, tab, row, a.s, c0, a.q, acc, diag);
+        else
+            qsun_row<T, V, HASQ>(d, smem_t, row, a.s, c0, a.q, acc, diag);
+        Pack<T, V> res;
+#pragma unroll
+        for (int v = 0; v < V; ++v) res.v[v] = T(0);
+        if constexpr (HASX) {
+            const Pack<T, V> xo = ldp<T, V>(a.x + off);
+#pragma unroll
+            for (int v = 0; v < V; ++v) res.v[v] = a.cx * xo.v[v];
+        }
+        Pack<T, V> qo;
+        if constexpr (HASQ) {
+            qo = ldp<T, V>(a.q + off);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const T hq = (acc[v] + diag * qo.v[v]) * a.inva - a.boa * qo.v[v];
+                res.v[v] = res.v[v] + a.alpha * hq;
+            }
+        }
+        if constexpr (HASP) {
+            const Pack<T, V> po = ldp<T, V>(a.p + off);
+#pragma unroll
+            for (int v = 0; v < V; ++v) res.v[v] = res.v[v] + a.beta * po.v[v];
+        }
+        stp<T, V>(a.out + off, res);
+        if constexpr (DOTS) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                dd1[v] += (double)res.v[v] * (double)res.v[v];
+                if constexpr (HASQ) dd2[v] += (double)res.v[v] * (double)qo.v[v];
+            }
+        }
+    }
+
+    if constexpr (DOTS) {
+        // Every item of a thread has column group threadIdx.x % G (G divides the
+        // grid stride; checked on the host).  Lanes of one group are first
+        // summed with warp shuffles, then per warp in shared memory.
+        const int Gi = a.G;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (Gi < 32) {
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                for (int o = 16; o >= Gi; o >>= 1) {
+                    dd1[v] += __shfl_xor_sync(0xffffffffu, dd1[v], o);
+                    dd2[v] += __shfl_xor_sync(0xffffffffu, dd2[v], o);
+                }
+        }
+        const int lanes = Gi < 32 ? Gi : 32;
+        __syncthreads();
+        double *red = reinterpret_cast<double *>(smem_raw);  // [8 warps][lanes][2V]
+        if (lane < lanes)
+            for (int v = 0; v < V; ++v) {
+                red[(warp * lanes + lane) * 2 * V + v] = dd1[v];
+                red[(warp * lanes + lane) * 2 * V + V + v] = dd2[v];
+            }
+        __syncthreads();
+        double *bv = red + (kThreads / 32) * lanes * 2 * V;  // [2 s]
+        for (int c = threadIdx.x; c < a.s; c += blockDim.x) {
+            const int g = c / V, v = c - g * V;
+            double s1 = 0.0, s2 = 0.0;
+            if (Gi < 32) {
+                for (int w = 0; w < kThreads / 32; ++w) {
+                    s1 += red[(w * lanes + g) * 2 * V + v];
+                    s2 += red[(w * lanes + g) * 2 * V + V + v];
+                }
+            } else {
+                for (int t = g; t < kThreads; t += Gi) {
+                    const int w = t >> 5, l = t & 31;
+                    s1 += red[(w * lanes + l) * 2 * V + v];
+                    s2 += red[(w * lanes + l) * 2 * V + V + v];
+                }
+            }
+            bv[c] = s1;
+            bv[a.s + c] = s2;
+        }
+        __syncthreads();
+        finish_reduction(2 * a.s, bv, a.partials, a.counter, a.dots);
+    }
+}
+
+int grid_for(pf_handle *h, int64_t work_items, int threads, int blocks_per_sm) {
+    int64_t need = (work_items + threads - 1) / threads;
+    int64_t cap = (int64_t)h->num_sms * blocks_per_sm;
+    if (need < 1) need = 1;
+    return (int)std::min(need, cap);
+}
+
+void ensure_reduction(pf_handle *h, size_t n) {
+    if (h->red_partials_len >= n) return;
+    if (h->red_partials) cudaFree(h->red_partials);
+    h->red_partials = nullptr;
+    h->red_partials_len = 0;
+    PF_CUDA(cudaMalloc(&h->red_partials, n * sizeof(double)));
+    h->red_partials_len = n;
+    if (!h->red_counter) {
+        PF_CUDA(cudaMalloc(&h->red_counter, 64 * sizeof(unsigned int)));
+        PF_CUDA(cudaMemset(h->red_counter, 0, 64 * sizeof(unsigned int)));
+    }
+}
+
+// Resident CTAs per SM of a kernel instance (occupancy calculator, cached).
+static int blocks_per_sm(const void *kern, int smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(kern, smem);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int nb = 0;
+    PF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kThreads, smem));
+    if (nb < 1) nb = 1;
+    cache[key] = nb;
+    return nb;
+}
+
+template <typename T, int V, class Desc, int FLAGS>
+static void launch_one(pf_op *op, cudaStream_t st, const Desc &d, StepArgs<T> a, int smem) {
+    auto kern = k_step<T, V, Desc, FLAGS>;
+    if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    // one item per thread when the whole block fits on the device at once,
+    // otherwise a persistent grid of every resident CTA
+    const int grid = grid_for(op->h, a.items, kThreads, blocks_per_sm((const void *)kern, smem));
+    if constexpr ((FLAGS & StepFlags::DOTS) != 0) {
+        ensure_reduction(op->h, (size_t)grid * 2 * a.s);
+        a.partials = op->h->red_partials;
+        a.counter = op->h->red_counter;
+    }
+    kern<<<grid, kThreads, smem, st>>>(d, a);
+    PF_CUDA(cudaGetLastError());
+}
+
+template <typename T, int V, class Desc>
+static void dispatch_flags(pf_op *op, cudaStream_t st, const Desc &d, const StepArgs<T> &a,
+                           int flags, int smem) {
+    using F = StepFlags;
+    switch (flags) {
+        case F::X: launch_one<T, V, Desc, F::X>(op, st, d, a, smem); break;
+        case F::Q: launch_one<T, V, Desc, F::Q>(op, st, d, a, smem); break;
+        case F::Q | F::X: launch_one<T, V, Desc, F::Q | F::X>(op, st, d, a, smem); break;
+        case F::Q | F::P: launch_one<T, V, Desc, F::Q | F::P>(op, st, d, a, smem); break;
+        case F::Q | F::P | F::X: launch_one<T, V, Desc, F::Q | F::P | F::X>(op, st, d, a, smem); break;
+        case F::Q | F::DOTS: launch_one<T, V, Desc, F::Q | F::DOTS>(op, st, d, a, smem); break;
+        case F::Q | F::P | F::DOTS:
+            launch_one<T, V, Desc, F::Q | F::P | F::DOTS>(op, st, d, a, smem);
+            break;
+        default: throw Error(PF_ERR_INVALID, "unsupported step flag combination");
+    }
+}
+
+template <typename T>
+static const ChainDesc<T> &chain_of(pf_op *op);
+template <>
+const ChainDesc<double> &chain_of<double>(pf_op *op) { return op->chain64; }
+template <>
+const ChainDesc<float> &chain_of<float>(pf_op *op) { return op->chain32; }
+template <typename T>
+static const QSunDesc<T> &qsun_of(pf_op *op);
+template <>
+const QSunDesc<double> &qsun_of<double>(pf_op *op) { return op->qsun64; }
+template <>
+const QSunDesc<float> &qsun_of<float>(pf_op *op) { return op->qsun32; }
+
+template <typename T, int V>
+static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int flags) {
+    int smem = 0;
+    const int lanes = a.G < 32 ? a.G : 32;
+    const int dots_smem = (kThreads / 32) * lanes * 2 * V * 8 + 2 * a.s * 8;
+    if (op->kind == OP_CHAIN) {
+        const ChainDesc<T> &d = chain_of<T>(op);
+        if ((flags & StepFlags::Q) && !d.full) smem = rank_table_entries(d.nchunks) * 4;
+        if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
+        dispatch_flags<T, V>(op, st, d, a, flags, smem);
+    } else {
+        const QSunDesc<T> &d = qsun_of<T>(op);
+        smem = QSunSmem<T>::bytes(d.dg);
+        if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
+        dispatch_flags<T, V>(op, st, d, a, flags, smem);
+    }
+}
+
+// Columns per thread: the widest power of two dividing s within one 64-byte
+// run by default, or the width the autotuner measured fastest for (s, dtype).
+int default_width(int s, int elem_bytes) {
+    const int vmax = 64 / elem_bytes;
+    for (int w = vmax; w >= 1; w /= 2)
+        if (s % w == 0) return w;
+    return 1;
+}
+
+template <typename T>
+void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p, const T *x, T *out,
+                       double cx, double alpha, double beta, double inva, double shift, int flags, double *dots,
+                       int V) {
+    PF_CHECK(D == op->dim, PF_ERR_INVALID, "block height does not match the operator dimension");
+    PF_CHECK(s >= 1, PF_ERR_INVALID, "block must have at least one column");
+    PF_CHECK(V >= 1 && s % V == 0 && V * (int)sizeof(T) <= 64, PF_ERR_INVALID, "invalid columns-per-thread width");
+    StepArgs<T> a;
+    a.D = (uint32_t)D;
+    a.s = s;
+    a.G = s / V;
+    PF_CHECK((int64_t)D * a.G < (int64_t)0xffffffffLL, PF_ERR_UNSUPPORTED, "block too large for one launch");
+    a.items = (uint32_t)(D * a.G);
+    a.q = q; a.p = p; a.x = x; a.out = out;
+    a.cx = (T)cx; a.alpha = (T)alpha; a.beta = (T)beta;
+    a.inva = (T)inva; a.boa = (T)(shift * inva);
+    a.partials = nullptr; a.counter = nullptr; a.dots = dots;
+    if (flags & StepFlags::DOTS)
+        PF_CHECK(kThreads % a.G == 0, PF_ERR_UNSUPPORTED, "fused dots need s/V to divide 256");
+    switch (V) {
+        case 1: dispatch_op<T, 1>(op, st, a, flags); break;
+        case 2: dispatch_op<T, 2>(op, st, a, flags); break;
+        case 4: dispatch_op<T, 4>(op, st, a, flags); break;
+        case 8: dispatch_op<T, 8>(op, st, a, flags); break;
+        case 16:
+            if constexpr (sizeof(T) == 4) { dispatch_op<T, 16>(op, st, a, flags); break; }
+            [[fallthrough]];
+        default: throw Error(PF_ERR_INVALID, "bad vector width");
+    }
+}
+
+template <typename T>
+void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p,
+                 const T *x, T *out, double cx, double alpha, double beta, double inva,
+                 double shift, int flags, double *dots) {
+    int V = default_width(s, (int)sizeof(T));
+    {
+        std::lock_guard<std::mutex> lock(op->tune_mu);
+        auto it = op->tuned_width.find(std::make_pair((int)sizeof(T), s));
+        if (it != op->tuned_width.end()) V = it->second;
+    }
+    if ((flags & StepFlags::DOTS) && kThreads % (s / V) != 0) V = default_width(s, (int)sizeof(T));
+    launch_step_width<T>(op, st, D, s, q, p, x, out, cx, alpha, beta, inva, shift, flags, dots, V);
+}
+
+template void launch_step_width<double>(pf_op *, cudaStream_t, int64_t, int, const double *, const double *,
+                                        const double *, double *, double, double, double, double, double, int,
+                                        double *, int);
+template void launch_step_width<float>(pf_op *, cudaStream_t, int64_t, int, const float *, const float *,
+                                       const float *, float *, double, double, double, double, double, int,
+                                       double *, int);
+template void launch_step<double>(pf_op *, cudaStream_t, int64_t, int, const double *, const double *,
+                                  const double *, double *, double, double, double, double, double,
+                                  int, double *);
+template void launch_step<float>(pf_op *, cudaStream_t, int64_t, int, const float *, const float *,
+                                 const float *, float *, double, double, double, double, double,
+                                 int, double *);
+
+// --------------------------------------------------------- layout changes
+template <typename TS, typename TD>
+__global__ void k_cm_to_ri(uint32_t D, int s, const TS *__restrict__ src, int64_t ld, TD *__restrict__ dst) {
+    // tile 32 rows x 32 cols through shared memory
+    __shared__ TD tile[32][33];
+    const uint32_t r0 = blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k;
+        const uint32_t r = r0 + threadIdx.x;
+        if (c < s && r < D) tile[k][threadIdx.x] = (TD)src[(size_t)c * ld + r];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const uint32_t r = r0 + k;
+        const int c = c0 + threadIdx.x;
+        if (c < s && r < D) dst[(size_t)r * s + c] = tile[threadIdx.x][k];
+    }
+}
+
+template <typename TS, typename TD>
+__global__ void k_ri_to_cm(uint32_t D, int s, const TS *__restrict__ src, TD *__restrict__ dst, int64_t ld) {
+    __shared__ TD tile[32][33];
+    const uint32_t r0 = blockIdx.x * 32;
+    const int c0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const uint32_t r = r0 + k;
+        const int c = c0 + threadIdx.x;
+        if (c < s && r < D) tile[k][threadIdx.x] = (TD)src[(size_t)r * s + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+        const int c = c0 + k;
+        const uint32_t r = r0 + threadIdx.x;
+        if (c < s && r < D) dst[(size_t)c * ld + r] = tile[threadIdx.x][k];
+    }
+}
+
+template <typename TS, typename TD>
+void launch_cm_to_ri(cudaStream_t st, int64_t D, int s, const TS *src, int64_t ld, TD *dst) {
+    dim3 grid((unsigned)((D + 31) / 32), (unsigned)((s + 31) / 32));
+    k_cm_to_ri<TS, TD><<<grid, dim3(32, 8), 0, st>>>((uint32_t)D, s, src, ld, dst);
+    PF_CUDA(cudaGetLastError());
+}
+template <typename TS, typename TD>
+void launch_ri_to_cm(cudaStream_t st, int64_t D, int s, const TS *src, TD *dst, int64_t ld) {
+    dim3 grid((unsigned)((D + 31) / 32), (unsigned)((s + 31) / 32));
+    k_ri_to_cm<TS, TD><<<grid, dim3(32, 8), 0, st>>>((uint32_t)D, s, src, dst, ld);
+    PF_CUDA(cudaGetLastError());
+}
+template void launch_cm_to_ri<double, double>(cudaStream_t, int64_t, int, const double *, int64_t, double *);
+template void launch_cm_to_ri<float, float>(cudaStream_t, int64_t, int, const float *, int64_t, float *);
+template void launch_cm_to_ri<double, float>(cudaStream_t, int64_t, int, const double *, int64_t, float *);
+template void launch_ri_to_cm<double, double>(cudaStream_t, int64_t, int, const double *, double *, int64_t);
+template void launch_ri_to_cm<float, float>(cudaStream_t, int64_t, int, const float *, float *, int64_t);
+template void launch_ri_to_cm<float, double>(cudaStream_t, int64_t, int, const float *, double *, int64_t);
+template void launch_ri_to_cm<double, float>(cudaStream_t, int64_t, int, const double *, float *, int64_t);
+template void launch_cm_to_ri<float, double>(cudaStream_t, int64_t, int, const float *, int64_t, double *);
+
+// ------------------------------------------------------- column reductions
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_coldots(uint32_t D, int s, uint32_t rows_per_block,
+                                                     const T *__restrict__ A, const T *__restrict__ B,
+                                                     double *partials, unsigned int *counter, double *out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *bv = reinterpret_cast<double *>(smem_raw);
+    const uint32_t r0 = blockIdx.x * rows_per_block;
+    const uint32_t r1 = min(D, r0 + rows_per_block);
+    for (int c = threadIdx.x; c < s; c += blockDim.x) {
+        double acc = 0.0;
+        for (uint32_t r = r0; r < r1; ++r) acc += (double)A[(size_t)r * s + c] * (double)B[(size_t)r * s + c];
+        bv[c] = acc;
+    }
+    __syncthreads();
+    finish_reduction(s, bv, partials, counter, out);
+}
+
+__global__ void __launch_bounds__(kThreads) k_colresid(uint32_t D, int s, uint32_t rows_per_block,
+                                                      const double *__restrict__ HA, const double *__restrict__ A,
+                                                      const double *__restrict__ e, double *partials,
+                                                      unsigned int *counter, double *out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *bv = reinterpret_cast<double *>(smem_raw);
+    const uint32_t r0 = blockIdx.x * rows_per_block;
+    const uint32_t r1 = min(D, r0 + rows_per_block);
+    for (int c = threadIdx.x; c < s; c += blockDim.x) {
+        const double ec = e[c];
+        double acc = 0.0;
+        for (uint32_t r = r0; r < r1; ++r) {
+            const double d = HA[(size_t)r * s + c] - ec * A[(size_t)r * s + c];
+            acc += d * d;
+        }
+        bv[c] = acc;
+    }
+    __syncthreads();
+    finish_reduction(s, bv, partials, counter, out);
+}
+
+// For narrow blocks (s < 64) the per-column loops above leave most threads
+// idle; this variant gives each thread a strided set of rows of one column.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_coldots_narrow(uint32_t D, int s, const T *__restrict__ A,
+                                                            const T *__restrict__ B, double *partials,
+                                                            unsigned int *counter, double *out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *red = reinterpret_cast<double *>(smem_raw);  // [kThreads]
+    double *bv = red + kThreads;                          // [s]
+    // lanes of one row group: threads t with t % s == c handle column c
+    const int per = kThreads / s;  // row slots per block iteration
+    const int t = threadIdx.x;
+    double acc = 0.0;
+    if (t < per * s) {
+        const int c = t % s, slot = t / s;
+        for (uint32_t r = blockIdx.x * per + slot; r < D; r += gridDim.x * per)
+            acc += (double)A[(size_t)r * s + c] * (double)B[(size_t)r * s + c];
+    }
+    red[t] = acc;
+    __syncthreads();
+    for (int c = t; c < s; c += blockDim.x) {
+        double a = 0.0;
+        for (int q = c; q < per * s; q += s) a += red[q];
+        bv[c] = a;
+    }
+    __syncthreads();
+    finish_reduction(s, bv, partials, counter, out);
+}
+
+template <typename T>
+void launch_coldots(pf_handle *h, cudaStream_t st, int64_t D, int s, const T *A, const T *B, double *out) {
+    if (s < 64) {
+        int grid = grid_for(h, D * s, kThreads, 2);
+        ensure_reduction(h, (size_t)grid * s);
+        size_t smem = (kThreads + s) * sizeof(double);
+        k_coldots_narrow<T><<<grid, kThreads, smem, st>>>((uint32_t)D, s, A, B, h->red_partials,
+                                                          h->red_counter, out);
+    } else {
+        uint32_t rpb = 64;
+        int grid = (int)((D + rpb - 1) / rpb);
+        if (grid > 4 * h->num_sms) {
+            rpb = (uint32_t)((D + 4 * h->num_sms - 1) / (4 * h->num_sms));
+            grid = (int)((D + rpb - 1) / rpb);
+        }
+        ensure_reduction(h, (size_t)grid * s);
+        size_t smem = s * sizeof(double);
+        if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(k_coldots<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_coldots<T><<<grid, kThreads, smem, st>>>((uint32_t)D, s, rpb, A, B, h->red_partials,
+                                                   h->red_counter, out);
+    }
+    PF_CUDA(cudaGetLastError());
+}
+template void launch_coldots<double>(pf_handle *, cudaStream_t, int64_t, int, const double *, const double *, double *);
+template void launch_coldots<float>(pf_handle *, cudaStream_t, int64_t, int, const float *, const float *, double *);
+
+void launch_colresid(pf_handle *h, cudaStream_t st, int64_t D, int s, const double *HA, const double *A,
+                     const double *e, double *out) {
+    uint32_t rpb = 64;
+    int grid = (int)((D + rpb - 1) / rpb);
+    if (grid > 4 * h->num_sms) {
+        rpb = (uint32_t)((D + 4 * h->num_sms - 1) / (4 * h->num_sms));
+        grid = (int)((D + rpb - 1) / rpb);
+    }
+    ensure_reduction(h, (size_t)grid * s);
+    size_t smem = s * sizeof(double);
+    if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(k_colresid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_colresid<<<grid, kThreads, smem, st>>>((uint32_t)D, s, rpb, HA, A, e, h->red_partials, h->red_counter, out);
+    PF_CUDA(cudaGetLastError());
+}
+
+// --------------------------------------------------------------- probes
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    // splitmix64 finaliser (Steele, Lea, Flood 2014)
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+template <typename T>
+__global__ void k_probes(uint32_t D, int R, int kind, uint64_t seed, int col0, T *dst) {
+    const uint64_t n = (uint64_t)D * R;
+    for (uint64_t it = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; it < n;
+         it += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t row = it / R;
+        const int c = (int)(it - row * R);
+        const uint64_t key = ((uint64_t)(col0 + c) << 32) ^ row;
+        const uint64_t h1 = mix64(seed ^ mix64(key));
+        double val;
+        if (kind == PF_PROBE_RADEMACHER) {
+            val = (h1 & 1ull) ? 1.0 : -1.0;
+        } else {
+            // Box-Muller on two 53-bit uniforms in (0, 1]
+            const uint64_t h2 = mix64(h1 ^ 0xd1b54a32d192ed03ULL);
+            const double u1 = ((double)(h1 >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+            const double u2 = (double)(h2 >> 11) * (1.0 / 9007199254740992.0);
+            val = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        }
+        dst[it] = (T)val;
+    }
+}
+
+template <typename T>
+void launch_probes(cudaStream_t st, int64_t D, int R, int kind, uint64_t seed, int col0, T *dst) {
+    int grid = (int)std::min<int64_t>((D * R + 255) / 256, 148 * 8);
+    k_probes<T><<<grid, 256, 0, st>>>((uint32_t)D, R, kind, seed, col0, dst);
+    PF_CUDA(cudaGetLastError());
+}
+template void launch_probes<double>(cudaStream_t, int64_t, int, int, uint64_t, int, double *);
+template void launch_probes<float>(cudaStream_t, int64_t, int, int, uint64_t, int, float *);
+
+template <typename T>
+__global__ void k_scale_cols(uint32_t D, int s, T *A, const double *scale) {
+    const uint64_t n = (uint64_t)D * s;
+    for (uint64_t it = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; it < n;
+         it += (uint64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(it % s);
+        A[it] = (T)((double)A[it] * scale[c]);
+    }
+}
+template <typename T>
+void launch_scale_cols(cudaStream_t st, int64_t D, int s, T *A, const double *scale) {
+    int grid = (int)std::min<int64_t>((D * s + 255) / 256, 148 * 8);
+    k_scale_cols<T><<<grid, 256, 0, st>>>((uint32_t)D, s, A, scale);
+    PF_CUDA(cudaGetLastError());
+}
+template void launch_scale_cols<double>(cudaStream_t, int64_t, int, double *, const double *);
+template void launch_scale_cols<float>(cudaStream_t, int64_t, int, float *, const double *);
+
+// --------------------------------------------------------------- basis
+__global__ void k_unrank(uint64_t n, int full, uint32_t D, const uint32_t *states, const int64_t *idx,
+                         uint64_t *out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const int64_t k = idx[i];
+        if (k < 0 || (uint64_t)k >= D) out[i] = ~0ull;
+        else out[i] = full ? (uint64_t)k : (uint64_t)states[k];
+    }
+}
+
+__global__ void k_rank(uint64_t n, int L, int Lup, int full, int nchunks, const uint32_t *tab,
+                       const uint64_t *states, int64_t *out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t *t = reinterpret_cast<uint32_t *>(smem_raw);
+    if (!full) {
+        const int ne = rank_table_entries(nchunks);
+        for (int i = threadIdx.x; i < ne; i += blockDim.x) t[i] = tab[i];
+    }
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t st = states[i];
+        if ((L < 64 && (st >> L) != 0ull)) { out[i] = -1; continue; }
+        if (full) { out[i] = (int64_t)st; continue; }
+        if (__popcll(st) != Lup) { out[i] = -1; continue; }
+        out[i] = (int64_t)sector_rank((uint32_t)st, t, nchunks);
+    }
+}
+
+void launch_unrank(pf_op *op, cudaStream_t st, int64_t n, const int64_t *idx, uint64_t *out) {
+    if (n <= 0) return;
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    k_unrank<<<grid, 256, 0, st>>>((uint64_t)n, op->chain64.full, (uint32_t)op->dim, op->d_states, idx, out);
+    PF_CUDA(cudaGetLastError());
+}
+
+void launch_rank(pf_op *op, cudaStream_t st, int64_t n, const uint64_t *states, int64_t *out) {
+    if (n <= 0) return;
+    const ChainDesc<double> &d = op->chain64;
+    int smem = d.full ? 0 : rank_table_entries(d.nchunks) * 4;
+    if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(k_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 4);
+    k_rank<<<grid, 256, smem, st>>>((uint64_t)n, d.L, d.Lup, d.full, d.nchunks, op->d_rank_tab, states, out);
+    PF_CUDA(cudaGetLastError());
+}
+
+}  // namespace pf

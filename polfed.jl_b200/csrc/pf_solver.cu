@@ -1,0 +1,872 @@
+// pf_solver.cu -- POLFED driver on one B200: Clenshaw filter (graph-captured),
+// KPM moments, block Lanczos with full reorthogonalisation, Ritz extraction
+// and FP64 residuals.  Reference: Polfed.jl (see each function's citation).
+#include "pf_internal.h"
+#include "pf_solver.h"
+#include "pf_spectral.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace pf {
+
+// ------------------------------------------------------------- utilities
+template <typename T>
+struct DevArray {
+    T *p = nullptr;
+    size_t n = 0;
+    DevArray() = default;
+    explicit DevArray(size_t count) { alloc(count); }
+    void alloc(size_t count) {
+        free();
+        if (count) PF_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void free() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevArray() { free(); }
+    DevArray(const DevArray &) = delete;
+    DevArray &operator=(const DevArray &) = delete;
+};
+
+// Accumulates stage times measured with CUDA events on the solve's stream.
+// Events are never reused inside one solve, so a pending pair stays valid
+// until flush() reads it after the stream has passed both events.
+struct StageClock {
+    cudaStream_t st;
+    std::vector<cudaEvent_t> all;
+    struct Pending { int stage; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    double *acc;
+    StageClock(cudaStream_t s, double *acc_) : st(s), acc(acc_) {}
+    ~StageClock() {
+        for (auto e : all) cudaEventDestroy(e);
+    }
+    cudaEvent_t mark() {
+        cudaEvent_t e;
+        PF_CUDA(cudaEventCreate(&e));
+        all.push_back(e);
+        PF_CUDA(cudaEventRecord(e, st));
+        return e;
+    }
+    void add(int stage, cudaEvent_t a, cudaEvent_t b) { pending.push_back({stage, a, b}); }
+    void flush() {
+        for (auto &p : pending) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess && acc) acc[p.stage] += ms * 1e-3;
+        }
+        pending.clear();
+    }
+};
+
+static void sync(pf_handle *h) { PF_CUDA(cudaStreamSynchronize(h->stream)); }
+
+// ------------------------------------------------------------ the filter
+// Y = sum_k c_k T_k(Htilde) X on RI blocks (ClenshawAlgorithm.jl:12-29).
+// b_k is written in place over b_{k+2}, so two work blocks suffice.
+template <typename T>
+struct Filter {
+    pf_op *op;
+    int s, K;
+    std::vector<double> c;
+    double a, b;
+    DevArray<T> X, Y, A, B;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+
+    Filter(pf_op *op_, int s_, const std::vector<double> &coeffs, double a_, double b_)
+        : op(op_), s(s_), K((int)coeffs.size() - 1), c(coeffs), a(a_), b(b_) {
+        const size_t n = (size_t)op->dim * s;
+        X.alloc(n);
+        Y.alloc(n);
+        if (K >= 1) A.alloc(n);
+        if (K >= 2) B.alloc(n);
+    }
+    ~Filter() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+    void enqueue(cudaStream_t st) {
+        const int64_t D = op->dim;
+        const double inva = 1.0 / a;
+        using F = StepFlags;
+        if (K == 0) {
+            launch_step<T>(op, st, D, s, nullptr, nullptr, X.p, Y.p, c[0], 0, 0, inva, b, F::X, nullptr);
+            return;
+        }
+        launch_step<T>(op, st, D, s, nullptr, nullptr, X.p, A.p, c[K], 0, 0, inva, b, F::X, nullptr);
+        if (K >= 2)
+            launch_step<T>(op, st, D, s, A.p, nullptr, X.p, B.p, c[K - 1], 2.0, 0, inva, b, F::Q | F::X, nullptr);
+        for (int k = K - 2; k >= 1; --k) {
+            T *q = ((K - k - 1) % 2 == 0) ? A.p : B.p;  // b_{k+1}
+            T *o = ((K - k) % 2 == 0) ? A.p : B.p;      // b_{k+2}, overwritten by b_k
+            launch_step<T>(op, st, D, s, q, o, X.p, o, c[k], 2.0, -1.0, inva, b, F::Q | F::P | F::X, nullptr);
+        }
+        T *b1 = ((K - 1) % 2 == 0) ? A.p : B.p;
+        if (K == 1) {
+            launch_step<T>(op, st, D, s, b1, nullptr, X.p, Y.p, c[0], 1.0, 0, inva, b, F::Q | F::X, nullptr);
+        } else {
+            T *b2 = ((K - 2) % 2 == 0) ? A.p : B.p;
+            launch_step<T>(op, st, D, s, b1, b2, X.p, Y.p, c[0], 1.0, -1.0, inva, b, F::Q | F::P | F::X, nullptr);
+        }
+    }
+    // Capture the K+1 launches once; every later application is one graph launch.
+    void run(cudaStream_t st) {
+        if (!exec) {
+            PF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            try {
+                enqueue(st);
+            } catch (...) {
+                cudaGraph_t g;
+                cudaStreamEndCapture(st, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            PF_CUDA(cudaStreamEndCapture(st, &graph));
+            PF_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        }
+        PF_CUDA(cudaGraphLaunch(exec, st));
+    }
+};
+
+// ------------------------------------------------------------- the KPM
+// mu_n = (D/R) sum_r <r|T_n(Htilde)|r>  (Moments.jl:42-140) evaluated with
+// the doubling identities mu_{2n} = 2<v_n,v_n> - mu_0 and
+// mu_{2n+1} = 2<v_{n+1},v_n> - mu_1 per probe (Weisse et al., Rev. Mod. Phys.
+// 78, 275 (2006)), i.e. ceil((N-1)/2) block steps instead of N-1, with the
+// dot products fused into the step kernel.  Probes are processed in
+// power-of-two column blocks of at most 64.
+template <typename T>
+static std::vector<double> kpm_moments(pf_op *op, double a, double b, int N, int R, const T *probes_cm,
+                                       int64_t ldp, int kind, uint64_t seed, int64_t *block_matvecs) {
+    pf_handle *h = op->h;
+    const int64_t D = op->dim;
+    cudaStream_t st = h->stream;
+    PF_CHECK(N >= 1 && R >= 1, PF_ERR_INVALID, "KPM needs N >= 1 and R >= 1");
+    std::vector<double> mu(N, 0.0);
+    const int M = (N - 1 + 1) / 2;  // steps: ceil((N-1)/2)
+    const int RB = std::min(64, R);
+    DevArray<T> v0((size_t)D * RB), v1((size_t)D * RB);
+    DevArray<double> dots((size_t)std::max(M, 1) * 2 * RB), n0(RB), scl(RB);
+    std::vector<double> hd((size_t)std::max(M, 1) * 2 * RB), h0(RB), hs(RB);
+    int64_t mv = 0;
+    int c0 = 0;
+    while (c0 < R) {
+        int nb = 64;
+        while (nb > R - c0) nb /= 2;
+        T *prev = v0.p, *cur = v1.p;
+        if (probes_cm) {
+            launch_cm_to_ri<T, T>(st, D, nb, probes_cm + (size_t)c0 * ldp, ldp, prev);
+        } else {
+            launch_probes<T>(st, D, nb, kind, seed, c0, prev);
+            launch_coldots<T>(h, st, D, nb, prev, prev, n0.p);
+            PF_CUDA(cudaMemcpyAsync(h0.data(), n0.p, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+            sync(h);
+            for (int c = 0; c < nb; ++c) hs[c] = 1.0 / std::sqrt(h0[c]);
+            PF_CUDA(cudaMemcpyAsync(scl.p, hs.data(), nb * sizeof(double), cudaMemcpyHostToDevice, st));
+            launch_scale_cols<T>(st, D, nb, prev, scl.p);
+        }
+        launch_coldots<T>(h, st, D, nb, prev, prev, n0.p);
+        if (M >= 1) {
+            launch_step<T>(op, st, D, nb, prev, nullptr, nullptr, cur, 0, 1.0, 0, 1.0 / a, b,
+                           StepFlags::Q | StepFlags::DOTS, dots.p);
+            for (int n = 1; n < M; ++n) {
+                launch_step<T>(op, st, D, nb, cur, prev, nullptr, prev, 0, 2.0, -1.0, 1.0 / a, b,
+                               StepFlags::Q | StepFlags::P | StepFlags::DOTS, dots.p + (size_t)n * 2 * nb);
+                std::swap(prev, cur);
+            }
+        }
+        PF_CUDA(cudaMemcpyAsync(h0.data(), n0.p, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (M >= 1)
+            PF_CUDA(cudaMemcpyAsync(hd.data(), dots.p, (size_t)M * 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync(h);
+        for (int c = 0; c < nb; ++c) {
+            const double m0 = h0[c];
+            mu[0] += m0;
+            if (M < 1) continue;
+            const double m1 = hd[nb + c];  // <v1, v0>
+            if (N > 1) mu[1] += m1;
+            for (int n = 0; n < M; ++n) {
+                const double dd = hd[(size_t)n * 2 * nb + c];
+                const double dq = hd[(size_t)n * 2 * nb + nb + c];
+                if (2 * n + 2 < N) mu[2 * n + 2] += 2.0 * dd - m0;
+                if (n >= 1 && 2 * n + 1 < N) mu[2 * n + 1] += 2.0 * dq - m1;
+            }
+        }
+        mv += (int64_t)nb * M;
+        c0 += nb;
+    }
+    for (double &m : mu) m *= (double)D / (double)R;
+    if (block_matvecs) *block_matvecs += mv;
+    return mu;
+}
+
+// ----------------------------------------------------- small dense helpers
+// Cholesky G = R^T R (upper R, column-major s x s).  Returns false on a
+// non-positive or negligible pivot.
+static bool host_cholesky(const std::vector<double> &G, int s, std::vector<double> &R) {
+    R.assign((size_t)s * s, 0.0);
+    for (int j = 0; j < s; ++j) {
+        double d = G[j + j * s];
+        for (int k = 0; k < j; ++k) d -= R[k + j * s] * R[k + j * s];
+        if (!(d > 1e-28 * std::max(1.0, std::fabs(G[j + j * s]))) || !std::isfinite(d)) return false;
+        if (d <= 1e-13 * std::fabs(G[j + j * s])) return false;
+        const double rjj = std::sqrt(d);
+        R[j + j * s] = rjj;
+        for (int i = j + 1; i < s; ++i) {
+            double v = G[j + i * s];
+            for (int k = 0; k < j; ++k) v -= R[k + j * s] * R[k + i * s];
+            R[j + i * s] = v / rjj;
+        }
+    }
+    return true;
+}
+
+// Householder QR of an RI (row-major) D x s block on the host, with the LAPACK
+// sign convention (R_jj = -sign(a_jj) ||x||).  Q overwrites A; R is s x s
+// column-major.  Used only when CholQR breaks down (a rank-deficient block).
+static void host_householder_qr(std::vector<double> &A, int64_t D, int s, std::vector<double> &R) {
+    std::vector<std::vector<double>> V(s);
+    std::vector<double> tau(s, 0.0);
+    for (int j = 0; j < s; ++j) {
+        double nrm2 = 0.0;
+        for (int64_t i = j; i < D; ++i) nrm2 += A[i * s + j] * A[i * s + j];
+        const double alpha = A[j * s + j];
+        const double nrm = std::sqrt(nrm2);
+        std::vector<double> v(D - j, 0.0);
+        if (nrm == 0.0) {
+            tau[j] = 0.0;
+            V[j] = v;
+            continue;
+        }
+        const double beta = -std::copysign(nrm, alpha);
+        v[0] = 1.0;
+        for (int64_t i = j + 1; i < D; ++i) v[i - j] = A[i * s + j] / (alpha - beta);
+        tau[j] = (beta - alpha) / beta;
+        for (int c = j; c < s; ++c) {
+            double w = 0.0;
+            for (int64_t i = j; i < D; ++i) w += v[i - j] * A[i * s + c];
+            w *= tau[j];
+            for (int64_t i = j; i < D; ++i) A[i * s + c] -= w * v[i - j];
+        }
+        V[j] = v;
+    }
+    R.assign((size_t)s * s, 0.0);
+    for (int j = 0; j < s; ++j)
+        for (int i = 0; i <= j; ++i) R[i + j * s] = A[(int64_t)i * s + j];
+    std::vector<double> Q((size_t)D * s, 0.0);
+    for (int j = 0; j < s; ++j) Q[(int64_t)j * s + j] = 1.0;
+    for (int j = s - 1; j >= 0; --j) {
+        if (tau[j] == 0.0) continue;
+        for (int c = 0; c < s; ++c) {
+            double w = 0.0;
+            for (int64_t i = j; i < D; ++i) w += V[j][i - j] * Q[i * s + c];
+            w *= tau[j];
+            for (int64_t i = j; i < D; ++i) Q[i * s + c] -= w * V[j][i - j];
+        }
+    }
+    A.swap(Q);
+}
+
+// ---------------------------------------------------------- block Lanczos
+// Lanczos.jl:119-143, LanczosMethod.jl:55-83, LanczosAlgorithm.jl:11-54,
+// Factorization/*, Convergence/* on RI blocks in FP64.  The basis is a
+// row-major D x maxdim array; cuBLAS sees it as its column-major transpose.
+struct LanczosOut {
+    std::vector<double> vals;      // ascending, nconv entries
+    DevArray<double> vecs;          // RI D x nconv, same order
+    int nconv = 0;
+    int numiter = 0, maxiter = 0, krylovdim = 0;
+    int converged = 0, eigenconverged = 0;
+    double residual = 1.0, eigenresidual = 1.0;
+    int numofchecks = 0;
+    std::vector<int> conv_hist, dim_hist;
+    std::vector<double> res_hist;
+};
+
+using BlockMap = std::function<void(const double *X, double *Y)>;  // RI D x s, on h->stream
+
+static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
+                    int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
+                    double *stage_acc) {
+    pf_handle *h = op->h;
+    const int64_t D = op->dim;
+    cudaStream_t st = h->stream;
+    cublasHandle_t blas = h->blas;
+    PF_CUBLAS(cublasSetStream(blas, st));
+    PF_CUSOLVER(cusolverDnSetStream(h->solver, st));
+
+    const int maxiter = (maxdim_req + s - 1) / s;
+    const int maxdim = maxiter * s;
+    PF_CHECK(maxdim >= 1, PF_ERR_INVALID, "maxdim must be positive");
+    out.maxiter = maxiter;
+    int nextcheck = std::max(howmany / s + 1, 2);
+
+    DevArray<double> basis((size_t)D * maxdim);
+    DevArray<double> bufs((size_t)D * s * 3);
+    double *vlast = bufs.p, *vprev = bufs.p + (size_t)D * s, *r = bufs.p + 2 * (size_t)D * s;
+    DevArray<double> smallA((size_t)s * s), smallB((size_t)s * s), G((size_t)maxdim * s);
+    std::vector<double> T((size_t)maxdim * maxdim, 0.0);  // column-major
+    std::vector<double> hA((size_t)s * s), hR, hR1, hR2, beta_last((size_t)s * s, 0.0);
+    const double one = 1.0, zero = 0.0, mone = -1.0;
+    const int ldb = maxdim;  // row stride of the basis
+    StageClock clk(st, stage_acc);
+
+    auto append = [&](const double *src, int col) {
+        PF_CUDA(cudaMemcpy2DAsync(basis.p + col, (size_t)ldb * sizeof(double), src, (size_t)s * sizeof(double),
+                                  (size_t)s * sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
+    };
+    // alpha = V^T W (s x s, column-major) -> host, upper-triangle symmetrised
+    auto overlap = [&](const double *Vb, const double *Wb) {
+        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, Vb, s, Wb, s, &zero, smallA.p, s));
+        PF_CUDA(cudaMemcpyAsync(hA.data(), smallA.p, (size_t)s * s * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync(h);
+        for (int j = 0; j < s; ++j)
+            for (int i = j + 1; i < s; ++i) hA[i + j * s] = hA[j + i * s];  // Hermitian(alpha): upper
+    };
+    // Q R = W in place (CholQR2; Householder on the host if it breaks down)
+    auto qr_inplace = [&](double *W, std::vector<double> &Rout) {
+        std::vector<double> Rtot((size_t)s * s, 0.0);
+        for (int i = 0; i < s; ++i) Rtot[i + i * s] = 1.0;
+        bool ok = true;
+        for (int pass = 0; pass < 2 && ok; ++pass) {
+            PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, smallA.p, s));
+            std::vector<double> hG((size_t)s * s), Rp;
+            PF_CUDA(cudaMemcpyAsync(hG.data(), smallA.p, (size_t)s * s * sizeof(double), cudaMemcpyDeviceToHost, st));
+            sync(h);
+            for (int j = 0; j < s; ++j)
+                for (int i = j + 1; i < s; ++i) hG[i + j * s] = hG[j + i * s];
+            if (!host_cholesky(hG, s, Rp)) { ok = false; break; }
+            PF_CUDA(cudaMemcpyAsync(smallB.p, Rp.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
+            // W^T <- R^{-T} W^T  (i.e. W <- W R^{-1})
+            PF_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, s,
+                                  (int)D, &one, smallB.p, s, W, s));
+            // Rtot <- Rp * Rtot
+            std::vector<double> Rn((size_t)s * s, 0.0);
+            for (int j = 0; j < s; ++j)
+                for (int i = 0; i <= j; ++i) {
+                    double v = 0.0;
+                    for (int k = i; k <= j; ++k) v += Rp[i + k * s] * Rtot[k + j * s];
+                    Rn[i + j * s] = v;
+                }
+            Rtot.swap(Rn);
+        }
+        if (!ok) {
+            std::vector<double> hW((size_t)D * s);
+            PF_CUDA(cudaMemcpyAsync(hW.data(), W, hW.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+            sync(h);
+            host_householder_qr(hW, D, s, Rtot);
+            PF_CUDA(cudaMemcpyAsync(W, hW.data(), hW.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        Rout.swap(Rtot);
+    };
+
+    // ---- lanczositer (Factorization.jl:50-67)
+    PF_CUDA(cudaMemcpyAsync(vlast, x0_ri, (size_t)D * s * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    PF_CUDA(cudaMemsetAsync(vprev, 0, (size_t)D * s * sizeof(double), st));
+    append(vlast, 0);
+    int k = s;
+    {
+        cudaEvent_t e0 = clk.mark();
+        fmap(vlast, r);
+        clk.add(1, e0, clk.mark());
+    }
+    overlap(vlast, r);
+    for (int j = 0; j < s; ++j)
+        for (int i = 0; i < s; ++i) T[(size_t)i + (size_t)j * maxdim] = hA[i + j * s];
+    PF_CUDA(cudaMemcpyAsync(smallA.p, hA.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
+    // r^T -= alpha^T x0^T
+    PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, smallA.p, s, vlast, s, &one, r, s));
+    int numiter = 1;
+
+    // eigen workspace
+    DevArray<double> dT((size_t)maxdim * maxdim), dW(maxdim);
+    DevArray<int> dinfo(1);
+    int lwork = 0;
+    PF_CUSOLVER(cusolverDnDsyevd_bufferSize(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, maxdim, dT.p,
+                                            maxdim, dW.p, &lwork));
+    DevArray<double> dwork((size_t)std::max(lwork, 1));
+
+    out.converged = 0;
+    out.eigenconverged = 0;
+    while (true) {
+        // 1 tridiagonalization: QR(r) -> beta (BlockLanczosFactorization.jl:115-131)
+        cudaEvent_t e0 = clk.mark();
+        qr_inplace(r, hR);
+        clk.flush();
+        for (int j = 0; j < s; ++j)
+            for (int i = 0; i < s; ++i) {
+                T[(size_t)(k + i) + (size_t)(k - s + j) * maxdim] = hR[i + j * s];
+                T[(size_t)(k - s + j) + (size_t)(k + i) * maxdim] = hR[i + j * s];
+            }
+        beta_last = hR;
+        std::swap(vprev, vlast);
+        std::swap(vlast, r);  // vlast <- Q ; r <- old vprev storage
+        append(vlast, k);
+        k += s;
+        cudaEvent_t e1 = clk.mark();
+        clk.add(0, e0, e1);
+        // 2 mapping
+        fmap(vlast, r);
+        cudaEvent_t e2 = clk.mark();
+        clk.add(1, e1, e2);
+        // 3 overlap
+        overlap(vlast, r);
+        for (int j = 0; j < s; ++j)
+            for (int i = 0; i < s; ++i) T[(size_t)(k - s + i) + (size_t)(k - s + j) * maxdim] = hA[i + j * s];
+        cudaEvent_t e3 = clk.mark();
+        clk.add(2, e2, e3);
+        // 4 orthogonalization: r -= vlast alpha + vprev beta^T  (orthogonalization.jl:31-33)
+        PF_CUDA(cudaMemcpyAsync(smallA.p, hA.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
+        PF_CUDA(cudaMemcpyAsync(smallB.p, beta_last.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
+        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, smallA.p, s, vlast, s, &one, r, s));
+        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, s, (int)D, s, &mone, smallB.p, s, vprev, s, &one, r, s));
+        cudaEvent_t e4 = clk.mark();
+        clk.add(3, e3, e4);
+        // 5 reorthogonalization: r -= B (B^T r), B = all but the last two blocks
+        const int nB = k - 2 * s;
+        if (nB > 0) {
+            for (int pass = 0; pass < reorth_passes; ++pass) {
+                PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, nB, s, (int)D, &one, basis.p, ldb, r, s, &zero,
+                                      G.p, nB));
+                PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, nB, &mone, G.p, nB, basis.p, ldb, &one,
+                                      r, s));
+            }
+        }
+        cudaEvent_t e5 = clk.mark();
+        clk.add(4, e4, e5);
+
+        // convergence (ConvergenceInfo.jl:63-130)
+        numiter += 1;
+        if (nextcheck == numiter || numiter >= maxiter) {
+            // projected matrix, upper triangle is authoritative (Hermitian view)
+            std::vector<double> Tk((size_t)k * k);
+            for (int j = 0; j < k; ++j)
+                for (int i = 0; i < k; ++i) {
+                    const int a = std::min(i, j), b2 = std::max(i, j);
+                    Tk[(size_t)i + (size_t)j * k] = T[(size_t)a + (size_t)b2 * maxdim];
+                }
+            PF_CUDA(cudaMemcpyAsync(dT.p, Tk.data(), Tk.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            PF_CUSOLVER(cusolverDnDsyevd(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, dT.p, k, dW.p,
+                                         dwork.p, lwork, dinfo.p));
+            std::vector<double> lam(k), tail((size_t)s * k);
+            int info = 0;
+            PF_CUDA(cudaMemcpyAsync(lam.data(), dW.p, k * sizeof(double), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpy2DAsync(tail.data(), s * sizeof(double), dT.p + (k - s), (size_t)k * sizeof(double),
+                                      s * sizeof(double), k, cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(&info, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            sync(h);
+            PF_CHECK(info == 0, PF_ERR_NUMERIC, "projected eigenproblem failed to converge");
+            std::vector<int> idx(k);
+            std::iota(idx.begin(), idx.end(), 0);
+            if (which == PF_WHICH_LR)
+                std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] > lam[y]; });
+            else
+                std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] < lam[y]; });
+            int conv = 0;
+            double maxres = 0.0;
+            const int nwant = std::min(howmany, k);
+            for (int i = 0; i < nwant; ++i) {
+                const int pos = idx[i];
+                double ss = 0.0;
+                for (int a = 0; a < s; ++a) {
+                    double v = 0.0;
+                    for (int b2 = 0; b2 < s; ++b2) v += beta_last[a + b2 * s] * tail[b2 + (size_t)pos * s];
+                    ss += v * v;
+                }
+                const double res = std::sqrt(ss);
+                if (res > maxres || std::isnan(res)) maxres = std::isnan(res) ? res : std::max(maxres, res);
+                if (maxres < tol) ++conv;
+            }
+            out.numofchecks += 1;
+            out.converged = conv;
+            out.residual = maxres;
+            out.conv_hist.push_back(conv);
+            out.dim_hist.push_back(k);
+            out.res_hist.push_back(maxres);
+            if (conv == howmany || numiter >= maxiter) {
+                // calculate_eigenvectors! (getvecs.jl:10-21): Psi = B Phi[:, idx[1:conv]]
+                out.vecs.alloc((size_t)D * std::max(conv, 1));
+                if (conv > 0) {
+                    DevArray<double> phisel((size_t)k * conv);
+                    for (int i = 0; i < conv; ++i)
+                        PF_CUDA(cudaMemcpyAsync(phisel.p + (size_t)i * k, dT.p + (size_t)idx[i] * k, k * sizeof(double),
+                                                cudaMemcpyDeviceToDevice, st));
+                    PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, conv, (int)D, k, &one, phisel.p, k, basis.p, ldb,
+                                          &zero, out.vecs.p, conv));
+                    // calculate_eigenvalues! / calculate_eigenresiduals! with the ORIGINAL H
+                    DevArray<double> HV((size_t)D * conv), E(conv), res2(conv);
+                    launch_step<double>(op, st, D, conv, out.vecs.p, nullptr, nullptr, HV.p, 0, 1.0, 0, 1.0, 0.0,
+                                        StepFlags::Q, nullptr);
+                    launch_coldots<double>(h, st, D, conv, out.vecs.p, HV.p, E.p);
+                    launch_colresid(h, st, D, conv, HV.p, out.vecs.p, E.p, res2.p);
+                    std::vector<double> hE(conv), hr(conv);
+                    PF_CUDA(cudaMemcpyAsync(hE.data(), E.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
+                    PF_CUDA(cudaMemcpyAsync(hr.data(), res2.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
+                    sync(h);
+                    int ec = 0;
+                    bool counting = true;
+                    double maxe = 0.0;
+                    for (int i = 0; i < conv; ++i) {
+                        const double rr = std::sqrt(std::max(hr[i], 0.0));
+                        if (counting && rr < eigentol) ++ec;
+                        else counting = false;
+                        maxe = std::max(maxe, rr);
+                    }
+                    out.vals = hE;
+                    out.eigenconverged = ec;
+                    out.eigenresidual = maxe;
+                } else {
+                    out.vals.clear();
+                    out.eigenconverged = 0;
+                    out.eigenresidual = 0.0;
+                }
+            }
+            // next_checking! (NextChecking.jl:23-42)
+            if (out.residual > 1e-2) nextcheck = numiter + 20;
+            else if (out.residual > 1e-3) nextcheck = numiter + 10;
+            else nextcheck = numiter + 5;
+            cudaEvent_t e6 = clk.mark();
+            clk.add(5, e5, e6);
+        }
+        if (out.converged == howmany || numiter >= maxiter) break;
+    }
+    sync(h);
+    clk.flush();
+    out.numiter = numiter;
+    out.krylovdim = k;
+    // LanczosMethod.jl:74-82: keep the converged prefix, ascending order
+    const int nconv = std::min(out.converged, out.eigenconverged);
+    std::vector<int> ord(nconv);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return out.vals[x] < out.vals[y]; });
+    std::vector<double> sv(nconv);
+    for (int i = 0; i < nconv; ++i) sv[i] = out.vals[ord[i]];
+    if (nconv > 0) {
+        const int cw = (int)(out.vecs.n / (size_t)D);  // columns of the RI vecs block
+        DevArray<double> perm((size_t)D * nconv);
+        for (int i = 0; i < nconv; ++i)
+            PF_CUDA(cudaMemcpy2DAsync(perm.p + i, nconv * sizeof(double), out.vecs.p + ord[i], cw * sizeof(double),
+                                      sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
+        sync(h);
+        std::swap(out.vecs.p, perm.p);
+        std::swap(out.vecs.n, perm.n);
+    }
+    out.vals = sv;
+    out.nconv = nconv;
+}
+
+// ------------------------------------------------------------- extrema
+// Emin / Emax by two scalar Lanczos probes on H (Plan.jl:136-168,
+// Lanczos.jl:183-212): which = :SR then :LR, howmany 1, tol 1e-14,
+// eigentol 1e-8 (the lanczos() defaults), mapvals = H.
+static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, double tol, double eigentol, double *Emin,
+                                double *Emax, double *stage_acc) {
+    const int64_t D = op->dim;
+    BlockMap happly = [&](const double *X, double *Y) {
+        launch_step<double>(op, op->h->stream, D, 1, X, nullptr, nullptr, Y, 0, 1.0, 0, 1.0, 0.0, StepFlags::Q, nullptr);
+    };
+    double dummy[10] = {0};
+    for (int w = 0; w < 2; ++w) {
+        LanczosOut o;
+        lanczos(op, 1, 1, maxdim, tol, eigentol, w == 0 ? PF_WHICH_SR : PF_WHICH_LR, 1, v0_dev, happly, o,
+                stage_acc ? dummy : nullptr);
+        PF_CHECK(o.nconv >= 1, PF_ERR_NUMERIC, "Failed to estimate extremal eigenvalue with Lanczos.");
+        if (w == 0) *Emin = o.vals.front();
+        else *Emax = o.vals.back();
+    }
+}
+
+void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, double eigentol, double *Emin,
+                     double *Emax) {
+    PF_CHECK(x0_host && Emin && Emax, PF_ERR_INVALID, "null argument");
+    const int64_t D = op->dim;
+    std::vector<double> seed(x0_host, x0_host + D);
+    double nrm = 0.0;
+    for (double v : seed) nrm += v * v;
+    nrm = std::sqrt(nrm);
+    PF_CHECK(nrm > 0 && std::isfinite(nrm), PF_ERR_INVALID, "lanczos_extrema requires a nonzero starting vector.");
+    for (double &v : seed) v /= nrm;
+    PF_CUDA(cudaSetDevice(op->h->device));
+    DevArray<double> v0(D);
+    PF_CUDA(cudaMemcpyAsync(v0.p, seed.data(), D * sizeof(double), cudaMemcpyHostToDevice, op->h->stream));
+    extrema_from_device(op, v0.p, maxdim, tol, eigentol, Emin, Emax, nullptr);
+}
+
+// ------------------------------------------------------- op-level filter
+void op_filter(pf_op *op, int dtype, double a, double b, int K, const double *coeffs, int s, const void *X,
+               int64_t ldx, void *Y, int64_t ldy) {
+    PF_CHECK(coeffs && X && Y && K >= 0 && s >= 1, PF_ERR_INVALID, "invalid filter arguments");
+    PF_CHECK(ldx >= op->dim && ldy >= op->dim, PF_ERR_INVALID, "leading dimension smaller than D");
+    PF_CHECK(a != 0.0 && std::isfinite(a) && std::isfinite(b), PF_ERR_INVALID, "rescaling a must be finite and nonzero");
+    PF_CUDA(cudaSetDevice(op->h->device));
+    std::vector<double> c(coeffs, coeffs + K + 1);
+    cudaStream_t st = op->h->stream;
+    const int64_t D = op->dim;
+    if (dtype == PF_F64) {
+        Filter<double> f(op, s, c, a, b);
+        launch_cm_to_ri<double, double>(st, D, s, (const double *)X, ldx, f.X.p);
+        f.enqueue(st);
+        launch_ri_to_cm<double, double>(st, D, s, f.Y.p, (double *)Y, ldy);
+        sync(op->h);
+    } else if (dtype == PF_F32) {
+        Filter<float> f(op, s, c, a, b);
+        launch_cm_to_ri<float, float>(st, D, s, (const float *)X, ldx, f.X.p);
+        f.enqueue(st);
+        launch_ri_to_cm<float, float>(st, D, s, f.Y.p, (float *)Y, ldy);
+        sync(op->h);
+    } else throw Error(PF_ERR_INVALID, "dtype must be PF_F64 or PF_F32");
+}
+
+void op_kpm(pf_op *op, int dtype, double a, double b, int N, int R, const void *probes, int64_t ldp, int probe_kind,
+            uint64_t seed, double *mu) {
+    PF_CHECK(mu && N >= 1 && R >= 1, PF_ERR_INVALID, "invalid KPM arguments");
+    PF_CHECK(!probes || ldp >= op->dim, PF_ERR_INVALID, "probe leading dimension smaller than D");
+    PF_CHECK(a != 0.0 && std::isfinite(a) && std::isfinite(b), PF_ERR_INVALID, "rescaling a must be finite and nonzero");
+    PF_CHECK(probe_kind == PF_PROBE_GAUSSIAN || probe_kind == PF_PROBE_RADEMACHER, PF_ERR_INVALID, "unknown probe kind");
+    PF_CUDA(cudaSetDevice(op->h->device));
+    std::vector<double> m;
+    if (dtype == PF_F64) m = kpm_moments<double>(op, a, b, N, R, (const double *)probes, ldp, probe_kind, seed, nullptr);
+    else if (dtype == PF_F32) m = kpm_moments<float>(op, a, b, N, R, (const float *)probes, ldp, probe_kind, seed, nullptr);
+    else throw Error(PF_ERR_INVALID, "dtype must be PF_F64 or PF_F32");
+    std::copy(m.begin(), m.end(), mu);
+}
+
+// ------------------------------------------------------------- the solve
+static int64_t expected_krylov_dim(int howmany, int s, double eta) {
+    return (int64_t)std::ceil((20.427 * s + 1.696 * howmany) * eta);  // PolfedDefaults.jl:61-62
+}
+
+// _prepare_polfed_initial_state (PolfedCore.jl:43-95) on a host D x s column-major copy.
+static void prepare_initial_state(std::vector<double> &x, int64_t D, int s) {
+    const double tol = std::max(1e-10, 10 * 2.220446049250313e-16);
+    for (double v : x) PF_CHECK(std::isfinite(v), PF_ERR_INVALID, "POLFED initial state must contain finite values.");
+    if (s == 1) {
+        double nrm = 0.0;
+        for (double v : x) nrm += v * v;
+        nrm = std::sqrt(nrm);
+        PF_CHECK(nrm != 0.0, PF_ERR_INVALID, "POLFED initial vector must be nonzero.");
+        if (std::fabs(nrm - 1.0) <= std::max(tol, tol * std::max(nrm, 1.0))) return;
+        for (double &v : x) v /= nrm;
+        return;
+    }
+    PF_CHECK(s <= D, PF_ERR_INVALID,
+             "POLFED initial matrix cannot have orthonormal columns when it has more columns than rows.");
+    std::vector<double> G((size_t)s * s, 0.0);
+    for (int i = 0; i < s; ++i)
+        for (int j = 0; j < s; ++j) {
+            double v = 0.0;
+            for (int64_t r = 0; r < D; ++r) v += x[r + i * D] * x[r + j * D];
+            G[i + j * s] = v;
+        }
+    double dn = 0.0, gn = 0.0;
+    for (int i = 0; i < s; ++i)
+        for (int j = 0; j < s; ++j) {
+            const double e = G[i + j * s] - (i == j ? 1.0 : 0.0);
+            dn += e * e;
+            gn += G[i + j * s] * G[i + j * s];
+        }
+    if (std::sqrt(dn) <= std::max(tol, tol * std::max(std::sqrt(gn), std::sqrt((double)s)))) return;
+    // orthonormalised copy: thin Q of a Householder QR (as Matrix(qr(x0).Q)[:, 1:s])
+    std::vector<double> A((size_t)D * s);
+    for (int64_t r = 0; r < D; ++r)
+        for (int c = 0; c < s; ++c) A[r * s + c] = x[r + c * D];
+    std::vector<double> R;
+    host_householder_qr(A, D, s, R);
+    for (int64_t r = 0; r < D; ++r)
+        for (int c = 0; c < s; ++c) x[r + c * D] = A[r * s + c];
+}
+
+void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int x0_mem, double *vals, double *vecs,
+           int vecs_mem, pf_report *rep, int *nconv) {
+    PF_CHECK(op && P && x0 && vals && nconv, PF_ERR_INVALID, "null argument");
+    PF_CHECK(s >= 1 && nev >= 1, PF_ERR_INVALID, "s and nev must be positive");
+    PF_CHECK(P->precision == PF_PREC_FP64 || P->precision == PF_PREC_MIXED, PF_ERR_INVALID, "unknown precision");
+    PF_CHECK(P->reorth_passes >= 1 && P->reorth_passes <= 2, PF_ERR_INVALID, "reorth_passes must be 1 or 2");
+    pf_handle *h = op->h;
+    PF_CUDA(cudaSetDevice(h->device));
+    cudaStream_t st = h->stream;
+    const int64_t D = op->dim;
+    PF_CHECK(s <= D, PF_ERR_INVALID,
+             "POLFED initial matrix cannot have orthonormal columns when it has more columns than rows.");
+    pf_report R;
+    std::memset(&R, 0, sizeof(R));
+    cudaEvent_t t_begin, t_end;
+    PF_CUDA(cudaEventCreate(&t_begin));
+    PF_CUDA(cudaEventCreate(&t_end));
+    PF_CUDA(cudaEventRecord(t_begin, st));
+    auto t_wall0 = std::chrono::steady_clock::now();
+
+    // x0 -> host column-major, validate / orthonormalise, -> device RI
+    std::vector<double> hx((size_t)D * s);
+    if (x0_mem == PF_MEM_DEVICE)
+        PF_CUDA(cudaMemcpy(hx.data(), x0, hx.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    else std::memcpy(hx.data(), x0, hx.size() * sizeof(double));
+    prepare_initial_state(hx, D, s);
+    DevArray<double> xcm((size_t)D * s), xri((size_t)D * s);
+    PF_CUDA(cudaMemcpyAsync(xcm.p, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    launch_cm_to_ri<double, double>(st, D, s, xcm.p, D, xri.p);
+
+    // mapping plan (Plan.jl:128-191)
+    double Emin = P->Emin, Emax = P->Emax;
+    {
+        auto w0 = std::chrono::steady_clock::now();
+        if (!P->has_Emin || !P->has_Emax) {
+            double lo = 0, hi = 0;
+            // v0 = x0[:, 1] (column 0 of the column-major copy)
+            extrema_from_device(op, xcm.p, P->extrema_maxdim > 0 ? P->extrema_maxdim : 1000, 1e-14, 1e-8, &lo, &hi,
+                                nullptr);
+            if (!P->has_Emin) Emin = lo;
+            if (!P->has_Emax) Emax = hi;
+        }
+        sync(h);
+        R.stage_seconds[6] = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+    }
+    const double a = (Emax - Emin) / 2, b = (Emax + Emin) / 2;
+    PF_CHECK(a > 0 && std::isfinite(a) && std::isfinite(b), PF_ERR_NUMERIC, "degenerate spectral range Emax <= Emin");
+
+    // transform plan (Plan.jl:203-236)
+    TransformState t;
+    t.target_kind = P->target_kind;
+    t.target_value = P->target_value;
+    t.a = a;
+    t.b = b;
+    t.howmany = nev;
+    t.cutoff = P->cutoff;
+    t.normalization = P->normalization;
+    t.order_safety_factor = P->order_safety_factor;
+    t.order = P->order;
+    t.has_left = P->has_left != 0;
+    t.has_right = P->has_right != 0;
+    if (t.has_left) t.left = (P->left - b) / a;
+    if (t.has_right) t.right = (P->right - b) / a;
+    if (t.target_kind == PF_TARGET_UNRESCALED) { t.target = (t.target_value - b) / a; t.has_target = true; }
+    else if (t.target_kind == PF_TARGET_RESCALED) { t.target = t.target_value; t.has_target = true; }
+    else if (t.target_kind == PF_TARGET_MIDDLE) { t.target = 0.0; t.has_target = true; }
+    else if (t.target_kind == PF_TARGET_OFFSET) {
+        PF_CHECK(t.target_value >= -1 && t.target_value <= 1, PF_ERR_INVALID, "Offset target requires eta in [-1, 1]");
+    } else if (t.target_kind != PF_TARGET_MAXDOS) throw Error(PF_ERR_INVALID, "Unsupported target specification");
+
+    // DoS (DensitiesOfStates.jl:14-43)
+    std::vector<double> mu;
+    {
+        auto w0 = std::chrono::steady_clock::now();
+        DevArray<double> pr64;
+        DevArray<float> pr32;
+        if (P->probes) {
+            pr64.alloc((size_t)D * P->dos_R);
+            PF_CUDA(cudaMemcpyAsync(pr64.p, P->probes, pr64.n * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        if (P->precision == PF_PREC_FP64) {
+            mu = kpm_moments<double>(op, a, b, P->dos_N, P->dos_R, pr64.p, D, P->probe_kind, P->seed, &R.kpm_block_matvecs);
+        } else {
+            if (P->probes) {
+                pr32.alloc((size_t)D * P->dos_R);
+                // FP64 host probes -> FP32 device copy (column-major kept)
+                launch_ri_to_cm<double, float>(st, (int64_t)P->dos_R * D, 1, pr64.p, pr32.p, (int64_t)P->dos_R * D);
+            }
+            mu = kpm_moments<float>(op, a, b, P->dos_N, P->dos_R, pr32.p, D, P->probe_kind, P->seed, &R.kpm_block_matvecs);
+        }
+        R.stage_seconds[7] = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+    }
+    Dos rho(mu, P->dos_N, P->dos_kernel);
+    {
+        auto w0 = std::chrono::steady_clock::now();
+        get_bounds(t, &rho);
+        get_order(t);
+        R.stage_seconds[8] = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+    }
+    const std::vector<double> coeffs = normalized_coefficients(t);
+
+    // factorization (FactorizationConfig.jl:99-118, polfed_algorithm.jl:25-34)
+    const int64_t maxdim = expected_krylov_dim(nev, s, P->overestimate_iters);
+    PF_CHECK(maxdim >= s && maxdim < (1 << 20), PF_ERR_INVALID, "unreasonable Krylov dimension");
+    LanczosOut out;
+    double stage[6] = {0, 0, 0, 0, 0, 0};
+    const int fdtype = P->precision == PF_PREC_FP64 ? PF_F64 : PF_F32;
+    if (P->autotune) {
+        bool have;
+        {
+            std::lock_guard<std::mutex> lock(op->tune_mu);
+            have = op->tuned_width.count(std::make_pair(fdtype == PF_F64 ? 8 : 4, s)) > 0;
+        }
+        if (!have) autotune_step(op, s, fdtype, nullptr);
+    }
+    if (P->precision == PF_PREC_FP64) {
+        Filter<double> filt(op, s, coeffs, a, b);
+        BlockMap fmap = [&](const double *X, double *Y) {
+            PF_CUDA(cudaMemcpyAsync(filt.X.p, X, (size_t)D * s * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            filt.run(st);
+            PF_CUDA(cudaMemcpyAsync(Y, filt.Y.p, (size_t)D * s * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        };
+        lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage);
+    } else {
+        Filter<float> filt(op, s, coeffs, a, b);
+        BlockMap fmap = [&](const double *X, double *Y) {
+            launch_ri_to_cm<double, float>(st, (int64_t)D * s, 1, X, filt.X.p, (int64_t)D * s);
+            filt.run(st);
+            launch_ri_to_cm<float, double>(st, (int64_t)D * s, 1, filt.Y.p, Y, (int64_t)D * s);
+        };
+        lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage);
+    }
+
+    // outputs
+    *nconv = out.nconv;
+    for (int i = 0; i < out.nconv; ++i) vals[i] = out.vals[i];
+    if (vecs && out.nconv > 0) {
+        if (vecs_mem == PF_MEM_DEVICE) {
+            launch_ri_to_cm<double, double>(st, D, out.nconv, out.vecs.p, vecs, D);
+            sync(h);
+        } else {
+            DevArray<double> cm((size_t)D * out.nconv);
+            launch_ri_to_cm<double, double>(st, D, out.nconv, out.vecs.p, cm.p, D);
+            PF_CUDA(cudaMemcpyAsync(vecs, cm.p, cm.n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            sync(h);
+        }
+    }
+    PF_CUDA(cudaEventRecord(t_end, st));
+    sync(h);
+    float tot_ms = 0.f;
+    cudaEventElapsedTime(&tot_ms, t_begin, t_end);
+    cudaEventDestroy(t_begin);
+    cudaEventDestroy(t_end);
+    (void)t_wall0;
+
+    if (rep) {
+        R.Emin = Emin; R.Emax = Emax; R.a = a; R.b = b;
+        R.target = t.target; R.left = t.left; R.right = t.right;
+        R.order = t.order;
+        R.order_safety_factor = t.order_safety_factor;
+        R.blocksize = s;
+        R.howmany = nev;
+        R.iters_needed = out.numiter;
+        R.iters_reserved = out.maxiter;
+        R.krylovdim = out.krylovdim;
+        R.matvecs = (int64_t)t.order * s * out.numiter + nev;  // SpectralTransformReport.jl:54
+        R.tol = P->tol;
+        R.residual = out.residual;
+        R.converged_tol = out.converged;
+        R.eigentol = P->eigentol;
+        R.eigenresidual = out.eigenresidual;
+        R.converged_eigentol = out.eigenconverged;
+        R.numofchecks = out.numofchecks;
+        for (int i = 0; i < (int)out.conv_hist.size() && i < PF_REPORT_MAX_CHECKS; ++i) {
+            R.converged_history[i] = out.conv_hist[i];
+            R.krylovdim_history[i] = out.dim_hist[i];
+            R.maxresidual_history[i] = out.res_hist[i];
+        }
+        for (int i = 0; i < 6; ++i) R.stage_seconds[i] = stage[i];
+        R.stage_seconds[9] = tot_ms * 1e-3;
+        R.basis_bytes_reserved = (double)D * out.maxiter * s * sizeof(double);
+        R.basis_bytes_used = (double)D * out.krylovdim * sizeof(double);
+        *rep = R;
+    }
+}
+
+}  // namespace pf

@@ -1,0 +1,32 @@
+// pf_solver.h -- host-side orchestration of the POLFED path on one device.
+#pragma once
+#include <functional>
+#include <vector>
+
+#include "pf_internal.h"
+
+namespace pf {
+
+pf_op *create_spin_chain(pf_handle *h, int L, int Lup, int nbonds, const int32_t *bonds, const double *J,
+                         const double *Delta, const double *fields);
+pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup, const int32_t *nbr,
+                   const double *fields, const double *grain);
+void destroy_op(pf_op *op);
+void *handle_scratch(pf_handle *h, size_t bytes);
+
+void op_apply(pf_op *op, int dtype, double a, double b, int s, const void *X, int64_t ldx, void *Y, int64_t ldy);
+void op_recurrence(pf_op *op, int dtype, double a, double b, double c, int s, void *b1, const void *b2,
+                   const void *b3, const void *X, int64_t ld);
+void op_finalsum(pf_op *op, int dtype, double a, double b, double c0, int s, const void *b1, const void *b2,
+                 void *Y, const void *X, int64_t ld);
+void op_filter(pf_op *op, int dtype, double a, double b, int K, const double *coeffs, int s, const void *X,
+               int64_t ldx, void *Y, int64_t ldy);
+void op_kpm(pf_op *op, int dtype, double a, double b, int N, int R, const void *probes, int64_t ldp,
+            int probe_kind, uint64_t seed, double *mu);
+
+void solve(pf_op *op, const pf_params *p, int s, int nev, const double *x0, int x0_mem, double *vals,
+           double *vecs, int vecs_mem, pf_report *rep, int *nconv);
+void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, double eigentol, double *Emin,
+                     double *Emax);
+
+}  // namespace pf

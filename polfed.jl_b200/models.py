@@ -1,0 +1,242 @@
+"""Model constructors mirroring ``Polfed.Models`` (SpinHalfChains.jl, QSun/).
+
+The reference constructors return a ``SparseMatrixCSC``; here they return a
+matrix-free operator descriptor whose device form (``pf_op``) the CUDA kernels
+apply directly.  Arguments, defaults and validation follow the reference:
+
+* ``xxz_hamiltonian``  -- SpinHalfChains.jl:74-99
+* ``j1j2_hamiltonian`` -- SpinHalfChains.jl:189-220
+* ``qsun_hamiltonian`` -- Models/Models.jl:97-115 -> QSun/QSun.jl:277-324 ->
+  QSun/QuantumSun.jl:1-102 (full space, S = 1/2)
+
+Random draws use a numpy ``Generator`` (``rng``); Julia's MersenneTwister
+streams are not reproducible outside Julia, so a realisation is identified by
+its explicit parameter arrays (``fields``, ``couplings``, ...), which every
+operator exposes.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+
+_SUPPORTED_BOUNDARIES = ("periodic", "open")
+
+
+def chain_bonds(L: int, distance: int, boundary: str = "periodic"):
+    """0-based bonds of ``_chain_bonds`` (SpinHalfChains.jl:227-243)."""
+    if boundary not in _SUPPORTED_BOUNDARIES:
+        raise ValueError(f"boundary must be one of (:periodic, :open); got {boundary}.")
+    if boundary == "open":
+        if distance >= L:
+            return []
+        return [(i, i + distance) for i in range(L - distance)]
+    bonds = []
+    for i in range(1, L + 1):
+        j = (i + distance - 1) % L + 1  # mod1(i + distance, L)
+        if i == j:
+            continue
+        bonds.append((i - 1, j - 1))
+    return bonds
+
+
+def _validate_chain_length(L: int) -> None:
+    if L < 2:
+        raise ValueError(f"L must be at least 2; got L={L}.")
+
+
+def _resolve_fields(L: int, field: float, W: float, fields, rng) -> np.ndarray:
+    """``_resolve_fields`` (SpinHalfChains.jl:245-257): h_i = field + W (2u - 1)."""
+    if fields is not None:
+        fields = np.asarray(fields, dtype=np.float64).ravel()
+        if len(fields) != L:
+            raise ValueError(f"fields must have length L={L}; got length {len(fields)}.")
+        return fields.copy()
+    W = float(W)
+    if W < 0:
+        raise ValueError(f"W must be non-negative; got {W}.")
+    if W == 0:
+        return np.full(L, float(field))
+    rng = np.random.default_rng() if rng is None else rng
+    return float(field) + W * (2 * rng.random(L) - 1)
+
+
+class Operator:
+    """Base of the matrix-free operators: owns the device descriptor."""
+
+    kind = "operator"
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self._op: Optional[int] = None
+
+    @property
+    def handle(self) -> int:
+        return _lib.handle(self.device)
+
+    @property
+    def op(self) -> int:
+        if self._op is None:
+            self._op = self._create()
+        return self._op
+
+    def _create(self) -> int:  # pragma: no cover - abstract
+        raise NotImplementedError
+
+    @property
+    def dim(self) -> int:
+        return int(_lib.load().pf_op_dim(self.op))
+
+    @property
+    def shape(self):
+        return (self.dim, self.dim)
+
+    def close(self) -> None:
+        if self._op is not None:
+            _lib.load().pf_op_destroy(self._op)
+            self._op = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SpinChainOperator(Operator):
+    """Spin-1/2 chain H = sum_b J_b[(S+S- + h.c.)/2 + Delta_b SzSz] + sum_i h_i Sz_i
+    on the sector with ``Lup`` up spins (``Lup=-1``: full 2^L space)."""
+
+    kind = "spin_chain"
+
+    def __init__(self, L: int, Lup: int, bonds: Sequence, couplings, anisotropies, fields, device: int = 0):
+        super().__init__(device)
+        if not (0 <= Lup <= L or Lup == -1):
+            raise ValueError(f"Lup must satisfy 0 <= Lup <= L; got Lup={Lup} for L={L}.")
+        self.L = int(L)
+        self.Lup = int(Lup)
+        self.bonds = [(int(i), int(j)) for i, j in bonds]
+        self.couplings = np.asarray(couplings, dtype=np.float64).reshape(-1)
+        self.anisotropies = np.asarray(anisotropies, dtype=np.float64).reshape(-1)
+        self.fields = np.asarray(fields, dtype=np.float64).reshape(-1)
+        if len(self.couplings) != len(self.bonds) or len(self.anisotropies) != len(self.bonds):
+            raise ValueError("one coupling and one anisotropy per bond are required")
+        if len(self.fields) != self.L:
+            raise ValueError(f"fields must have length L={self.L}; got length {len(self.fields)}.")
+
+    def _create(self) -> int:
+        nb = len(self.bonds)
+        bonds = np.ascontiguousarray(np.array(self.bonds, dtype=np.int32).reshape(-1) if nb else np.zeros(2, np.int32))
+        J = np.ascontiguousarray(self.couplings if nb else np.zeros(1))
+        Dl = np.ascontiguousarray(self.anisotropies if nb else np.zeros(1))
+        f = np.ascontiguousarray(self.fields)
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().pf_op_spin_chain_create(
+            self.handle, self.L, self.Lup, nb, bonds.ctypes.data, J.ctypes.data, Dl.ctypes.data,
+            f.ctypes.data, ctypes.byref(out)))
+        return out.value
+
+    def expected_dim(self) -> int:
+        return 2 ** self.L if self.Lup < 0 else math.comb(self.L, self.Lup)
+
+
+class QSunOperator(Operator):
+    """Spin-1/2 Quantum Sun in the full space (QuantumSun.jl:1-102)."""
+
+    kind = "qsun"
+
+    def __init__(self, L_loc: int, L_grain: int, g0: float, couplings, neighbors, fields, grain,
+                 device: int = 0):
+        super().__init__(device)
+        self.L_loc = int(L_loc)
+        self.L_grain = int(L_grain)
+        self.g0 = float(g0)
+        self.couplings = np.asarray(couplings, dtype=np.float64).reshape(-1)
+        self.neighbors = np.asarray(neighbors, dtype=np.int32).reshape(-1)
+        self.fields = np.asarray(fields, dtype=np.float64).reshape(-1)
+        dg = 2 ** self.L_grain
+        self.grain = np.asarray(grain, dtype=np.float64).reshape(dg, dg)
+        for arr, name in ((self.couplings, "couplings"), (self.neighbors, "neighbors"), (self.fields, "fields")):
+            if len(arr) != self.L_loc:
+                raise ValueError(f"{name} must have length L_loc={self.L_loc}")
+
+    def _create(self) -> int:
+        c = np.ascontiguousarray(self.couplings)
+        n = np.ascontiguousarray(self.neighbors, dtype=np.int32)
+        f = np.ascontiguousarray(self.fields)
+        g = np.ascontiguousarray(self.grain)
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().pf_op_qsun_create(
+            self.handle, self.L_loc, self.L_grain, self.g0, c.ctypes.data, n.ctypes.data, f.ctypes.data,
+            g.ctypes.data, ctypes.byref(out)))
+        return out.value
+
+
+def xxz_hamiltonian(L: int, Lup: int, J: float, Delta: float, W: float, *, boundary: str = "periodic",
+                    field: float = 0.0, fields=None, rng=None, device: int = 0) -> SpinChainOperator:
+    """XXZ chain (SpinHalfChains.jl:74-99)."""
+    _validate_chain_length(L)
+    bonds = chain_bonds(int(L), 1, boundary)
+    local_fields = _resolve_fields(int(L), field, W, fields, rng)
+    return SpinChainOperator(L, Lup, bonds, [float(J)] * len(bonds), [float(Delta)] * len(bonds),
+                             local_fields, device=device)
+
+
+def j1j2_hamiltonian(L: int, Lup: int, J1: float, J2: float, Delta1: float, Delta2: float, W: float, *,
+                     boundary: str = "periodic", field: float = 0.0, fields=None, rng=None,
+                     device: int = 0) -> SpinChainOperator:
+    """J1-J2 XXZ chain (SpinHalfChains.jl:189-220)."""
+    _validate_chain_length(L)
+    nn = chain_bonds(int(L), 1, boundary)
+    nnn = chain_bonds(int(L), 2, boundary)
+    local_fields = _resolve_fields(int(L), field, W, fields, rng)
+    return SpinChainOperator(L, Lup, nn + nnn, [float(J1)] * len(nn) + [float(J2)] * len(nnn),
+                             [float(Delta1)] * len(nn) + [float(Delta2)] * len(nnn), local_fields,
+                             device=device)
+
+
+def goe_matrix(n: int, rng) -> np.ndarray:
+    """(X + X^T)/sqrt(2), X ~ randn (RandomUtils.jl:5-8)."""
+    X = rng.standard_normal((n, n))
+    return (X + X.T) / math.sqrt(2)
+
+
+def qsun_parameters(L_loc: int, L_grain: int, alpha: float, *, gamma: float = 1.0, w: float = 0.5,
+                    hz: float = 1.0, zeta: float = 0.2, rng=None):
+    """Random draws of build_hamiltonian (QuantumSun.jl:21-30) in the same order:
+    fields ~ U[hz-w, hz+w], neighbours ~ U{0..L_grain-1}, couplings c_1 = 1,
+    c_j = alpha^(j-1+U(-zeta,zeta)), grain = gamma * GOE / sqrt(dg + 1)."""
+    rng = np.random.default_rng() if rng is None else rng
+    fields = rng.random(L_loc) * ((hz + w) - (hz - w)) + (hz - w)
+    neighbors = rng.integers(0, L_grain, size=L_loc)
+    couplings = np.zeros(L_loc)
+    if alpha > 0:
+        couplings[0] = 1.0
+        for j in range(2, L_loc + 1):
+            u = j - 1 + rng.random() * 2 * zeta - zeta
+            couplings[j - 1] = alpha ** u
+    dg = 2 ** L_grain
+    grain = gamma * goe_matrix(dg, rng) / math.sqrt(dg + 1)
+    return fields, neighbors, couplings, grain
+
+
+def qsun_hamiltonian(L_loc: int, L_grain: int, g0: float, alpha: float, *, gamma: float = 1.0, w: float = 0.5,
+                     hz: float = 1.0, zeta: float = 0.2, S: float = 0.5, rng=None, use_U1: bool = False,
+                     S_z: float = 0.0, couplings=None, neighbors=None, fields=None, grain=None,
+                     device: int = 0) -> QSunOperator:
+    """Quantum Sun model (QSun.jl:277-324 / QuantumSun.jl:1-102).  Explicit
+    ``couplings`` / ``neighbors`` / ``fields`` / ``grain`` override the draws."""
+    if not float(2 * S).is_integer():
+        raise ValueError(f"Wrong value of spin. Only integer spins or half-integer spins are possible. You chose S = {S}")
+    if S != 0.5:
+        raise NotImplementedError("the B200 path implements the spin-1/2 Quantum Sun only")
+    if use_U1:
+        raise NotImplementedError("the U(1) Quantum Sun sector is not implemented on the B200 path")
+    f, n, c, g = qsun_parameters(L_loc, L_grain, alpha, gamma=gamma, w=w, hz=hz, zeta=zeta, rng=rng)
+    return QSunOperator(L_loc, L_grain, g0, c if couplings is None else couplings,
+                        n if neighbors is None else neighbors, f if fields is None else fields,
+                        g if grain is None else grain, device=device)

@@ -1,0 +1,197 @@
+"""End-to-end POLFED solves on the B200 against the CPU oracle and dense eigh.
+
+Shared inputs pin what the reference leaves random: explicit fields,
+couplings and grain blocks, explicit KPM probe vectors and x0.  With those
+fixed, the GPU and the oracle resolve the same target, interval and order,
+and return the same eigenvalues to 1e-10 relative, each with an FP64
+residual ||H psi - E psi|| below the eigen tolerance.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_pairs(H, vals, vecs, tol):
+    assert np.all(np.diff(vals) >= 0), "eigenvalues must be ascending (LanczosMethod.jl:76)"
+    for j in range(len(vals)):
+        v = vecs[:, j]
+        assert abs(np.linalg.norm(v) - 1) < 1e-9
+        r = np.linalg.norm(H @ v - vals[j] * v)
+        assert r < tol, (j, r)
+
+
+def _vs_exact(H, vals):
+    ev = np.linalg.eigvalsh(H.toarray())
+    return float(np.max(np.min(np.abs(ev[:, None] - vals[None, :]), axis=0) / np.maximum(1, np.abs(vals))))
+
+
+def _solve_both(pkg, orc, op, H, x0, nev, target, *, N=96, R=24, seed=0, overestimate_iters=2.0, **kw):
+    """Oracle and GPU solves on identical inputs.  The Krylov budget is doubled
+    (overestimate_iters = 2) so that neither run stops at the last allowed
+    iteration: there the reference's tol = 1e-14 sits at the rounding floor and
+    whether the last pair passes depends on rounding, not on the algorithm."""
+    D = H.shape[0]
+    probes = orc.normalized_gaussian_probes(D, R, np.random.default_rng(seed))
+    okw = {k: v for k, v in kw.items() if k in ("Emin", "Emax", "order", "tol", "eigentol")}
+    ref = orc.polfed(orc.CSROperator(H), x0, nev, target, N=N, R=R, probes=probes,
+                     overestimate_iters=overestimate_iters, **okw)
+    mapping = pkg.MappingConfig(Emin=kw.get("Emin"), Emax=kw.get("Emax"))
+    transform = pkg.TransformConfig(order=kw.get("order"))
+    fact = pkg.FactorizationConfig(tol=kw.get("tol", 1e-14), eigentol=kw.get("eigentol", 1e-9),
+                                   overestimate_iters=overestimate_iters)
+    vals, vecs, rep = pkg.polfed(op, x0, nev, target, produce_report=True, mapping=mapping,
+                                 transform=transform, fact=fact, dos=pkg.DoSConfig(N=N, R=R, probes=probes))
+    return ref, vals, vecs, rep
+
+
+def test_xxz_scalar_lanczos_matches_oracle(pkg, orc, cuda):
+    # C1 shape at L = 12: random-field XXZ, Sz = 0, s = 1, target eps = 0.5
+    L = 12
+    rng = np.random.default_rng(1)
+    f = 5 * (2 * rng.random(L) - 1)
+    op = pkg.xxz_hamiltonian(L, L // 2, 1.0, 1.0, 0.0, fields=f)
+    H = orc.xxz_matrix(L, L // 2, 1.0, 1.0, f)
+    x0 = rng.random(H.shape[0])
+    ref, vals, vecs, rep = _solve_both(pkg, orc, op, H, x0, 10, ("rescaled", 0.5))
+    s = rep.spectral
+    assert abs(s.Emin - ref.Emin) < 1e-9 * abs(ref.Emin) and abs(s.Emax - ref.Emax) < 1e-9 * abs(ref.Emax)
+    assert s.order == ref.order
+    assert abs(s.left - ref.left) < 1e-7 and abs(s.right - ref.right) < 1e-7
+    assert len(vals) == len(ref.vals) == 10
+    np.testing.assert_allclose(vals, ref.vals, rtol=1e-10, atol=1e-10)
+    _check_pairs(H, vals, vecs, 1e-9)
+    assert _vs_exact(H, vals) < 1e-10
+    assert rep.factorization.blocksize == 1 and rep.factorization.converged_tol == 10
+    assert rep.spectral.matrixvec_muls == s.order * rep.factorization.itersneeded + 10
+
+
+@pytest.mark.parametrize("s", [2, 4, 8])
+def test_qsun_block_lanczos_matches_oracle(pkg, orc, cuda, s):
+    rng = np.random.default_rng(10 + s)
+    f, n, c, g = pkg.qsun_parameters(7, 3, 0.75, rng=rng)
+    op = pkg.QSunOperator(7, 3, 1.0, c, n, f, g)
+    H = orc.qsun_matrix(7, 3, 1.0, c, n, f, g)
+    D = H.shape[0]
+    x0, _ = np.linalg.qr(rng.standard_normal((D, s)))
+    ref, vals, vecs, rep = _solve_both(pkg, orc, op, H, x0, 24, ("rescaled", 0.5), seed=s)
+    assert rep.spectral.order == ref.order
+    assert len(vals) == len(ref.vals) == 24
+    np.testing.assert_allclose(vals, ref.vals, rtol=1e-10, atol=1e-10)
+    _check_pairs(H, vals, vecs, 1e-9)
+    assert _vs_exact(H, vals) < 1e-10
+
+
+@pytest.mark.parametrize("target", ["maxdos", "middle", ("offset", 0.3), ("offset", -0.4), ("unrescaled", 1.5)])
+def test_j1j2_targets(pkg, orc, cuda, target):
+    rng = np.random.default_rng(5)
+    L = 14
+    f = 2 * rng.random(L) - 1
+    op = pkg.j1j2_hamiltonian(L, 7, 1.0, 0.5, 1.0, 1.0, 0.0, fields=f)
+    H = orc.j1j2_matrix(L, 7, 1.0, 0.5, 1.0, 1.0, f)
+    D = H.shape[0]
+    x0, _ = np.linalg.qr(rng.standard_normal((D, 4)))
+    ref, vals, vecs, rep = _solve_both(pkg, orc, op, H, x0, 16, target, N=128, R=32)
+    assert abs(rep.spectral.target - ref.target) < 1e-9
+    assert rep.spectral.order == ref.order
+    np.testing.assert_allclose(vals, ref.vals, rtol=1e-10, atol=1e-10)
+    _check_pairs(H, vals, vecs, 1e-9)
+
+
+def test_explicit_extrema_and_order(pkg, orc, cuda):
+    rng = np.random.default_rng(8)
+    L = 12
+    f = 3 * (2 * rng.random(L) - 1)
+    op = pkg.xxz_hamiltonian(L, 6, 1.0, 0.5, 0.0, fields=f)
+    H = orc.xxz_matrix(L, 6, 1.0, 0.5, f)
+    ev = np.linalg.eigvalsh(H.toarray())
+    x0, _ = np.linalg.qr(rng.standard_normal((H.shape[0], 3)))
+    ref, vals, vecs, rep = _solve_both(pkg, orc, op, H, x0, 9, 0.0, Emin=ev[0] - 0.1, Emax=ev[-1] + 0.1,
+                                       order=150)
+    assert rep.spectral.order == 150 == ref.order
+    assert rep.spectral.Emin == ev[0] - 0.1
+    np.testing.assert_allclose(vals, ref.vals, rtol=1e-10, atol=1e-10)
+    _check_pairs(H, vals, vecs, 1e-9)
+
+
+def test_cgs2_and_tolerances(pkg, orc, cuda):
+    # two reorthogonalisation passes (CGS2) give the same eigenpairs
+    rng = np.random.default_rng(9)
+    L = 12
+    f = 5 * (2 * rng.random(L) - 1)
+    op = pkg.xxz_hamiltonian(L, 6, 1.0, 1.0, 0.0, fields=f)
+    H = orc.xxz_matrix(L, 6, 1.0, 1.0, f)
+    x0, _ = np.linalg.qr(rng.standard_normal((H.shape[0], 4)))
+    probes = orc.normalized_gaussian_probes(H.shape[0], 16, rng)
+    dos = pkg.DoSConfig(N=64, R=16, probes=probes)
+    v1, _ = pkg.polfed(op, x0, 12, ("rescaled", -0.2), dos=dos, vecs=False)
+    v2, w2 = pkg.polfed(op, x0, 12, ("rescaled", -0.2), dos=dos,
+                        fact=pkg.FactorizationConfig(reorth_passes=2))
+    np.testing.assert_allclose(v1, v2, rtol=1e-11, atol=1e-11)
+    _check_pairs(H, v2, w2, 1e-9)
+
+
+def test_device_probes_and_repeatability(pkg, orc, cuda):
+    # the default path draws probes on the device; a fixed seed repeats bit for bit
+    rng = np.random.default_rng(12)
+    L = 12
+    f = 4 * (2 * rng.random(L) - 1)
+    op = pkg.xxz_hamiltonian(L, 6, 1.0, 1.0, 0.0, fields=f)
+    H = orc.xxz_matrix(L, 6, 1.0, 1.0, f)
+    x0 = rng.random(H.shape[0])
+    dos = pkg.DoSConfig(seed=1234)
+    a = pkg.polfed(op, x0, 8, ("rescaled", 0.2), dos=dos, produce_report=True)
+    b = pkg.polfed(op, x0, 8, ("rescaled", 0.2), dos=dos, produce_report=True)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert a[2].spectral.order == b[2].spectral.order
+    _check_pairs(H, a[0], a[1], 1e-9)
+    assert _vs_exact(H, a[0]) < 1e-10
+
+
+def test_input_validation(pkg, cuda):
+    from polfed_b200 import _lib
+    op = pkg.xxz_hamiltonian(8, 4, 1.0, 1.0, 0.0, fields=[0.1] * 8)
+    D = op.dim
+    with pytest.raises(ValueError):
+        pkg.polfed(op, np.ones(D + 1), 2, "middle")
+    with pytest.raises(ValueError):
+        pkg.polfed(op, np.ones(D), 2, ("offset", 2.0))
+    with pytest.raises(_lib.PolfedArgumentError):
+        pkg.polfed(op, np.zeros(D), 2, "middle")
+    with pytest.raises(_lib.PolfedArgumentError):
+        pkg.polfed(op, np.full(D, np.nan), 2, "middle")
+    with pytest.raises(_lib.PolfedArgumentError):
+        pkg.polfed(op, np.ones(D), 2, "middle",
+                   transform=pkg.TransformConfig(left=-1.0, right=1.0, order=20),
+                   mapping=pkg.MappingConfig(Emin=-5.0, Emax=5.0))
+
+
+def test_unnormalised_start_is_normalised(pkg, orc, cuda):
+    # PolfedCore.jl:43-95: a non-orthonormal x0 is replaced by an orthonormal copy
+    rng = np.random.default_rng(4)
+    L = 10
+    f = 2 * rng.random(L) - 1
+    op = pkg.xxz_hamiltonian(L, 5, 1.0, 1.0, 0.0, fields=f)
+    H = orc.xxz_matrix(L, 5, 1.0, 1.0, f)
+    x0 = rng.random((H.shape[0], 2)) * 7.0
+    x0c = x0.copy()
+    vals, vecs = pkg.polfed(op, x0, 6, ("rescaled", 0.1), dos=pkg.DoSConfig(N=64, R=8, seed=5))
+    np.testing.assert_array_equal(x0, x0c)
+    assert len(vals) == 6
+    _check_pairs(H, vals, vecs, 1e-9)
+
+
+def test_config_c1_full_size(pkg, orc, cuda):
+    # the reference's CPU-runnable configuration: XXZ L=14, PBC, J=1, Delta=1, h~U[-5,5],
+    # Sz=0 (D=3432), eps=0.5, nev=20, s=1, automatic order, DoS defaults (N=250, R=300)
+    rng = np.random.default_rng(2024)
+    L = 14
+    op = pkg.xxz_hamiltonian(L, 7, 1.0, 1.0, 5.0, rng=rng)
+    H = orc.xxz_matrix(L, 7, 1.0, 1.0, op.fields)
+    x0 = rng.random(H.shape[0])
+    vals, vecs, rep = pkg.polfed(op, x0, 20, ("rescaled", 0.5), produce_report=True,
+                                 dos=pkg.DoSConfig(seed=7), fact=pkg.FactorizationConfig(eigentol=1e-10))
+    assert len(vals) == 20
+    _check_pairs(H, vals, vecs, 1e-10)
+    assert _vs_exact(H, vals) < 1e-10

@@ -1,0 +1,105 @@
+"""Host-side logic and the C-ABI library's presence (CPU only, no compute calls)."""
+import ctypes
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "polfed_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = set(re.findall(r"\b(pf_[a-z_0-9]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = pkg.load_library()
+    declared = _declared_symbols()
+    assert len(declared) >= 20
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in include/polfed_b200.h but not exported"
+    assert lib.pf_abi_version() == 1
+
+
+def test_params_defaults_match_reference(pkg):
+    from polfed_b200 import _lib
+    p = _lib.pf_params()
+    _lib.load().pf_params_default(ctypes.byref(p))
+    # PolfedDefaults.jl:119-217, Plan.jl:143
+    assert p.cutoff == 0.17 and p.normalization == 1.0 and p.order_safety_factor == 0.97
+    assert p.tol == 1e-14 and p.eigentol == 1e-9 and p.overestimate_iters == 1.25
+    assert p.which == _lib.PF_WHICH_LR and p.dos_N == 250 and p.dos_R == 300
+    assert p.dos_kernel == _lib.KERNEL_IDS["Jackson"] and p.extrema_maxdim == 1000
+    assert p.precision == _lib.PF_PREC_FP64 and p.reorth_passes == 1
+
+
+def test_target_spec(pkg):
+    from polfed_b200 import _lib
+    n = pkg.normalize_target_spec
+    assert n("maxdos") == (_lib.PF_TARGET_MAXDOS, 0.0)
+    assert n("middle") == (_lib.PF_TARGET_MIDDLE, 0.0)
+    assert n(("offset", 0.25)) == (_lib.PF_TARGET_OFFSET, 0.25)
+    assert n(("unrescaled", -1.2)) == (_lib.PF_TARGET_UNRESCALED, -1.2)
+    assert n(0.7) == (_lib.PF_TARGET_UNRESCALED, 0.7)
+    assert n(("rescaled", 0.4)) == (_lib.PF_TARGET_RESCALED, 0.4)
+    for bad in ["unknown", ("offset", 1.5), ("offset", "0.2"), ("absolute", 0.0), ("quantile", 0.5),
+                ("other", 0.0), True]:
+        with pytest.raises(ValueError):
+            n(bad)
+
+
+def test_krylov_dim(pkg):
+    # PolfedDefaults.jl:61-62 and the shapes quoted for the benchmark configurations
+    assert pkg.expectedkrylovdim(20, 1, 1.25) == 68
+    assert pkg.expectedkrylovdim(200, 8, 1.25) == 629
+    assert pkg.expectedkrylovdim(100, 16, 1.25) == 621
+    assert pkg.expectedkrylovdim(3, 2, 1.0) == 46
+
+
+def test_chain_bonds_and_models(pkg, orc):
+    for L in (2, 3, 4, 7):
+        for d in (1, 2):
+            for bc in ("open", "periodic"):
+                assert pkg.chain_bonds(L, d, bc) == orc.chain_bonds(L, d, bc)
+    op = pkg.xxz_hamiltonian(6, 3, 1.0, 0.8, 0.0, fields=[0.1] * 6)
+    assert op.expected_dim() == 20 and len(op.bonds) == 6
+    op = pkg.j1j2_hamiltonian(6, 3, 1.0, 0.5, 1.0, 1.0, 0.0, fields=[0.0] * 6)
+    assert len(op.bonds) == 12
+    assert op.couplings.tolist() == [1.0] * 6 + [0.5] * 6
+    rng = np.random.default_rng(0)
+    op = pkg.xxz_hamiltonian(8, 4, 1.0, 1.0, 3.0, rng=rng)
+    assert np.all(np.abs(op.fields) <= 3.0)
+    for bad in [dict(L=1, Lup=0), dict(L=4, Lup=-2), dict(L=4, Lup=5)]:
+        with pytest.raises(ValueError):
+            pkg.xxz_hamiltonian(bad["L"], bad["Lup"], 1.0, 1.0, 0.0)
+    with pytest.raises(ValueError):
+        pkg.xxz_hamiltonian(4, 2, 1.0, 1.0, 0.0, boundary="twisted")
+    with pytest.raises(ValueError):
+        pkg.xxz_hamiltonian(4, 2, 1.0, 1.0, 0.0, fields=[0.0, 1.0])
+    with pytest.raises(ValueError):
+        pkg.xxz_hamiltonian(4, 2, 1.0, 1.0, -1.0)
+    with pytest.raises(ValueError):
+        pkg.j1j2_hamiltonian(4, 2, 1.0, 0.5, 1.0, 0.8, -1.0)
+
+
+def test_qsun_parameters(pkg):
+    rng = np.random.default_rng(11)
+    f, n, c, g = pkg.qsun_parameters(13, 3, 0.75, zeta=0.2, hz=1.0, w=0.5, gamma=1.0, rng=rng)
+    assert f.shape == (13,) and np.all((f >= 0.5) & (f <= 1.5))
+    assert n.shape == (13,) and np.all((n >= 0) & (n < 3))
+    assert c[0] == 1.0
+    for j in range(2, 14):
+        u = math.log(c[j - 1]) / math.log(0.75)
+        assert (j - 1) - 0.2 <= u <= (j - 1) + 0.2
+    assert g.shape == (8, 8) and np.allclose(g, g.T)
+    op = pkg.qsun_hamiltonian(13, 3, 1.0, 0.75, rng=np.random.default_rng(1))
+    assert op.L_loc == 13 and op.grain.shape == (8, 8)
+    with pytest.raises(NotImplementedError):
+        pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, S=1.0)
+    with pytest.raises(ValueError):
+        pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, S=0.3)

@@ -1,0 +1,220 @@
+"""Pins the CPU oracle to the reference's own known-answer tests (CPU only).
+
+Every case below comes from the reference's Julia test suite
+(tests/golden/reference_known_answers.json cites file:line).  The oracle is
+the checker for the CUDA path, so it has to reproduce these values first.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_known_answers.json")))
+
+
+@pytest.mark.parametrize("name", ["xxz_L2_open", "xxz_L2_periodic_is_twice_open", "xxz_fields_only_is_diagonal",
+                                  "xxz_three_site"])
+def test_xxz_known_answers(orc, name):
+    g = GOLD[name]
+    H = orc.xxz_matrix(g["L"], g["Lup"], g["J"], g["Delta"], g["fields"], boundary=g["boundary"]).toarray()
+    np.testing.assert_allclose(H, np.array(g["expected"]), rtol=0, atol=1e-14)
+    assert np.allclose(H, H.T)
+
+
+def test_j1j2_hardcoded(orc):
+    g = GOLD["j1j2_L4_open_hardcoded"]
+    H = orc.j1j2_matrix(g["L"], g["Lup"], g["J1"], g["J2"], g["Delta1"], g["Delta2"], g["fields"],
+                        boundary=g["boundary"]).toarray()
+    np.testing.assert_allclose(H, np.array(g["expected"]), rtol=0, atol=1e-14)
+
+
+def test_j1j2_reductions(orc):
+    # test_models.jl:99-157: J2 = 0 reduces to XXZ; periodic J2 doubles the L=4 open chain;
+    # the L=3 periodic J2 chain equals the XXZ triangle.
+    f = [0.1, -0.2, 0.3, -0.4]
+    a = orc.j1j2_matrix(4, 2, 1.3, 0.0, 0.8, 2.0, f, boundary="open").toarray()
+    b = orc.xxz_matrix(4, 2, 1.3, 0.8, f, boundary="open").toarray()
+    np.testing.assert_allclose(a, b, atol=1e-14)
+    z = [0.0] * 4
+    op_ = orc.j1j2_matrix(4, 2, 0.0, 1.0, 1.0, 1.0, z, boundary="open").toarray()
+    pe = orc.j1j2_matrix(4, 2, 0.0, 1.0, 1.0, 1.0, z, boundary="periodic").toarray()
+    np.testing.assert_allclose(pe, 2 * op_, atol=1e-14)
+    t1 = orc.j1j2_matrix(3, 1, 0.0, 0.7, 2.0, 0.5, [0.0] * 3, boundary="periodic").toarray()
+    t2 = orc.xxz_matrix(3, 1, 0.7, 0.5, [0.0] * 3, boundary="periodic").toarray()
+    np.testing.assert_allclose(t1, t2, atol=1e-14)
+
+
+def test_sector_dims_and_basis(orc):
+    for L, Lup, D in GOLD["sector_dims"]["cases"]:
+        basis = orc.sector_basis(L, Lup)
+        assert len(basis) == D == math.comb(L, Lup)
+        assert np.all(np.diff(basis.astype(np.int64)) > 0)
+        assert all(bin(int(s)).count("1") == Lup for s in basis)
+        idx = orc.sector_rank(basis, basis)
+        np.testing.assert_array_equal(idx, np.arange(D))
+
+
+def test_chain_bonds(orc):
+    assert orc.chain_bonds(2, 1, "periodic") == [(0, 1), (1, 0)]
+    assert orc.chain_bonds(4, 2, "open") == [(0, 2), (1, 3)]
+    assert orc.chain_bonds(3, 1, "open") == [(0, 1), (1, 2)]
+    assert orc.chain_bonds(4, 2, "periodic") == [(0, 2), (1, 3), (2, 0), (3, 1)]
+    with pytest.raises(ValueError):
+        orc.chain_bonds(4, 1, "twisted")
+
+
+def test_qsun_structure(orc):
+    # test_qsun.jl:5-76 checks sizes and Hermiticity only; the QSun values are unpinned.
+    rng = np.random.default_rng(3)
+    L_loc, L_grain = 4, 2
+    dg = 2 ** L_grain
+    X = rng.standard_normal((dg, dg))
+    Hg = (X + X.T) / math.sqrt(2) / math.sqrt(dg + 1)
+    H = orc.qsun_matrix(L_loc, L_grain, 1.0, np.array([1.0, 0.7, 0.5, 0.3]), np.array([0, 1, 0, 1]),
+                        rng.random(L_loc) + 0.5, Hg).toarray()
+    assert H.shape == (64, 64)
+    np.testing.assert_allclose(H, H.T, atol=1e-15)
+    # the grain block sits on the low bits: rows 0..3 couple through Hg
+    np.testing.assert_allclose(H[:dg, :dg] - np.diag(np.diag(H[:dg, :dg])), Hg - np.diag(np.diag(Hg)), atol=1e-15)
+
+
+def test_structured_csr_apply(orc):
+    # optimization.jl:236-304: the optimized map equals H * x for vectors and blocks.
+    g = GOLD["structured_packing"]
+    H = sp.lil_matrix((5, 5))
+    for i, v in enumerate(g["diagonals"]):
+        H[i, i] = v
+    for i, j, v in g["offdiag"]:
+        H[i - 1, j - 1] = v
+        H[j - 1, i - 1] = v
+    op = orc.CSROperator(H.tocsr())
+    x = np.array([1.0, 2, 3, 4, 5])
+    X = np.stack([x, 2 * x], axis=1)
+    np.testing.assert_allclose(op.apply(x), H @ x)
+    np.testing.assert_allclose(op.apply(X), H @ X)
+    # Clenshaw step formulas (optimization.jl:307-325) via a K=1 filter
+    c = 0.5
+    b2 = np.array([4.0, 3, 2, 1, 0])
+    out = c * x + 2 * (H @ b2) - np.ones(5)
+    y = op.rescaled(b2, 1.0, 0.0)
+    np.testing.assert_allclose(c * x + 2 * y - np.ones(5), out)
+
+
+def test_dos_kernels(orc):
+    k = GOLD["dos_kernels"]
+    assert orc.Dirichlet(0, 8) == k["Dirichlet(0,8)"]
+    assert orc.Dirichlet(5, 8) == k["Dirichlet(5,8)"]
+    assert orc.Fejer(0, 10) == 1 and math.isclose(orc.Fejer(4, 10), 0.6) and orc.Fejer(10, 10) == 0
+    assert math.isclose(orc.Lorentz(0, 10), 1) and math.isclose(orc.Lorentz(10, 10), 0, abs_tol=1e-15)
+    assert orc.LanczosK(0, 10) == 1 and orc.WangZunger(0, 10) == 1
+    assert orc.WangZunger(5, 10) < orc.WangZunger(0, 10)
+    assert math.isclose(orc.Jackson(0, 10), 1)
+    with pytest.raises(ValueError):
+        orc.get_kernel("UnknownKernel")
+
+
+def test_dos_moments_identity(orc):
+    g = GOLD["dos_moments_identity"]
+    # trace! with the identity map gives mu == 1 (test_spectral_helpers.jl:38-46)
+    op = orc.CSROperator(sp.identity(2, format="csr"))
+    mu = op.kpm_trace(1.0, 0.0, g["N"], np.array(g["trace_probe"]).reshape(2, 1))
+    np.testing.assert_allclose(mu, g["trace_expected"])
+    # dos_moments(identity, N=5, R=3, D=4) == 4 (test_spectral_helpers.jl:48-50)
+    op4 = orc.CSROperator(sp.identity(4, format="csr"))
+    probes = orc.normalized_gaussian_probes(4, 3, np.random.default_rng(0))
+    mu = orc.dos_moments(op4, 1.0, 0.0, 5, probes)
+    np.testing.assert_allclose(mu, np.full(5, 4.0))
+    rho = orc.make_rho(mu, 5, "Dirichlet")
+    assert math.isclose(float(rho(0.0)), 4 / math.pi)
+
+
+def test_spectral_helpers(orc):
+    assert abs(orc.bisection(lambda x: x - 0.25, 0.0, 1.0, tol=1e-10) - 0.25) < 1e-8
+    with pytest.raises(RuntimeError):
+        orc.bisection(lambda x: x * x + 1, -1.0, 1.0)
+    assert math.isclose(orc.analytical_orderofexpansion(0.0, 0.5), 2.65499 / 0.5)
+    assert orc.analytical_orderofexpansion(0.0, 0.25) > orc.analytical_orderofexpansion(0.0, 0.5)
+    assert orc.analytical_orderofexpansion(0.8, 0.5) < orc.analytical_orderofexpansion(0.0, 0.5)
+    g = GOLD["bounds_flat_rho"]
+    plan = orc.build_transform_plan("middle", 1, 1.0, 0.0)
+    orc.getbounds_from_dos(plan, lambda x: np.ones_like(np.asarray(x, dtype=float)), "mean")
+    assert abs(plan.left - g["left"]) < g["atol"] and abs(plan.right - g["right"]) < g["atol"]
+    g = GOLD["bounds_from_order"]
+    plan = orc.build_transform_plan("middle", 1, 1.0, 0.0, order=g["order"], cutoff=g["cutoff"])
+    orc.getbounds_from_K(plan)
+    assert -1 <= plan.left < plan.target < plan.right <= 1
+    assert abs(plan.left + plan.right) < 1e-7
+    plan = orc.build_transform_plan("middle", 1, 1.0, 0.0, order=12)
+    orc.getorderofexpansion(plan)
+    assert plan.order == 12
+    g = GOLD["order_resolved"]
+    plan = orc.build_transform_plan("middle", 1, 1.0, 0.0, left=g["left"], right=g["right"], cutoff=g["cutoff"],
+                                    osf=g["osf"])
+    orc.getorderofexpansion(plan)
+    assert isinstance(plan.order, int) and plan.order >= g["min_order"]
+    plan = orc.build_transform_plan("middle", 1, 1.0, 0.0, left=-0.2, right=0.2, order=12)
+    with pytest.raises(RuntimeError):
+        orc.getbounds(plan, 1.0, 0.0, lambda x: 1.0)
+
+
+def test_target_spec(orc):
+    assert orc.normalize_target_spec("maxdos") == ("maxdos", None)
+    assert orc.normalize_target_spec("middle") == ("middle", None)
+    assert orc.normalize_target_spec(("offset", 0.25)) == ("offset", 0.25)
+    assert orc.normalize_target_spec(("unrescaled", -1.2)) == ("unrescaled", -1.2)
+    assert orc.normalize_target_spec(0.7) == ("unrescaled", 0.7)
+    assert orc.normalize_target_spec(("rescaled", 0.4)) == ("rescaled", 0.4)
+    for bad in ["unknown", ("offset", 1.5), ("offset", "0.2"), ("absolute", 0.0), ("quantile", 0.5),
+                ("other", 0.0)]:
+        with pytest.raises(ValueError):
+            orc.normalize_target_spec(bad)
+
+
+def test_initial_state(orc):
+    v = np.array([3.0, 4.0])
+    p = orc.prepare_initial_state(v)
+    assert np.allclose(v, [3.0, 4.0]) and math.isclose(np.linalg.norm(p), 1.0)
+    x0 = np.array([[1.0, 1.0], [0.0, 1.0], [1.0, 0.0]])
+    q = orc.prepare_initial_state(x0)
+    np.testing.assert_allclose(q.T @ q, np.eye(2), atol=1e-14)
+    with pytest.raises(ValueError):
+        orc.prepare_initial_state(np.zeros(3))
+    with pytest.raises(ValueError):
+        orc.prepare_initial_state(np.ones((2, 3)))
+
+
+def test_small_polfed_end_to_end(orc):
+    # test_polfed.jl:29-61,166-176: whatever is returned is sorted with small residuals.
+    g = GOLD["small_polfed"]
+    M = sp.diags(g["diag"]).tocsr()
+    op = orc.CSROperator(M)
+    rng = np.random.default_rng(1234)
+    q, _ = np.linalg.qr(rng.standard_normal((6, g["blocksize"])))
+    r = orc.polfed(op, q, g["howmany"], g["target"], Emin=min(g["diag"]), Emax=max(g["diag"]), order=g["order"],
+                   tol=g["tol"], eigentol=g["eigentol"], overestimate_iters=g["overestimate_iters"], N=g["dos_N"],
+                   R=g["dos_R"], probe_rng=rng)
+    assert np.all(np.diff(r.vals) >= 0)
+    assert r.vecs.shape[1] == len(r.vals)
+    for j, v in enumerate(r.vals):
+        assert np.linalg.norm(M @ r.vecs[:, j] - v * r.vecs[:, j]) <= g["residual_atol"] * max(1, abs(v))
+
+
+def test_oracle_solve_matches_dense(orc):
+    # an XXZ chain in the Sz=0 sector: the oracle's POLFED eigenpairs are exact eigenpairs
+    L = 10
+    rng = np.random.default_rng(5)
+    fields = 5 * (2 * rng.random(L) - 1)
+    H = orc.xxz_matrix(L, 5, 1.0, 1.0, fields)
+    op = orc.CSROperator(H)
+    x0 = rng.random(H.shape[0])
+    r = orc.polfed(op, x0, 8, ("rescaled", 0.5), N=64, R=16, probe_rng=rng)
+    ev = np.linalg.eigvalsh(H.toarray())
+    assert len(r.vals) == 8
+    assert np.max(np.min(np.abs(ev[:, None] - r.vals[None, :]), axis=0)) < 1e-10
+    # they are the 8 eigenvalues with the largest filter value P((E - b)/a)
+    P = orc.clenshaw_coeffs_scalar(r.coeffs, (ev - r.b) / r.a)
+    top = np.sort(ev[np.argsort(-P)[:8]])
+    np.testing.assert_allclose(np.sort(r.vals), top, atol=1e-10)
