@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark: converged eigenpairs per second at FP64 residual <= 1e-10.
+
+Workload (the Quantum Sun configuration the headline metric is quoted on):
+spin-1/2 Quantum Sun, a grain of N=3 spins with a seeded GOE 8x8 block scaled
+by gamma=1, L_loc=13 outer spins (full dimension 2^16 = 65536), couplings
+alpha^{u_j} with alpha=0.75, u_j = (j-1) + U[-0.2, 0.2], fields U[0.5, 1.5],
+g0=1; block Lanczos with block size s=8, nev=200 at rescaled energy 0.5,
+FP64 throughout; KPM DoS with the reference defaults (N=250, R=300, Jackson).
+
+One step = one complete POLFED solve of a fresh disorder realisation
+(Emin/Emax Lanczos probes, KPM, interval and order, Chebyshev-filtered block
+Lanczos, Ritz extraction, FP64 Rayleigh quotients and residuals).  An
+eigenpair counts iff its FP64 residual ||H psi - E psi|| <= 1e-10 (eigentol).
+
+* ``value``  -- whole-job eigenpairs/s with x0 and the outputs resident in HBM;
+  timed with CUDA events on the library's stream, max over ranks.
+* ``e2e``    -- the same metric through the public Python API with host x0 and
+  host eigenvectors (H2D / D2H inside the timed region).
+* ``roofline`` -- the dominant kernel (the Clenshaw recurrence step):
+  algorithmic bytes per launch 4*D*s*8 (read b_{k+1}, b_{k+2}, X; write b_k)
+  over its average duration inside the timed solves (CUDA events in the library).
+* ``cpu_baseline`` -- the CPU port of the reference algorithm (oracle/) on this
+  host's cores over a bounded sample, scaled to eigenpairs/s.
+
+N > 1 (torchrun): every rank solves its own realisations (replicas, no data
+path collective); ``scaling`` is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {
+    "workload": "qsun_Lloc13_Lgrain3_D65536_s8_nev200_eps0.5_fp64",
+    "model": "Quantum Sun (S=1/2, full space)", "L_loc": 13, "L_grain": 3, "D": 65536, "g0": 1.0,
+    "alpha": 0.75, "zeta": 0.2, "hz": 1.0, "w": 0.5, "gamma": 1.0, "blocksize": 8, "nev": 200,
+    "target": "(:rescaled, 0.5)", "dos_N": 250, "dos_R": 300, "kernel": "Jackson", "eigentol": 1e-10,
+}
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_step_qsun_fp64_D65536_s8.md")
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------- the workload
+def make_realisations(pkg, n, seed0, device=0):
+    import numpy as np
+    ops, x0s = [], []
+    for i in range(n):
+        rng = np.random.default_rng(seed0 + i)
+        op = pkg.qsun_hamiltonian(WORKLOAD["L_loc"], WORKLOAD["L_grain"], WORKLOAD["g0"], WORKLOAD["alpha"],
+                                  gamma=WORKLOAD["gamma"], w=WORKLOAD["w"], hz=WORKLOAD["hz"],
+                                  zeta=WORKLOAD["zeta"], rng=rng, device=device)
+        D = 2 ** (WORKLOAD["L_loc"] + WORKLOAD["L_grain"])
+        q, _ = np.linalg.qr(rng.standard_normal((D, WORKLOAD["blocksize"])))
+        ops.append(op)
+        x0s.append(np.asfortranarray(q))
+    return ops, x0s
+
+
+def solve(pkg, op, x0, seed):
+    return pkg.polfed(op, x0, WORKLOAD["nev"], ("rescaled", 0.5), produce_report=True,
+                      dos=pkg.DoSConfig(N=WORKLOAD["dos_N"], R=WORKLOAD["dos_R"], seed=seed),
+                      fact=pkg.FactorizationConfig(eigentol=WORKLOAD["eigentol"]))
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def read_traffic():
+    """DRAM bytes per launch of the step kernel from the committed ncu summary."""
+    try:
+        text = open(PROFILE_SUMMARY).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", text)
+    return float(m.group(1)) if m else None
+
+
+# ------------------------------------------------------- CPU baseline
+def cpu_sample(seed=4242, kpm_probes=4, verbose=False):
+    """Time the CPU port of the reference algorithm (oracle/) on a bounded
+    sample of one solve of the workload and scale it to eigenpairs/s.
+
+    Sample: the two Emin/Emax Lanczos probes in full, KPM on ``kpm_probes``
+    probes (scaled by R / kpm_probes), one Chebyshev filter application of
+    the resolved order K to an s=8 block and one full reorthogonalisation
+    against a half-full basis (both scaled by the iteration budget)."""
+    import numpy as np
+    from oracle import oracle as orc
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+    rng = np.random.default_rng(seed)
+    f, n, c, g = pkg.qsun_parameters(WORKLOAD["L_loc"], WORKLOAD["L_grain"], WORKLOAD["alpha"],
+                                     gamma=WORKLOAD["gamma"], w=WORKLOAD["w"], hz=WORKLOAD["hz"],
+                                     zeta=WORKLOAD["zeta"], rng=rng)
+    H = orc.qsun_matrix(WORKLOAD["L_loc"], WORKLOAD["L_grain"], WORKLOAD["g0"], c, n, f, g)
+    op = orc.CSROperator(H)
+    D, s, nev = op.D, WORKLOAD["blocksize"], WORKLOAD["nev"]
+    x0, _ = np.linalg.qr(rng.standard_normal((D, s)))
+    t0 = time.perf_counter()
+    Emin, Emax = orc.lanczos_extrema(op.apply, x0[:, 0])
+    t_ext = time.perf_counter() - t0
+    a, b = (Emax - Emin) / 2, (Emax + Emin) / 2
+    probes = orc.normalized_gaussian_probes(D, kpm_probes, rng)
+    t0 = time.perf_counter()
+    mu = orc.dos_moments(op, a, b, WORKLOAD["dos_N"], probes)
+    t_kpm = (time.perf_counter() - t0) * WORKLOAD["dos_R"] / kpm_probes
+    rho = orc.make_rho(mu, WORKLOAD["dos_N"])
+    plan = orc.build_transform_plan(("rescaled", 0.5), nev, a, b)
+    orc.getbounds(plan, a, b, rho)
+    orc.getorderofexpansion(plan)
+    coeffs = orc.filter_coefficients(plan)
+    iters = math.ceil(orc.expectedkrylovdim(nev, s, 1.25) / s)
+    X = np.asfortranarray(x0)
+    t0 = time.perf_counter()
+    Y = op.filter(X, a, b, coeffs)
+    t_filter = time.perf_counter() - t0
+    B = np.asfortranarray(rng.standard_normal((D, (iters // 2) * s)))
+    t0 = time.perf_counter()
+    Y = Y - B @ (B.T @ Y)
+    t_reorth = time.perf_counter() - t0
+    T = t_ext + t_kpm + iters * (t_filter + t_reorth)
+    threads = orc.lib().orc_num_threads()
+    if verbose:
+        print(f"cpu sample: extrema {t_ext:.2f}s kpm(est) {t_kpm:.2f}s filter {t_filter:.3f}s x {iters} "
+              f"reorth {t_reorth:.3f}s -> {T:.1f}s per solve, K={plan.order}", file=sys.stderr)
+    return {
+        "value": nev / T, "unit": "eigenpairs/s", "cores": threads, "kind": "port",
+        "sample": (f"CPU port of the reference path (oracle: C/OpenMP CSR kernels + numpy) on one realisation: "
+                   f"2 Emin/Emax Lanczos probes timed in full ({t_ext:.2f}s), KPM on {kpm_probes} of "
+                   f"{WORKLOAD['dos_R']} probes scaled x{WORKLOAD['dos_R'] / kpm_probes:.0f} ({t_kpm:.2f}s), one "
+                   f"K={plan.order} filter on s={s} ({t_filter:.3f}s) and one reorthogonalisation "
+                   f"({t_reorth:.3f}s) scaled x{iters} iterations; {nev} pairs per estimated {T:.1f}s solve"),
+        "seconds_per_solve": T,
+    }
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the CPU implementation of the path on this host."""
+    if rank != 0:
+        return 0
+    vals, per = [], None
+    for i in range(args.warmup + args.steps):
+        per = cpu_sample(seed=4242 + i)
+        if i >= args.warmup:
+            vals.append(per["value"])
+    v = statistics.median(vals)
+    cb = dict(per)
+    cb["value"] = v
+    cb.pop("seconds_per_solve", None)
+    out = {
+        "metric": "converged eigenpairs/s at resid<=1e-10", "value": v, "unit": "eigenpairs/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * WORKLOAD["nev"] / v, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded realisations)",
+        "config": dict(WORKLOAD), "impl": "reference", "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# -------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import __graft_entry__ as ge
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    pkg = ge.load_package()
+    from polfed_b200 import _lib
+    pkg.load_library()
+    nsteps = args.warmup + args.steps
+    ops, x0s = make_realisations(pkg, nsteps, 1000 + 7919 * rank, device=local_rank)
+    handle = _lib.handle(local_rank)
+    stream = torch.cuda.ExternalStream(_lib.stream_of(handle), device=dev)
+    # set-up outside the timed region: device descriptors, tuned step width, device x0
+    width, _ = pkg.autotune(ops[0], WORKLOAD["blocksize"], "fp64")
+    for o in ops[1:]:
+        pkg.autotune(o, WORKLOAD["blocksize"], "fp64")
+    x0_dev = []
+    for x in x0s:
+        t = pkg.col_major(x.shape[0], x.shape[1], device=local_rank)
+        t.copy_(torch.from_numpy(np.ascontiguousarray(x)).to(dev))
+        x0_dev.append(t)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def reduce(x, op):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    for i in range(args.warmup):
+        solve(pkg, ops[i], x0_dev[i], seed=17 + i)
+    torch.cuda.synchronize()
+
+    def timed(host_inputs):
+        sampler = ClockSampler(local_rank)
+        barrier()
+        torch.cuda.synchronize()
+        sampler.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        nconv, reps = [], []
+        w0 = time.perf_counter()
+        e0.record(stream)
+        for k in range(args.steps):
+            i = args.warmup + k
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))  # evict the previous solve's blocks from L2
+            x = x0s[i] if host_inputs else x0_dev[i]
+            vals, vecs, rep = solve(pkg, ops[i], x, seed=17 + i)
+            nconv.append(len(vals))
+            reps.append(rep)
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - w0
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop()
+        return nconv, e0.elapsed_time(e1) * 1e-3, wall, reps, clocks
+
+    nconv, sec, wall, reps, clocks = timed(host_inputs=False)
+    sec_max = reduce(sec, dist.ReduceOp.MAX if world > 1 else None)
+    value = reduce(float(sum(nconv)), dist.ReduceOp.SUM if world > 1 else None) / sec_max
+    e_nconv, e_sec, e_wall, e_reps, e_clocks = timed(host_inputs=True)
+    e_value = reduce(float(sum(e_nconv)), dist.ReduceOp.SUM if world > 1 else None) / \
+        reduce(e_sec, dist.ReduceOp.MAX if world > 1 else None)
+    D, s = ops[0].dim, WORKLOAD["blocksize"]
+
+    # roofline of the Clenshaw step from the library's CUDA-event stage timers
+    step_time, steps_total = 0.0, 0
+    for r in reps:
+        step_time += r.benchmark.stage_seconds["mapping"]
+        steps_total += r.factorization.itersneeded * (r.spectral.order + 1)
+    avg_step = step_time / max(steps_total, 1)
+    alg_bytes = 4.0 * D * s * 8
+    achieved = alg_bytes / avg_step / 1e9
+    peak, peak_kind = read_peaks()
+    launches = sum(r.benchmark.kernel_launches for r in reps)
+    stages = {k: sum(r.benchmark.stage_seconds[k] for r in reps) / len(reps) for k in reps[0].benchmark.stage_seconds}
+    if rank != 0:
+        return 0
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample()
+        cpu.pop("seconds_per_solve", None)
+    out = {
+        "metric": "converged eigenpairs/s at resid<=1e-10", "value": value, "unit": "eigenpairs/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sec_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded disorder realisations, one per step)",
+        "config": dict(WORKLOAD, **{"l2": "256 MB buffer written between solves (inside the timed region)",
+                                    "step": "one full POLFED solve", "parallelism": f"replicas x{world}",
+                                    "step_width": width}),
+        "e2e": {"value": e_value, "unit": "eigenpairs/s", "h2d_bytes_per_step": D * s * 8,
+                "d2h_bytes_per_step": int(statistics.mean(e_nconv) * (D * 8 + 8)), "wall_seconds": e_wall},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_step (Clenshaw recurrence)", "achieved": achieved,
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": read_traffic(), "algorithmic_bytes_per_launch": alg_bytes,
+                     "avg_launch_us": avg_step * 1e6},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "e2e_clocks": e_clocks,
+        "converged_per_step": statistics.mean(nconv),
+        "stage_seconds_per_solve": stages,
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

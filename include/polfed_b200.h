@@ -205,6 +205,7 @@ typedef struct pf_report {
      * 6 Emin/Emax probes, 7 KPM DoS, 8 bounds+order, 9 total */
     double  stage_seconds[10];
     double  basis_bytes_reserved, basis_bytes_used;
+    int64_t kernel_launches;            /* this library's kernel launches in the solve */
 } pf_report;
 
 void pf_params_default(pf_params *p);

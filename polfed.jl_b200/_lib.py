@@ -81,6 +81,7 @@ class pf_report(ctypes.Structure):
         ("maxresidual_history", ctypes.c_double * PF_REPORT_MAX_CHECKS),
         ("stage_seconds", ctypes.c_double * 10),
         ("basis_bytes_reserved", ctypes.c_double), ("basis_bytes_used", ctypes.c_double),
+        ("kernel_launches", ctypes.c_int64),
     ]
 
 

@@ -160,6 +160,7 @@ class BenchmarkReport:
     basis_bytes_reserved: float
     basis_bytes_used: float
     kpm_block_matvecs: int
+    kernel_launches: int
 
 
 @dataclass
@@ -184,7 +185,7 @@ def _make_report(r: _lib.pf_report, kind: int, value: float) -> Report:
                               r.numofchecks, list(r.converged_history[:n]), list(r.krylovdim_history[:n]),
                               list(r.maxresidual_history[:n]))
     bench = BenchmarkReport({k: r.stage_seconds[i] for i, k in enumerate(STAGES)}, r.basis_bytes_reserved,
-                            r.basis_bytes_used, int(r.kpm_block_matvecs))
+                            r.basis_bytes_used, int(r.kpm_block_matvecs), int(r.kernel_launches))
     return Report(spec, fac, bench)
 
 
@@ -265,41 +266,76 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
            precision: str = "fp64", vecs: bool = True):
     """POLFED on the B200 (PolfedCore.jl:194-263).
 
-    ``x0`` is a host array, D (scalar Lanczos) or D x s (block Lanczos); a
-    non-normalised / non-orthonormal start is replaced by a normalised copy,
-    as the reference does.  Returns ``(vals, vecs)`` or
-    ``(vals, vecs, report)``: the converged eigenpairs, ascending."""
+    ``x0`` is D (scalar Lanczos) or D x s (block Lanczos): a host array, or a
+    column-major float64 CUDA tensor (then the eigenvectors are returned as a
+    column-major CUDA tensor and never leave HBM).  A non-normalised /
+    non-orthonormal start is replaced by a normalised copy, as the reference
+    does.  Returns ``(vals, vecs)`` or ``(vals, vecs, report)``: the converged
+    eigenpairs, ascending."""
     mapping = mapping or MappingConfig()
     transform = transform or TransformConfig()
     fact = fact or FactorizationConfig()
     dos = dos or DoSConfig()
     if howmany < 1:
         raise ValueError("howmany must be positive")
-    x = np.asarray(x0, dtype=np.float64)
-    if x.ndim not in (1, 2):
-        raise ValueError("x0 must be a vector or a matrix")
     D = op.dim
-    if x.shape[0] != D:
-        raise ValueError(f"x0 has {x.shape[0]} rows; the operator dimension is {D}")
-    if x.size == 0:
-        raise ValueError("POLFED initial vector must not be empty.")
-    s = 1 if x.ndim == 1 else x.shape[1]
-    xf = np.asfortranarray(x.reshape(D, s))
+    on_device = _is_cuda_tensor(x0)
+    if on_device:
+        # device path: x0 and the eigenvectors stay in HBM (column-major CUDA tensors)
+        import torch
+        if x0.dtype != torch.float64:
+            raise ValueError("x0 must be float64")
+        if x0.dim() == 1:
+            s = 1
+            if x0.shape[0] != D or x0.stride(0) != 1:
+                raise ValueError(f"x0 must be a contiguous vector of length {D}")
+        elif x0.dim() == 2:
+            s = x0.shape[1]
+            if x0.shape[0] != D or x0.stride(0) != 1 or x0.stride(1) != D:
+                raise ValueError(f"x0 must be a column-major {D} x s CUDA tensor")
+        else:
+            raise ValueError("x0 must be a vector or a matrix")
+        x_ptr, x_mem = x0.data_ptr(), _lib.PF_MEM_DEVICE
+        V = col_major(D, howmany, device=x0.device.index or 0) if vecs else None
+        v_ptr, v_mem = (V.data_ptr() if vecs else None), _lib.PF_MEM_DEVICE
+        keep_x = x0
+    else:
+        x = np.asarray(x0, dtype=np.float64)
+        if x.ndim not in (1, 2):
+            raise ValueError("x0 must be a vector or a matrix")
+        if x.shape[0] != D:
+            raise ValueError(f"x0 has {x.shape[0]} rows; the operator dimension is {D}")
+        if x.size == 0:
+            raise ValueError("POLFED initial vector must not be empty.")
+        s = 1 if x.ndim == 1 else x.shape[1]
+        keep_x = np.asfortranarray(x.reshape(D, s))
+        x_ptr, x_mem = keep_x.ctypes.data, _lib.PF_MEM_HOST
+        V = np.zeros((D, howmany), order="F") if vecs else None
+        v_ptr, v_mem = (V.ctypes.data if vecs else None), _lib.PF_MEM_HOST
     p, keep, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
     vals = np.zeros(howmany)
-    V = np.zeros((D, howmany), order="F") if vecs else None
     rep = _lib.pf_report()
     n = ctypes.c_int(0)
-    _lib.check(_lib.load().pf_solve(op.op, ctypes.byref(p), s, howmany, xf.ctypes.data, _lib.PF_MEM_HOST,
-                                    vals.ctypes.data, V.ctypes.data if vecs else None, _lib.PF_MEM_HOST,
-                                    ctypes.byref(rep), ctypes.byref(n)))
-    del keep
+    _lib.check(_lib.load().pf_solve(op.op, ctypes.byref(p), s, howmany, x_ptr, x_mem, vals.ctypes.data, v_ptr,
+                                    v_mem, ctypes.byref(rep), ctypes.byref(n)))
+    del keep, keep_x
     k = n.value
     out_vals = vals[:k].copy()
-    out_vecs = V[:, :k].copy() if vecs else None
+    if vecs:
+        out_vecs = V[:, :k] if on_device else V[:, :k].copy()
+    else:
+        out_vecs = None
     if produce_report:
         return out_vals, out_vecs, _make_report(rep, kind, val)
     return out_vals, out_vecs
+
+
+def _is_cuda_tensor(x) -> bool:
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        return False
+    return isinstance(x, torch.Tensor) and x.is_cuda
 
 
 def lanczos_extrema(op: Operator, x0, maxdim: int = 1000, tol: float = 1e-14, eigentol: float = 1e-8):

@@ -194,4 +194,10 @@ int grid_for(pf_handle *h, int64_t work_items, int threads, int blocks_per_sm);
 
 void ensure_reduction(pf_handle *h, size_t n);
 
+// Launches of this library's kernels issued by the calling host thread (a
+// graph replay counts every kernel node).  A solve runs on one host thread, so
+// the difference across a solve is exactly that solve's launches.
+void count_launches(int64_t n);
+int64_t thread_launches();
+
 }  // namespace pf

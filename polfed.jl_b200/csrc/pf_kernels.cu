@@ -364,6 +364,10 @@ __global__ void __launch_bounds__(kThreads) k_step(const Desc d, const StepArgs<
     }
 }
 
+static thread_local int64_t t_launches = 0;
+void count_launches(int64_t n) { t_launches += n; }
+int64_t thread_launches() { return t_launches; }
+
 int grid_for(pf_handle *h, int64_t work_items, int threads, int blocks_per_sm) {
     int64_t need = (work_items + threads - 1) / threads;
     int64_t cap = (int64_t)h->num_sms * blocks_per_sm;
@@ -413,6 +417,7 @@ static void launch_one(pf_op *op, cudaStream_t st, const Desc &d, StepArgs<T> a,
     }
     kern<<<grid, kThreads, smem, st>>>(d, a);
     PF_CUDA(cudaGetLastError());
+    count_launches(1);
 }
 
 template <typename T, int V, class Desc>
@@ -573,12 +578,14 @@ template <typename TS, typename TD>
 void launch_cm_to_ri(cudaStream_t st, int64_t D, int s, const TS *src, int64_t ld, TD *dst) {
     dim3 grid((unsigned)((D + 31) / 32), (unsigned)((s + 31) / 32));
     k_cm_to_ri<TS, TD><<<grid, dim3(32, 8), 0, st>>>((uint32_t)D, s, src, ld, dst);
+    count_launches(1);
     PF_CUDA(cudaGetLastError());
 }
 template <typename TS, typename TD>
 void launch_ri_to_cm(cudaStream_t st, int64_t D, int s, const TS *src, TD *dst, int64_t ld) {
     dim3 grid((unsigned)((D + 31) / 32), (unsigned)((s + 31) / 32));
     k_ri_to_cm<TS, TD><<<grid, dim3(32, 8), 0, st>>>((uint32_t)D, s, src, dst, ld);
+    count_launches(1);
     PF_CUDA(cudaGetLastError());
 }
 template void launch_cm_to_ri<double, double>(cudaStream_t, int64_t, int, const double *, int64_t, double *);
@@ -666,6 +673,7 @@ void launch_coldots(pf_handle *h, cudaStream_t st, int64_t D, int s, const T *A,
         size_t smem = (kThreads + s) * sizeof(double);
         k_coldots_narrow<T><<<grid, kThreads, smem, st>>>((uint32_t)D, s, A, B, h->red_partials,
                                                           h->red_counter, out);
+        count_launches(1);
     } else {
         uint32_t rpb = 64;
         int grid = (int)((D + rpb - 1) / rpb);
@@ -678,6 +686,7 @@ void launch_coldots(pf_handle *h, cudaStream_t st, int64_t D, int s, const T *A,
         if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(k_coldots<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_coldots<T><<<grid, kThreads, smem, st>>>((uint32_t)D, s, rpb, A, B, h->red_partials,
                                                    h->red_counter, out);
+        count_launches(1);
     }
     PF_CUDA(cudaGetLastError());
 }
@@ -696,6 +705,7 @@ void launch_colresid(pf_handle *h, cudaStream_t st, int64_t D, int s, const doub
     size_t smem = s * sizeof(double);
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(k_colresid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_colresid<<<grid, kThreads, smem, st>>>((uint32_t)D, s, rpb, HA, A, e, h->red_partials, h->red_counter, out);
+    count_launches(1);
     PF_CUDA(cudaGetLastError());
 }
 
@@ -735,6 +745,7 @@ template <typename T>
 void launch_probes(cudaStream_t st, int64_t D, int R, int kind, uint64_t seed, int col0, T *dst) {
     int grid = (int)std::min<int64_t>((D * R + 255) / 256, 148 * 8);
     k_probes<T><<<grid, 256, 0, st>>>((uint32_t)D, R, kind, seed, col0, dst);
+    count_launches(1);
     PF_CUDA(cudaGetLastError());
 }
 template void launch_probes<double>(cudaStream_t, int64_t, int, int, uint64_t, int, double *);
@@ -753,6 +764,7 @@ template <typename T>
 void launch_scale_cols(cudaStream_t st, int64_t D, int s, T *A, const double *scale) {
     int grid = (int)std::min<int64_t>((D * s + 255) / 256, 148 * 8);
     k_scale_cols<T><<<grid, 256, 0, st>>>((uint32_t)D, s, A, scale);
+    count_launches(1);
     PF_CUDA(cudaGetLastError());
 }
 template void launch_scale_cols<double>(cudaStream_t, int64_t, int, double *, const double *);
@@ -792,6 +804,7 @@ void launch_unrank(pf_op *op, cudaStream_t st, int64_t n, const int64_t *idx, ui
     if (n <= 0) return;
     int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
     k_unrank<<<grid, 256, 0, st>>>((uint64_t)n, op->chain64.full, (uint32_t)op->dim, op->d_states, idx, out);
+    count_launches(1);
     PF_CUDA(cudaGetLastError());
 }
 
@@ -802,6 +815,7 @@ void launch_rank(pf_op *op, cudaStream_t st, int64_t n, const uint64_t *states, 
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(k_rank, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 4);
     k_rank<<<grid, 256, smem, st>>>((uint64_t)n, d.L, d.Lup, d.full, d.nchunks, op->d_rank_tab, states, out);
+    count_launches(1);
     PF_CUDA(cudaGetLastError());
 }
 

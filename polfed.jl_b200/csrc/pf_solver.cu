@@ -120,8 +120,10 @@ struct Filter {
     void run(cudaStream_t st) {
         if (!exec) {
             PF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            const int64_t before = thread_launches();  // captured launches do not execute
             try {
                 enqueue(st);
+                count_launches(before - thread_launches());
             } catch (...) {
                 cudaGraph_t g;
                 cudaStreamEndCapture(st, &g);
@@ -132,6 +134,7 @@ struct Filter {
             PF_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         }
         PF_CUDA(cudaGraphLaunch(exec, st));
+        count_launches(K + 1);
     }
 };
 
@@ -697,6 +700,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
              "POLFED initial matrix cannot have orthonormal columns when it has more columns than rows.");
     pf_report R;
     std::memset(&R, 0, sizeof(R));
+    const int64_t launches0 = thread_launches();
     cudaEvent_t t_begin, t_end;
     PF_CUDA(cudaEventCreate(&t_begin));
     PF_CUDA(cudaEventCreate(&t_end));
@@ -865,6 +869,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
         R.stage_seconds[9] = tot_ms * 1e-3;
         R.basis_bytes_reserved = (double)D * out.maxiter * s * sizeof(double);
         R.basis_bytes_used = (double)D * out.krylovdim * sizeof(double);
+        R.kernel_launches = thread_launches() - launches0;
         *rep = R;
     }
 }
