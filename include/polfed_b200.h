@@ -128,6 +128,18 @@ int pf_apply(pf_op *op, int dtype, double a, double b, int s,
 /* b1 = c X + 2 Htilde b2 - b3       (clenshaw_recurrence, vector_dispatch.jl:120-124) */
 int pf_clenshaw_recurrence(pf_op *op, int dtype, double a, double b, double c, int s,
                            void *b1, const void *b2, const void *b3, const void *X, int64_t ld);
+/* Same result as pf_apply, for callers that cannot let a library allocate
+ * device memory (a CuArray / caching-allocator pool that owns the HBM budget,
+ * or a loop that cannot absorb cudaMalloc's implicit synchronisation).  This
+ * entry point has no counterpart in the reference.  It never allocates: blocks
+ * with s > 1 are staged in one fixed 16 MiB device array built into the
+ * library (held by every GPU that loads it until exit), so 2*D*s*element_size
+ * must not exceed 16 MiB -- larger blocks are rejected with PF_ERR_INVALID.
+ * The array's device address is looked up inside the first call on each
+ * device; make that first call before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be ordered by the caller. */
+int pf_apply_noalloc(pf_op *op, int dtype, double a, double b, int s,
+                     const void *X, int64_t ldx, void *Y, int64_t ldy);
 /* Y = c0 X + Htilde b1 - b2        (clenshaw_finalsum, vector_dispatch.jl:134-137) */
 int pf_clenshaw_finalsum(pf_op *op, int dtype, double a, double b, double c0, int s,
                          const void *b1, const void *b2, void *Y, const void *X, int64_t ld);

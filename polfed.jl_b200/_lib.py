@@ -32,7 +32,7 @@ EXPORTED = [
     "pf_handle_synchronize", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_destroy",
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
-    "pf_lanczos_extrema", "pf_autotune",
+    "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc",
 ]
 
 
@@ -111,6 +111,7 @@ def load():
         "pf_basis_unrank": (i32, [vp, i64, vp, vp]),
         "pf_basis_rank": (i32, [vp, i64, vp, vp]),
         "pf_apply": (i32, [vp, i32, f64, f64, i32, vp, i64, vp, i64]),
+        "pf_apply_noalloc": (i32, [vp, i32, f64, f64, i32, vp, i64, vp, i64]),
         "pf_clenshaw_recurrence": (i32, [vp, i32, f64, f64, f64, i32, vp, vp, vp, vp, i64]),
         "pf_clenshaw_finalsum": (i32, [vp, i32, f64, f64, f64, i32, vp, vp, vp, vp, i64]),
         "pf_filter": (i32, [vp, i32, f64, f64, i32, vp, i32, vp, i64, vp, i64]),

@@ -147,6 +147,14 @@ int pf_apply(pf_op *op, int dtype, double a, double b, int s, const void *X, int
     PF_API_END
 }
 
+int pf_apply_noalloc(pf_op *op, int dtype, double a, double b, int s, const void *X, int64_t ldx, void *Y,
+                     int64_t ldy) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::op_apply_noalloc(op, dtype, a, b, s, X, ldx, Y, ldy);
+    PF_API_END
+}
+
 int pf_clenshaw_recurrence(pf_op *op, int dtype, double a, double b, double c, int s, void *b1, const void *b2,
                            const void *b3, const void *X, int64_t ld) {
     PF_API_BEGIN

@@ -15,6 +15,8 @@ void destroy_op(pf_op *op);
 void *handle_scratch(pf_handle *h, size_t bytes);
 
 void op_apply(pf_op *op, int dtype, double a, double b, int s, const void *X, int64_t ldx, void *Y, int64_t ldy);
+void op_apply_noalloc(pf_op *op, int dtype, double a, double b, int s, const void *X, int64_t ldx, void *Y,
+                      int64_t ldy);
 void op_recurrence(pf_op *op, int dtype, double a, double b, double c, int s, void *b1, const void *b2,
                    const void *b3, const void *X, int64_t ld);
 void op_finalsum(pf_op *op, int dtype, double a, double b, double c0, int s, const void *b1, const void *b2,
