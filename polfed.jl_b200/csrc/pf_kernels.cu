@@ -72,16 +72,27 @@ __device__ __forceinline__ uint32_t sector_rank(uint32_t st, const uint32_t *tab
 // thread keeps several L2/HBM requests in flight (the loop bodies have no
 // load-to-load dependence); accumulation follows the reference's term order.
 // U shrinks as the per-thread column count V grows, to bound registers.
-template <int V>
+template <typename T, int V>
 struct Batch {
-    static constexpr int U = V >= 16 ? 2 : (V >= 8 ? 4 : 8);
+    static constexpr int bytes = V * (int)sizeof(T);
+    static constexpr int U = bytes >= 64 ? 2 : (bytes >= 16 ? 4 : 8);
+};
+
+// Resident CTAs per SM the step kernel is compiled for: caps registers so
+// enough warps stay resident to cover L2 latency with independent gathers
+// (with no cap the 64-byte-per-thread variants took 170 registers, one CTA
+// per SM, 8 warps -- latency-bound).
+template <typename T, int V>
+struct MinBlocks {
+    static constexpr int bytes = V * (int)sizeof(T);
+    static constexpr int value = bytes >= 32 ? 2 : 3;
 };
 
 template <typename T, int V, bool HASQ>
 __device__ __forceinline__ void chain_row(const ChainDesc<T> &d, const uint32_t *tab, uint32_t row,
                                           int s, int c0, const T *__restrict__ q, T (&acc)[V],
                                           T &diag) {
-    constexpr int U = Batch<V>::U;
+    constexpr int U = Batch<T, V>::U;
     const uint32_t st = d.full ? row : __ldg(d.states + row);
     T dg = T(0);
     for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
@@ -136,7 +147,7 @@ template <typename T, int V, bool HASQ>
 __device__ __forceinline__ void qsun_row(const QSunDesc<T> &d, const T *smem_t, uint32_t row,
                                          int s, int c0, const T *__restrict__ q, T (&acc)[V],
                                          T &diag) {
-    constexpr int U = Batch<V>::U;
+    constexpr int U = Batch<T, V>::U;
     const int gs = d.dg + 1;
     const T *dtab = smem_t + d.dg * gs;
     const uint32_t outer = row >> d.L_grain;
@@ -235,7 +246,7 @@ __device__ void finish_reduction(int nvals, const double *blockvals, double *par
 }
 
 template <typename T, int V, class Desc, int FLAGS>
-__global__ void __launch_bounds__(kThreads) k_step(const Desc d, const StepArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, MinBlocks<T, V>::value) k_step(const Desc d, const StepArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool HASQ = (FLAGS & StepFlags::Q) != 0;
     constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
@@ -519,7 +530,11 @@ void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const
         auto it = op->tuned_width.find(std::make_pair((int)sizeof(T), s));
         if (it != op->tuned_width.end()) V = it->second;
     }
-    if ((flags & StepFlags::DOTS) && kThreads % (s / V) != 0) V = default_width(s, (int)sizeof(T));
+    if (flags & StepFlags::DOTS) {
+        // the fused dots keep 2V FP64 accumulators per thread: at most 32 bytes of columns
+        V = default_width(s, (int)sizeof(T));
+        while (V * (int)sizeof(T) > 32 || kThreads % (s / V) != 0) V /= 2;
+    }
     launch_step_width<T>(op, st, D, s, q, p, x, out, cx, alpha, beta, inva, shift, flags, dots, V);
 }
 
