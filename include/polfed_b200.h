@@ -109,6 +109,12 @@ int pf_op_spin_chain_create(pf_handle *h, int L, int Lup, int nbonds, const int3
 int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup,
                       const int32_t *nbr, const double *fields, const double *grain,
                       pf_op **out);
+/* A view of op that runs on handle h (same device).  It shares op's device
+ * tables, so several host threads can solve concurrently, each on its own
+ * handle / stream.  Destroy views and the original in any order; the tables
+ * are freed with the last of them.  (No reference counterpart: the reference
+ * runs one solve at a time.) */
+int     pf_op_bind(const pf_op *op, pf_handle *h, pf_op **out);
 int     pf_op_destroy(pf_op *op);
 int64_t pf_op_dim(const pf_op *op);
 

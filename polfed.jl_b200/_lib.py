@@ -32,7 +32,7 @@ EXPORTED = [
     "pf_handle_synchronize", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_destroy",
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
-    "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc",
+    "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind",
 ]
 
 
@@ -107,6 +107,7 @@ def load():
         "pf_op_spin_chain_create": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_qsun_create": (i32, [vp, i32, i32, f64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_destroy": (i32, [vp]),
+        "pf_op_bind": (i32, [vp, vp, ctypes.POINTER(vp)]),
         "pf_op_dim": (i64, [vp]),
         "pf_basis_unrank": (i32, [vp, i64, vp, vp]),
         "pf_basis_rank": (i32, [vp, i64, vp, vp]),
@@ -150,6 +151,13 @@ def handle(device: int = 0) -> int:
         check(load().pf_handle_create(device, ctypes.byref(h)))
         _HANDLES[device] = h.value
     return _HANDLES[device]
+
+
+def new_handle(device: int = 0) -> int:
+    """A fresh handle (own stream, cuBLAS / cuSOLVER handles, workspaces)."""
+    h = ctypes.c_void_p()
+    check(load().pf_handle_create(device, ctypes.byref(h)))
+    return h.value
 
 
 def stream_of(h: int) -> int:

@@ -330,6 +330,49 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
     return out_vals, out_vecs
 
 
+_WORKERS: dict = {}
+
+
+def worker_handles(n: int, device: int = 0):
+    """n process-wide worker handles of a device (each its own stream)."""
+    hs = _WORKERS.setdefault(device, [])
+    while len(hs) < n:
+        hs.append(_lib.new_handle(device))
+    return hs[:n]
+
+
+def polfed_batch(ops, x0s, howmany: int, target, *, workers: int = 4, **kwargs):
+    """Solve many independent problems (e.g. disorder realisations) with
+    ``workers`` solves in flight at once, each on its own handle / stream, so
+    their latency-bound launches and host round trips overlap on the GPU.
+    Returns one ``polfed`` result tuple per problem, in order."""
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+    if len(ops) != len(x0s):
+        raise ValueError("one x0 per operator is required")
+    if not ops:
+        return []
+    hs = worker_handles(max(1, min(workers, len(ops))), ops[0].device)
+    free = list(range(len(hs)))
+    lock = threading.Lock()
+
+    def run(i):
+        with lock:
+            slot = free.pop()
+        try:
+            view = ops[i].bind(hs[slot])
+            try:
+                return polfed(view, x0s[i], howmany, target, **kwargs)
+            finally:
+                view.close()
+        finally:
+            with lock:
+                free.append(slot)
+
+    with ThreadPoolExecutor(max_workers=len(hs)) as ex:
+        return list(ex.map(run, range(len(ops))))
+
+
 def _is_cuda_tensor(x) -> bool:
     try:
         import torch

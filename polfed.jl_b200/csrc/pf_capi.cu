@@ -114,6 +114,13 @@ int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const dou
     PF_API_END
 }
 
+int pf_op_bind(const pf_op *op, pf_handle *h, pf_op **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    *out = pf::bind_op(op, h);
+    PF_API_END
+}
+
 int pf_op_destroy(pf_op *op) {
     PF_API_BEGIN
     pf::destroy_op(op);

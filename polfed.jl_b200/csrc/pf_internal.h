@@ -6,6 +6,7 @@
 #include <cusolverDn.h>
 #include <stdint.h>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -126,6 +127,8 @@ struct pf_op {
     pf::QSunDesc<float> qsun32;
     uint32_t *d_states = nullptr;
     uint32_t *d_rank_tab = nullptr;
+    // owns d_states / d_rank_tab; shared with the views pf_op_bind makes on other handles
+    std::shared_ptr<void> tables_owner;
     int smem_bytes = 0;               // dynamic shared memory of the step kernels
     // autotuned columns-per-thread of the step kernel, keyed by (element bytes, s)
     std::mutex tune_mu;

@@ -533,7 +533,7 @@ void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const
     if (flags & StepFlags::DOTS) {
         // the fused dots keep 2V FP64 accumulators per thread: at most 32 bytes of columns
         V = default_width(s, (int)sizeof(T));
-        while (V * (int)sizeof(T) > 32 || kThreads % (s / V) != 0) V /= 2;
+        while (V > 1 && (V * (int)sizeof(T) > 32 || kThreads % (s / V) != 0)) V /= 2;
     }
     launch_step_width<T>(op, st, D, s, q, p, x, out, cx, alpha, beta, inva, shift, flags, dots, V);
 }

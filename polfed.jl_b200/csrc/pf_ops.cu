@@ -130,12 +130,21 @@ pf_op *create_spin_chain(pf_handle *h, int L, int Lup, int nbonds, const int32_t
             std::vector<uint32_t> tab = build_rank_tables(nchunks);
             PF_CUDA(cudaMalloc(&op->d_rank_tab, tab.size() * sizeof(uint32_t)));
             PF_CUDA(cudaMemcpy(op->d_rank_tab, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+            uint32_t *tst = op->d_states, *trk = op->d_rank_tab;
+            const int dev = h->device;
+            op->tables_owner = std::shared_ptr<void>(nullptr, [tst, trk, dev](void *) {
+                cudaSetDevice(dev);
+                cudaFree(tst);
+                cudaFree(trk);
+            });
         }
         fill_chain(op->chain64, op);
         fill_chain(op->chain32, op);
     } catch (...) {
-        if (op->d_states) cudaFree(op->d_states);
-        if (op->d_rank_tab) cudaFree(op->d_rank_tab);
+        if (!op->tables_owner) {
+            if (op->d_states) cudaFree(op->d_states);
+            if (op->d_rank_tab) cudaFree(op->d_rank_tab);
+        }
         delete op;
         throw;
     }
@@ -179,10 +188,41 @@ pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double
 
 void destroy_op(pf_op *op) {
     if (!op) return;
-    if (op->h) cudaSetDevice(op->h->device);
-    if (op->d_states) cudaFree(op->d_states);
-    if (op->d_rank_tab) cudaFree(op->d_rank_tab);
-    delete op;
+    delete op;  // the device tables go with the last operator sharing them
+}
+
+pf_op *bind_op(const pf_op *src, pf_handle *h) {
+    PF_CHECK(src && h, PF_ERR_INVALID, "null argument");
+    PF_CHECK(src->h->device == h->device, PF_ERR_INVALID, "an operator can only be bound to a handle of its device");
+    pf_op *op = new pf_op();
+    op->h = h;
+    op->kind = src->kind;
+    op->dim = src->dim;
+    op->L = src->L;
+    op->Lup = src->Lup;
+    op->chain64 = src->chain64;
+    op->chain32 = src->chain32;
+    op->qsun64 = src->qsun64;
+    op->qsun32 = src->qsun32;
+    op->d_states = src->d_states;
+    op->d_rank_tab = src->d_rank_tab;
+    op->tables_owner = src->tables_owner;
+    op->smem_bytes = src->smem_bytes;
+    {
+        std::lock_guard<std::mutex> lock(const_cast<pf_op *>(src)->tune_mu);
+        op->tuned_width = src->tuned_width;
+    }
+    op->bonds = src->bonds;
+    op->J = src->J;
+    op->Delta = src->Delta;
+    op->fields = src->fields;
+    op->coup = src->coup;
+    op->grain = src->grain;
+    op->nbr = src->nbr;
+    op->g0 = src->g0;
+    op->L_loc = src->L_loc;
+    op->L_grain = src->L_grain;
+    return op;
 }
 
 // ------------------------------------------------------- handle scratch

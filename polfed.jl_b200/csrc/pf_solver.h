@@ -12,6 +12,7 @@ pf_op *create_spin_chain(pf_handle *h, int L, int Lup, int nbonds, const int32_t
 pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup, const int32_t *nbr,
                    const double *fields, const double *grain);
 void destroy_op(pf_op *op);
+pf_op *bind_op(const pf_op *src, pf_handle *h);
 void *handle_scratch(pf_handle *h, size_t bytes);
 
 void op_apply(pf_op *op, int dtype, double a, double b, int s, const void *X, int64_t ldx, void *Y, int64_t ldy);

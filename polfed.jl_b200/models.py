@@ -95,6 +95,11 @@ class Operator:
     def shape(self):
         return (self.dim, self.dim)
 
+    def bind(self, handle: int) -> "BoundOperator":
+        """A view of this operator that runs on another handle (stream) of the
+        same device; it shares the device tables (pf_op_bind)."""
+        return BoundOperator(self, handle)
+
     def close(self) -> None:
         if self._op is not None:
             _lib.load().pf_op_destroy(self._op)
@@ -105,6 +110,23 @@ class Operator:
             self.close()
         except Exception:
             pass
+
+
+class BoundOperator(Operator):
+    """An operator view bound to a specific handle (see Operator.bind)."""
+
+    def __init__(self, base: Operator, handle: int):
+        super().__init__(base.device)
+        self.base = base
+        self.kind = base.kind
+        self._handle = handle
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().pf_op_bind(base.op, handle, ctypes.byref(out)))
+        self._op = out.value
+
+    @property
+    def handle(self) -> int:
+        return self._handle
 
 
 class SpinChainOperator(Operator):
