@@ -43,6 +43,14 @@ int pf_handle_create(int device, pf_handle **out) {
     PF_CUDA(cudaGetDeviceCount(&ndev));
     PF_CHECK(device >= 0 && device < ndev, PF_ERR_INVALID, "no such CUDA device");
     PF_CUDA(cudaSetDevice(device));
+    {
+        // solver workspaces are allocated stream-ordered from the device pool;
+        // keep freed memory in the pool so later allocations never synchronise
+        cudaMemPool_t pool;
+        PF_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = UINT64_MAX;
+        PF_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     cudaDeviceProp prop;
     PF_CUDA(cudaGetDeviceProperties(&prop, device));
     PF_CHECK(prop.major >= 10, PF_ERR_UNSUPPORTED, "libpolfed_b200 is built for sm_100a (B200) only");

@@ -14,19 +14,38 @@
 namespace pf {
 
 // ------------------------------------------------------------- utilities
+// Stream of the entry point running on this host thread.  DevArray allocates
+// stream-ordered on it (cudaMallocAsync from the device pool, which keeps
+// freed memory), so solves in flight on other handles are never stalled by a
+// cudaMalloc / cudaFree device synchronisation.
+static thread_local cudaStream_t t_alloc_stream = nullptr;
+struct AllocStream {
+    cudaStream_t prev;
+    explicit AllocStream(cudaStream_t st) : prev(t_alloc_stream) { t_alloc_stream = st; }
+    ~AllocStream() { t_alloc_stream = prev; }
+};
+
 template <typename T>
 struct DevArray {
     T *p = nullptr;
     size_t n = 0;
+    cudaStream_t st = nullptr;
     DevArray() = default;
     explicit DevArray(size_t count) { alloc(count); }
     void alloc(size_t count) {
         free();
-        if (count) PF_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        st = t_alloc_stream;
+        if (count) {
+            if (st) PF_CUDA(cudaMallocAsync((void **)&p, count * sizeof(T), st));
+            else PF_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        }
         n = count;
     }
     void free() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (st) cudaFreeAsync(p, st);
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
     }
@@ -597,6 +616,7 @@ void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, d
     PF_CHECK(nrm > 0 && std::isfinite(nrm), PF_ERR_INVALID, "lanczos_extrema requires a nonzero starting vector.");
     for (double &v : seed) v /= nrm;
     PF_CUDA(cudaSetDevice(op->h->device));
+    AllocStream alloc_guard(op->h->stream);
     DevArray<double> v0(D);
     PF_CUDA(cudaMemcpyAsync(v0.p, seed.data(), D * sizeof(double), cudaMemcpyHostToDevice, op->h->stream));
     extrema_from_device(op, v0.p, maxdim, tol, eigentol, Emin, Emax, nullptr);
@@ -609,6 +629,7 @@ void op_filter(pf_op *op, int dtype, double a, double b, int K, const double *co
     PF_CHECK(ldx >= op->dim && ldy >= op->dim, PF_ERR_INVALID, "leading dimension smaller than D");
     PF_CHECK(a != 0.0 && std::isfinite(a) && std::isfinite(b), PF_ERR_INVALID, "rescaling a must be finite and nonzero");
     PF_CUDA(cudaSetDevice(op->h->device));
+    AllocStream alloc_guard(op->h->stream);
     std::vector<double> c(coeffs, coeffs + K + 1);
     cudaStream_t st = op->h->stream;
     const int64_t D = op->dim;
@@ -634,6 +655,7 @@ void op_kpm(pf_op *op, int dtype, double a, double b, int N, int R, const void *
     PF_CHECK(a != 0.0 && std::isfinite(a) && std::isfinite(b), PF_ERR_INVALID, "rescaling a must be finite and nonzero");
     PF_CHECK(probe_kind == PF_PROBE_GAUSSIAN || probe_kind == PF_PROBE_RADEMACHER, PF_ERR_INVALID, "unknown probe kind");
     PF_CUDA(cudaSetDevice(op->h->device));
+    AllocStream alloc_guard(op->h->stream);
     std::vector<double> m;
     if (dtype == PF_F64) m = kpm_moments<double>(op, a, b, N, R, (const double *)probes, ldp, probe_kind, seed, nullptr);
     else if (dtype == PF_F32) m = kpm_moments<float>(op, a, b, N, R, (const float *)probes, ldp, probe_kind, seed, nullptr);
@@ -694,6 +716,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
     PF_CHECK(P->reorth_passes >= 1 && P->reorth_passes <= 2, PF_ERR_INVALID, "reorth_passes must be 1 or 2");
     pf_handle *h = op->h;
     PF_CUDA(cudaSetDevice(h->device));
+    AllocStream alloc_guard(h->stream);
     cudaStream_t st = h->stream;
     const int64_t D = op->dim;
     PF_CHECK(s <= D, PF_ERR_INVALID,
@@ -710,7 +733,10 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
     // x0 -> host column-major, validate / orthonormalise, -> device RI
     std::vector<double> hx((size_t)D * s);
     if (x0_mem == PF_MEM_DEVICE)
-        PF_CUDA(cudaMemcpy(hx.data(), x0, hx.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    {
+        PF_CUDA(cudaMemcpyAsync(hx.data(), x0, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync(h);
+    }
     else std::memcpy(hx.data(), x0, hx.size() * sizeof(double));
     prepare_initial_state(hx, D, s);
     DevArray<double> xcm((size_t)D * s), xri((size_t)D * s);
