@@ -117,6 +117,27 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------- ranks
+def rank_seed0(rank: int) -> int:
+    """First realisation seed of a rank: ranks solve disjoint realisations."""
+    return 1000 + 7919 * rank
+
+
+def aggregate(nconv: float, seconds: float, world: int, device="cpu"):
+    """Whole-job throughput over ranks: every rank's converged pairs divided
+    by the slowest rank's device time.  Returns (value, total, max_seconds);
+    collectives run on ``device`` (cuda with NCCL, cpu with gloo)."""
+    if world == 1:
+        return nconv / seconds, float(nconv), float(seconds)
+    import torch
+    import torch.distributed as dist
+    tot = torch.tensor([float(nconv)], dtype=torch.float64, device=device)
+    mx = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    return float(tot.item()) / float(mx.item()), float(tot.item()), float(mx.item())
+
+
 # ----------------------------------------------------------- the workload
 def make_realisations(pkg, n, seed0, device=0):
     import numpy as np
@@ -256,7 +277,7 @@ def run_ours(args, rank, world, local_rank):
     pkg.load_library()
     B = max(1, args.batch)
     nsteps = args.warmup + args.steps
-    ops, x0s = make_realisations(pkg, nsteps * B, 1000 + 7919 * rank, device=local_rank)
+    ops, x0s = make_realisations(pkg, nsteps * B, rank_seed0(rank), device=local_rank)
     handle = _lib.handle(local_rank)
     stream = torch.cuda.ExternalStream(_lib.stream_of(handle), device=dev)
     # set-up outside the timed region: device descriptors, tuned step width, device x0,
@@ -278,13 +299,6 @@ def run_ours(args, rank, world, local_rank):
     def barrier():
         if world > 1:
             dist.barrier()
-
-    def reduce(x, op):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=op)
-        return float(t.item())
 
     def batch(step, host):
         idx = list(range(step * B, (step + 1) * B))
@@ -335,11 +349,9 @@ def run_ours(args, rank, world, local_rank):
         return nconv, e0.elapsed_time(e1) * 1e-3, wall, reps, clocks
 
     nconv, sec, wall, breps, clocks = timed(host_inputs=False)
-    sec_max = reduce(sec, dist.ReduceOp.MAX if world > 1 else None)
-    value = reduce(float(sum(nconv)), dist.ReduceOp.SUM if world > 1 else None) / sec_max
+    value, _, sec_max = aggregate(sum(nconv), sec, world, device=dev)
     e_nconv, e_sec, e_wall, e_reps, e_clocks = timed(host_inputs=True)
-    e_value = reduce(float(sum(e_nconv)), dist.ReduceOp.SUM if world > 1 else None) / \
-        reduce(e_sec, dist.ReduceOp.MAX if world > 1 else None)
+    e_value, _, _ = aggregate(sum(e_nconv), e_sec, world, device=dev)
     # plain single solves (one at a time on one stream): the kernels run alone,
     # so the library's stage timers give the step kernel's own duration
     reps, s_conv = [], 0
