@@ -291,8 +291,8 @@ def run_ours(args, rank, world, local_rank):
         t.copy_(torch.from_numpy(np.ascontiguousarray(x)).to(dev))
         x0_dev.append(t)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    wstreams = [torch.cuda.ExternalStream(_lib.stream_of(h), device=dev)
-                for h in pkg.worker_handles(B, local_rank)]
+    pool = pkg.solver_pool(B, local_rank)   # native request pool: B workers, one stream each
+    wstreams = [torch.cuda.ExternalStream(st, device=dev) for st in pool.streams()]
     tstream = torch.cuda.Stream(device=dev)
     torch.cuda.synchronize()
 
@@ -303,7 +303,7 @@ def run_ours(args, rank, world, local_rank):
     def batch(step, host):
         idx = list(range(step * B, (step + 1) * B))
         xs = [x0s[i] if host else x0_dev[i] for i in idx]
-        return pkg.polfed_batch([ops[i] for i in idx], xs, WORKLOAD["nev"], ("rescaled", 0.5), workers=B,
+        return pool.solve_batch([ops[i] for i in idx], xs, WORKLOAD["nev"], ("rescaled", 0.5),
                                 produce_report=True, dos=pkg.DoSConfig(N=WORKLOAD["dos_N"], R=WORKLOAD["dos_R"],
                                                                        seed=17 + step),
                                 fact=pkg.FactorizationConfig(eigentol=WORKLOAD["eigentol"]))

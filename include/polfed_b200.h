@@ -237,6 +237,60 @@ int pf_solve(pf_op *op, const pf_params *params, int s, int nev,
              const double *x0, int x0_mem, double *vals, double *vecs, int vecs_mem,
              pf_report *report, int *nconv);
 
+/* ------------------------------------------------ batching and serving */
+/* No reference counterpart: the reference solves one problem per call.  A
+ * pool owns `workers` handles (one stream each) and a request queue.  Each
+ * worker runs one solve at a time; up to `workers` solves are in flight
+ * together, so their latency-bound launches and host round trips overlap.
+ * A request is admitted when a worker is free and its estimated device
+ * footprint fits in what `hbm_budget` (bytes; 0 = 90 % of free memory at
+ * creation) leaves; otherwise it waits in FIFO order.  Requests run the
+ * same solve as pf_solve and give the same result alone or in a mix. */
+typedef struct pf_pool pf_pool;
+
+typedef struct pf_pool_stats {
+    int64_t submitted, completed, failed, queued, running;
+    int64_t eigenpairs;            /* converged pairs of completed requests */
+    double  bytes_budget, bytes_in_use, bytes_peak;
+    double  p50_latency, p99_latency, mean_latency;  /* seconds, submit -> done */
+    double  busy_seconds;          /* wall time with at least one request running */
+} pf_pool_stats;
+
+#define PF_REQ_QUEUED  0
+#define PF_REQ_RUNNING 1
+#define PF_REQ_DONE    2
+#define PF_REQ_FAILED  3
+
+int pf_pool_create(int device, int workers, double hbm_budget, pf_pool **out);
+int pf_pool_destroy(pf_pool *pool);   /* waits for running requests */
+/* The CUDA stream (cudaStream_t) of worker w, for callers that order their own
+ * work or timing events against the pool's solves. */
+int pf_pool_stream(pf_pool *pool, int worker, void **stream);
+/* Estimated device bytes of one solve (what admission charges). */
+double pf_solve_footprint(const pf_op *op, const pf_params *params, int s, int nev);
+/* Solve n problems concurrently; arrays of length n (params may repeat one
+ * struct by passing the same pointer n times).  x0[i] is D x s[i] in x0_mem;
+ * vals[i] holds nev[i] doubles; vecs[i] (may be NULL) D x nev[i] in vecs_mem;
+ * reports may be NULL.  Returns the first failing status (all are run). */
+int pf_pool_solve_batch(pf_pool *pool, int n, pf_op *const *ops, const pf_params *const *params,
+                        const int *s, const int *nev, const double *const *x0, int x0_mem,
+                        double *const *vals, double *const *vecs, int vecs_mem, pf_report *reports,
+                        int *nconv);
+/* Queue one solve; x0 (host, D x s) is copied.  vecs_out (may be NULL, host
+ * or device per vecs_mem, D x nev) must stay valid until the request is
+ * fetched or cancelled. */
+int pf_pool_submit(pf_pool *pool, pf_op *op, const pf_params *params, int s, int nev, const double *x0,
+                   double *vecs_out, int vecs_mem, int64_t *request);
+int pf_pool_poll(pf_pool *pool, int64_t request, int *state);
+/* Wait for (timeout_s < 0: indefinitely) and collect a finished request: vals
+ * (nev doubles, host), report (may be NULL), *nconv; the request is released.
+ * A failed request returns its error status. */
+int pf_pool_fetch(pf_pool *pool, int64_t request, double timeout_s, double *vals, pf_report *report,
+                  int *nconv);
+/* Drop a queued request (a running one finishes and is then discarded). */
+int pf_pool_cancel(pf_pool *pool, int64_t request);
+int pf_pool_get_stats(pf_pool *pool, pf_pool_stats *stats);
+
 /* (Emin, Emax) from two Lanczos probes on H (Lanczos.jl:183-212); x0 length D (host). */
 int pf_lanczos_extrema(pf_op *op, const double *x0, int maxdim, double tol, double eigentol,
                        double *Emin, double *Emax);

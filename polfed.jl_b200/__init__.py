@@ -12,7 +12,7 @@ from .core import (autotune, BenchmarkReport, DoSConfig, FactorizationConfig, Fa
                    Report, SpectralTransformReport, TransformConfig, apply, basis_index, basis_states,
                    chebyshev_filter, clenshaw_finalsum, clenshaw_recurrence, col_major, display_report,
                    expectedkrylovdim, kpm_moments, lanczos_extrema, normalize_target_spec, polfed,
-                   polfed_batch, worker_handles)
+                   polfed_batch, worker_handles, SolverPool, PoolStats, solver_pool)
 from .models import (BoundOperator, QSunOperator, SpinChainOperator, chain_bonds, goe_matrix, j1j2_hamiltonian,
                      qsun_hamiltonian, qsun_parameters, xxz_hamiltonian)
 
@@ -22,7 +22,7 @@ __all__ = [
     "xxz_hamiltonian", "j1j2_hamiltonian", "qsun_hamiltonian", "qsun_parameters", "chain_bonds",
     "goe_matrix", "SpinChainOperator", "QSunOperator", "apply", "clenshaw_recurrence",
     "clenshaw_finalsum", "chebyshev_filter", "kpm_moments", "basis_states", "basis_index", "col_major",
-    "normalize_target_spec", "expectedkrylovdim", "load_library", "autotune", "polfed_batch", "worker_handles", "BoundOperator",
+    "normalize_target_spec", "expectedkrylovdim", "load_library", "autotune", "polfed_batch", "worker_handles", "SolverPool", "PoolStats", "solver_pool", "BoundOperator",
 ]
 
 

@@ -33,7 +33,10 @@ EXPORTED = [
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
     "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind",
+    "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
+    "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
 ]
+PF_REQ_QUEUED, PF_REQ_RUNNING, PF_REQ_DONE, PF_REQ_FAILED = 0, 1, 2, 3
 
 
 class PolfedError(RuntimeError):
@@ -85,6 +88,16 @@ class pf_report(ctypes.Structure):
     ]
 
 
+class pf_pool_stats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+        ("queued", ctypes.c_int64), ("running", ctypes.c_int64), ("eigenpairs", ctypes.c_int64),
+        ("bytes_budget", ctypes.c_double), ("bytes_in_use", ctypes.c_double), ("bytes_peak", ctypes.c_double),
+        ("p50_latency", ctypes.c_double), ("p99_latency", ctypes.c_double), ("mean_latency", ctypes.c_double),
+        ("busy_seconds", ctypes.c_double),
+    ]
+
+
 _LIB = None
 
 
@@ -122,6 +135,16 @@ def load():
                            ctypes.POINTER(pf_report), ctypes.POINTER(i32)]),
         "pf_lanczos_extrema": (i32, [vp, vp, i32, f64, f64, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
         "pf_autotune": (i32, [vp, i32, i32, ctypes.POINTER(i32), vp]),
+        "pf_pool_create": (i32, [i32, i32, f64, ctypes.POINTER(vp)]),
+        "pf_pool_destroy": (i32, [vp]),
+        "pf_pool_stream": (i32, [vp, i32, ctypes.POINTER(vp)]),
+        "pf_solve_footprint": (f64, [vp, ctypes.POINTER(pf_params), i32, i32]),
+        "pf_pool_solve_batch": (i32, [vp, i32, vp, vp, vp, vp, vp, i32, vp, vp, i32, vp, vp]),
+        "pf_pool_submit": (i32, [vp, vp, ctypes.POINTER(pf_params), i32, i32, vp, vp, i32, ctypes.POINTER(i64)]),
+        "pf_pool_poll": (i32, [vp, i64, ctypes.POINTER(i32)]),
+        "pf_pool_fetch": (i32, [vp, i64, f64, vp, ctypes.POINTER(pf_report), ctypes.POINTER(i32)]),
+        "pf_pool_cancel": (i32, [vp, i64]),
+        "pf_pool_get_stats": (i32, [vp, ctypes.POINTER(pf_pool_stats)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -341,36 +341,249 @@ def worker_handles(n: int, device: int = 0):
     return hs[:n]
 
 
+def _host_x0(op: Operator, x0):
+    x = np.asarray(x0, dtype=np.float64)
+    if x.ndim not in (1, 2):
+        raise ValueError("x0 must be a vector or a matrix")
+    if x.shape[0] != op.dim:
+        raise ValueError(f"x0 has {x.shape[0]} rows; the operator dimension is {op.dim}")
+    if x.size == 0:
+        raise ValueError("POLFED initial vector must not be empty.")
+    s = 1 if x.ndim == 1 else x.shape[1]
+    return np.asfortranarray(x.reshape(op.dim, s)), s
+
+
+def _device_x0(op: Operator, x0):
+    import torch
+    D = op.dim
+    if x0.dtype != torch.float64:
+        raise ValueError("x0 must be float64")
+    if x0.dim() == 1:
+        if x0.shape[0] != D or x0.stride(0) != 1:
+            raise ValueError(f"x0 must be a contiguous vector of length {D}")
+    elif x0.dim() == 2:
+        if x0.shape[0] != D or x0.stride(0) != 1 or x0.stride(1) != D:
+            raise ValueError(f"x0 must be a column-major {D} x s CUDA tensor")
+    else:
+        raise ValueError("x0 must be a vector or a matrix")
+    return x0
+
+
+def _solve_kwargs(kwargs):
+    allowed = {"mapping", "transform", "fact", "dos", "precision", "produce_report", "vecs"}
+    bad = set(kwargs) - allowed
+    if bad:
+        raise TypeError(f"unexpected keyword arguments {sorted(bad)}")
+    return (kwargs.get("mapping") or MappingConfig(), kwargs.get("transform") or TransformConfig(),
+            kwargs.get("fact") or FactorizationConfig(), kwargs.get("dos") or DoSConfig(),
+            kwargs.get("precision", "fp64"), bool(kwargs.get("produce_report", False)), bool(kwargs.get("vecs", True)))
+
+
+@dataclass
+class PoolStats:
+    """Counters and latency percentiles of a SolverPool (seconds, bytes)."""
+    submitted: int
+    completed: int
+    failed: int
+    queued: int
+    running: int
+    eigenpairs: int
+    bytes_budget: float
+    bytes_in_use: float
+    bytes_peak: float
+    p50_latency: float
+    p99_latency: float
+    mean_latency: float
+    busy_seconds: float
+
+
+class SolverPool:
+    """Many POLFED solves on one device through the native request pool.
+
+    ``workers`` solves run at once, each on its own handle and stream, so their
+    latency-bound launches and host round trips overlap.  A request starts when
+    a worker is free and its device footprint (``footprint``) fits in
+    ``hbm_budget`` bytes (``None``: 90 % of the free memory at creation);
+    otherwise it waits, first in first out.  ``solve_batch`` runs a list of
+    problems to completion; ``submit`` / ``poll`` / ``result`` serve a stream
+    of requests.  Every request runs the same solve as ``polfed`` and gives
+    the same result whether it runs alone or among others."""
+
+    def __init__(self, workers: int = 4, device: int = 0, hbm_budget: Optional[float] = None):
+        self.device = device
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().pf_pool_create(device, int(workers), float(hbm_budget or 0.0), ctypes.byref(h)))
+        self._pool = h
+        self._pending: dict = {}
+
+    def close(self):
+        if self._pool is not None and self._pool.value:
+            _lib.check(_lib.load().pf_pool_destroy(self._pool))
+        self._pool = None
+        self._pending.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover - interpreter shutdown
+            pass
+
+    @staticmethod
+    def footprint(op: Operator, howmany: int, target, s: int, **kwargs) -> float:
+        """Estimated device bytes of one solve (what admission charges)."""
+        mapping, transform, fact, dos, precision, _, _ = _solve_kwargs(kwargs)
+        p, keep, _, _ = _params(op, howmany, target, mapping, transform, fact, dos, precision)
+        return _lib.load().pf_solve_footprint(op.op, ctypes.byref(p), int(s), int(howmany))
+
+    def streams(self):
+        """The workers' CUDA stream handles (integers), one per worker."""
+        out, w = [], 0
+        while True:
+            st = ctypes.c_void_p()
+            if _lib.load().pf_pool_stream(self._pool, w, ctypes.byref(st)) != _lib.PF_OK:
+                return out
+            out.append(st.value or 0)
+            w += 1
+
+    def solve_batch(self, ops, x0s, howmany: int, target, **kwargs):
+        """Solve ``ops[i]`` from ``x0s[i]`` for all i; returns one ``polfed``
+        result tuple per problem, in order.  ``x0s`` are all host arrays, or
+        all column-major float64 CUDA tensors (then the eigenvectors come back
+        as CUDA tensors and never leave HBM)."""
+        if len(ops) != len(x0s):
+            raise ValueError("one x0 per operator is required")
+        n = len(ops)
+        if n == 0:
+            return []
+        mapping, transform, fact, dos, precision, want_rep, want_vecs = _solve_kwargs(kwargs)
+        on_device = _is_cuda_tensor(x0s[0])
+        if any(_is_cuda_tensor(x) != on_device for x in x0s):
+            raise ValueError("x0s must be all host arrays or all CUDA tensors")
+        keep = []
+        params, xptr, ss, vals, vecs = [], [], [], [], []
+        for op, x0 in zip(ops, x0s):
+            if op.device != self.device:
+                raise ValueError("operator and pool are on different devices")
+            if on_device:
+                x, s = _device_x0(op, x0), (1 if x0.dim() == 1 else x0.shape[1])
+                xptr.append(x.data_ptr())
+                V = col_major(op.dim, howmany, device=self.device) if want_vecs else None
+            else:
+                x, s = _host_x0(op, x0)
+                xptr.append(x.ctypes.data)
+                V = np.zeros((op.dim, howmany), order="F") if want_vecs else None
+            p, kp, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
+            keep += [x, kp]
+            params.append(p)
+            ss.append(s)
+            vals.append(np.zeros(howmany))
+            vecs.append(V)
+        P = ctypes.c_void_p
+        mem = _lib.PF_MEM_DEVICE if on_device else _lib.PF_MEM_HOST
+        vptr = [(V.data_ptr() if on_device else V.ctypes.data) for V in vecs] if want_vecs else None
+        a_ops = (P * n)(*[op.op for op in ops])
+        a_par = (P * n)(*[ctypes.addressof(p) for p in params])
+        a_s = (ctypes.c_int * n)(*ss)
+        a_nev = (ctypes.c_int * n)(*([int(howmany)] * n))
+        a_x = (P * n)(*xptr)
+        a_v = (P * n)(*[v.ctypes.data for v in vals])
+        a_V = (P * n)(*vptr) if want_vecs else None
+        reps = (_lib.pf_report * n)()
+        nconv = (ctypes.c_int * n)()
+        _lib.check(_lib.load().pf_pool_solve_batch(self._pool, n, a_ops, a_par, a_s, a_nev, a_x, mem,
+                                                   a_v, a_V, mem, reps, nconv))
+        del keep
+        out = []
+        for i in range(n):
+            k = nconv[i]
+            if want_vecs:
+                V = vecs[i][:, :k] if on_device else vecs[i][:, :k].copy()
+            else:
+                V = None
+            res = (vals[i][:k].copy(), V)
+            if want_rep:
+                res = res + (_make_report(reps[i], kind, val),)
+            out.append(res)
+        return out
+
+    def submit(self, op: Operator, x0, howmany: int, target, **kwargs) -> int:
+        """Queue one solve; returns its request id.  ``x0`` is copied."""
+        mapping, transform, fact, dos, precision, want_rep, want_vecs = _solve_kwargs(kwargs)
+        if op.device != self.device:
+            raise ValueError("operator and pool are on different devices")
+        if dos.probes is not None:
+            raise ValueError("served requests draw their KPM probes from dos.seed")
+        x, s = _host_x0(op, x0)
+        p, _, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
+        V = np.zeros((op.dim, howmany), order="F") if want_vecs else None
+        rid = ctypes.c_int64()
+        _lib.check(_lib.load().pf_pool_submit(self._pool, op.op, ctypes.byref(p), s, int(howmany), x.ctypes.data,
+                                              V.ctypes.data if want_vecs else None, _lib.PF_MEM_HOST,
+                                              ctypes.byref(rid)))
+        self._pending[rid.value] = (V, int(howmany), want_rep, kind, val)
+        return rid.value
+
+    def poll(self, request: int) -> str:
+        """"queued", "running", "done" or "failed"."""
+        st = ctypes.c_int()
+        _lib.check(_lib.load().pf_pool_poll(self._pool, int(request), ctypes.byref(st)))
+        return ("queued", "running", "done", "failed")[st.value]
+
+    def result(self, request: int, timeout: Optional[float] = None):
+        """Wait for a request and return its ``polfed`` result tuple; raises the
+        request's error if it failed (the request is released either way)."""
+        V, howmany, want_rep, kind, val = self._pending[request]
+        vals = np.zeros(howmany)
+        rep = _lib.pf_report()
+        n = ctypes.c_int()
+        st = _lib.load().pf_pool_fetch(self._pool, int(request), -1.0 if timeout is None else float(timeout),
+                                       vals.ctypes.data, ctypes.byref(rep), ctypes.byref(n))
+        if not (st == _lib.PF_ERR_NUMERIC and b"timeout" in _lib.load().pf_last_error()):
+            self._pending.pop(request, None)
+        _lib.check(st)
+        k = n.value
+        res = (vals[:k].copy(), V[:, :k].copy() if V is not None else None)
+        if want_rep:
+            res = res + (_make_report(rep, kind, val),)
+        return res
+
+    def cancel(self, request: int):
+        _lib.check(_lib.load().pf_pool_cancel(self._pool, int(request)))
+        self._pending.pop(request, None)
+
+    def stats(self) -> PoolStats:
+        st = _lib.pf_pool_stats()
+        _lib.check(_lib.load().pf_pool_get_stats(self._pool, ctypes.byref(st)))
+        return PoolStats(**{f: getattr(st, f) for f, _ in st._fields_})
+
+
+_POOLS: dict = {}
+
+
+def solver_pool(workers: int = 4, device: int = 0) -> SolverPool:
+    """A process-wide SolverPool per (device, workers), created on first use."""
+    key = (device, int(workers))
+    if key not in _POOLS:
+        _POOLS[key] = SolverPool(workers=workers, device=device)
+    return _POOLS[key]
+
+
 def polfed_batch(ops, x0s, howmany: int, target, *, workers: int = 4, **kwargs):
     """Solve many independent problems (e.g. disorder realisations) with
-    ``workers`` solves in flight at once, each on its own handle / stream, so
-    their latency-bound launches and host round trips overlap on the GPU.
-    Returns one ``polfed`` result tuple per problem, in order."""
-    import threading
-    from concurrent.futures import ThreadPoolExecutor
+    ``workers`` solves in flight at once through the native request pool.
+    ``x0s`` are host arrays or column-major CUDA tensors.  Returns one
+    ``polfed`` result tuple per problem, in order."""
     if len(ops) != len(x0s):
         raise ValueError("one x0 per operator is required")
     if not ops:
         return []
-    hs = worker_handles(max(1, min(workers, len(ops))), ops[0].device)
-    free = list(range(len(hs)))
-    lock = threading.Lock()
-
-    def run(i):
-        with lock:
-            slot = free.pop()
-        try:
-            view = ops[i].bind(hs[slot])
-            try:
-                return polfed(view, x0s[i], howmany, target, **kwargs)
-            finally:
-                view.close()
-        finally:
-            with lock:
-                free.append(slot)
-
-    with ThreadPoolExecutor(max_workers=len(hs)) as ex:
-        return list(ex.map(run, range(len(ops))))
+    return solver_pool(max(1, workers), ops[0].device).solve_batch(ops, x0s, howmany, target, **kwargs)
 
 
 def _is_cuda_tensor(x) -> bool:

@@ -260,4 +260,78 @@ int pf_lanczos_extrema(pf_op *op, const double *x0, int maxdim, double tol, doub
     PF_API_END
 }
 
+// ------------------------------------------------------------- request pool
+int pf_pool_create(int device, int workers, double hbm_budget, pf_pool **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    *out = pf::pool_create(device, workers, hbm_budget);
+    PF_API_END
+}
+
+int pf_pool_destroy(pf_pool *pool) {
+    PF_API_BEGIN
+    pf::pool_destroy(pool);
+    PF_API_END
+}
+
+int pf_pool_stream(pf_pool *pool, int worker, void **stream) {
+    PF_API_BEGIN
+    PF_CHECK(pool && stream, PF_ERR_INVALID, "null argument");
+    *stream = (void *)pf::pool_stream(pool, worker);
+    PF_API_END
+}
+
+double pf_solve_footprint(const pf_op *op, const pf_params *params, int s, int nev) {
+    if (!op || !params || s < 1 || nev < 1) return -1.0;
+    return pf::solve_footprint(op, params, s, nev);
+}
+
+int pf_pool_solve_batch(pf_pool *pool, int n, pf_op *const *ops, const pf_params *const *params, const int *s,
+                        const int *nev, const double *const *x0, int x0_mem, double *const *vals,
+                        double *const *vecs, int vecs_mem, pf_report *reports, int *nconv) {
+    PF_API_BEGIN
+    std::string err;
+    int st = pf::pool_solve_batch(pool, n, ops, params, s, nev, x0, x0_mem, vals, vecs, vecs_mem, reports, nconv, err);
+    if (st != PF_OK) throw pf::Error(st, err);
+    PF_API_END
+}
+
+int pf_pool_submit(pf_pool *pool, pf_op *op, const pf_params *params, int s, int nev, const double *x0,
+                   double *vecs_out, int vecs_mem, int64_t *request) {
+    PF_API_BEGIN
+    PF_CHECK(request != nullptr, PF_ERR_INVALID, "null output pointer");
+    *request = pf::pool_submit(pool, op, params, s, nev, x0, vecs_out, vecs_mem);
+    PF_API_END
+}
+
+int pf_pool_poll(pf_pool *pool, int64_t request, int *state) {
+    PF_API_BEGIN
+    PF_CHECK(pool && state, PF_ERR_INVALID, "null argument");
+    *state = pf::pool_poll(pool, request);
+    PF_API_END
+}
+
+int pf_pool_fetch(pf_pool *pool, int64_t request, double timeout_s, double *vals, pf_report *report, int *nconv) {
+    PF_API_BEGIN
+    PF_CHECK(pool, PF_ERR_INVALID, "null pool");
+    std::string err;
+    int st = pf::pool_fetch(pool, request, timeout_s, vals, report, nconv, err);
+    if (st != PF_OK) throw pf::Error(st, err);
+    PF_API_END
+}
+
+int pf_pool_cancel(pf_pool *pool, int64_t request) {
+    PF_API_BEGIN
+    PF_CHECK(pool, PF_ERR_INVALID, "null pool");
+    pf::pool_cancel(pool, request);
+    PF_API_END
+}
+
+int pf_pool_get_stats(pf_pool *pool, pf_pool_stats *stats) {
+    PF_API_BEGIN
+    PF_CHECK(pool && stats, PF_ERR_INVALID, "null argument");
+    pf::pool_stats(pool, stats);
+    PF_API_END
+}
+
 }  // extern "C"

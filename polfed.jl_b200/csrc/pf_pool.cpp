@@ -1,0 +1,362 @@
+// pf_pool.cpp -- batched and served POLFED solves on one device.
+//
+// A pool owns W worker threads, each with its own pf_handle (stream, cuBLAS,
+// cuSOLVER, workspaces).  Requests wait in one FIFO queue; a free worker takes
+// the head as soon as its estimated device footprint fits in the pool's HBM
+// budget (continuous batching: requests that arrive while others run start as
+// workers and memory free up).  Each request runs exactly pf_solve on a view
+// of its operator bound to the worker's handle, so a result does not depend on
+// what else is in flight.  Solver workspaces are stream-ordered allocations
+// from the device pool, so concurrent solves never synchronise the device.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <thread>
+#include <unordered_map>
+
+#include "pf_internal.h"
+#include "pf_solver.h"
+
+namespace pf {
+
+using Clock = std::chrono::steady_clock;
+
+struct PoolRequest {
+    int64_t id = 0;
+    pf_op *op = nullptr;
+    pf_params params{};
+    int s = 1, nev = 1;
+    std::vector<double> x0_copy;        // serving path: owned copy of x0
+    const double *x0 = nullptr;         // what the solve reads
+    int x0_mem = PF_MEM_HOST;
+    double *vecs_out = nullptr;
+    int vecs_mem = PF_MEM_HOST;
+    double *vals_out = nullptr;         // batch path: caller's arrays
+    pf_report *rep_out = nullptr;
+    int *nconv_out = nullptr;
+    std::vector<double> vals;           // serving path: results kept until fetch
+    pf_report rep{};
+    int nconv = 0;
+    int state = PF_REQ_QUEUED;
+    int status = PF_OK;
+    std::string error;
+    double footprint = 0.0;
+    bool cancelled = false, batch = false;
+    Clock::time_point t_submit, t_done;
+};
+
+}  // namespace pf
+
+struct pf_pool {
+    int device = 0;
+    std::vector<pf_handle *> handles;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<pf::PoolRequest>> queue;
+    std::unordered_map<int64_t, std::shared_ptr<pf::PoolRequest>> requests;
+    double budget = 0.0, in_use = 0.0, peak = 0.0;
+    int64_t next_id = 1, submitted = 0, completed = 0, failed = 0, running = 0, eigenpairs = 0;
+    std::vector<double> latencies;
+    double busy = 0.0;
+    pf::Clock::time_point busy_since;
+    bool stop = false;
+};
+
+namespace pf {
+
+double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev) {
+    const double D = (double)op->dim;
+    const int64_t md0 = (int64_t)std::ceil((20.427 * s + 1.696 * nev) * p->overestimate_iters);
+    const double maxdim = (double)((md0 + s - 1) / s * s);
+    const double ext = (p->has_Emin && p->has_Emax) ? 0.0 : (double)(p->extrema_maxdim > 0 ? p->extrema_maxdim : 1000);
+    const double w = p->precision == PF_PREC_FP64 ? 8.0 : 4.0;
+    double bytes = 8.0 * D * std::max(ext + 3.0, maxdim + 3.0 * s);  // Krylov basis + Lanczos blocks
+    bytes += 4.0 * D * s * w + 2.0 * 8.0 * D * s;                     // filter blocks, x0 copies
+    bytes += 2.0 * D * 64 * w;                                        // KPM probe blocks
+    bytes += 2.0 * 8.0 * D * nev;                                     // Ritz vectors and H psi
+    bytes += 2.0 * 8.0 * maxdim * maxdim + (64 << 20);                // projected problem, slack
+    return bytes;
+}
+
+static void pool_worker(pf_pool *pool, int w) {
+    pf_handle *h = pool->handles[w];
+    cudaSetDevice(pool->device);
+    while (true) {
+        std::shared_ptr<PoolRequest> req;
+        {
+            std::unique_lock<std::mutex> lock(pool->mu);
+            pool->cv_work.wait(lock, [&] {
+                if (pool->stop) return true;
+                if (pool->queue.empty()) return false;
+                const auto &head = pool->queue.front();
+                // strict FIFO; a request larger than the whole budget still runs alone
+                return head->cancelled || pool->in_use + head->footprint <= pool->budget || pool->running == 0;
+            });
+            if (pool->stop && pool->queue.empty()) return;
+            if (pool->queue.empty()) continue;
+            req = pool->queue.front();
+            pool->queue.pop_front();
+            if (req->cancelled) {
+                pool->requests.erase(req->id);
+                pool->cv_work.notify_all();
+                continue;
+            }
+            pool->in_use += req->footprint;
+            pool->peak = std::max(pool->peak, pool->in_use);
+            if (pool->running++ == 0) pool->busy_since = Clock::now();
+            req->state = PF_REQ_RUNNING;
+        }
+        int status = PF_OK;
+        std::string err;
+        pf_op *view = nullptr;
+        try {
+            view = bind_op(req->op, h);
+            double *vals = req->batch ? req->vals_out : req->vals.data();
+            solve(view, &req->params, req->s, req->nev, req->x0, req->x0_mem, vals, req->vecs_out, req->vecs_mem,
+                  &req->rep, &req->nconv);
+            {
+                // keep the autotuned step width on the caller's operator for later requests
+                std::lock_guard<std::mutex> lk(req->op->tune_mu);
+                std::lock_guard<std::mutex> lv(view->tune_mu);
+                for (auto &kv : view->tuned_width) req->op->tuned_width.insert(kv);
+            }
+        } catch (const Error &e) {
+            status = e.code;
+            err = e.what();
+        } catch (const std::exception &e) {
+            status = PF_ERR_CUDA;
+            err = e.what();
+        }
+        destroy_op(view);
+        {
+            std::lock_guard<std::mutex> lock(pool->mu);
+            pool->in_use -= req->footprint;
+            if (--pool->running == 0)
+                pool->busy += std::chrono::duration<double>(Clock::now() - pool->busy_since).count();
+            req->t_done = Clock::now();
+            req->status = status;
+            req->error = err;
+            req->state = status == PF_OK ? PF_REQ_DONE : PF_REQ_FAILED;
+            if (status == PF_OK) {
+                ++pool->completed;
+                pool->eigenpairs += req->nconv;
+                pool->latencies.push_back(std::chrono::duration<double>(req->t_done - req->t_submit).count());
+                if (req->batch) {
+                    if (req->rep_out) *req->rep_out = req->rep;
+                    if (req->nconv_out) *req->nconv_out = req->nconv;
+                }
+            } else {
+                ++pool->failed;
+            }
+            if (req->cancelled) pool->requests.erase(req->id);
+        }
+        pool->cv_done.notify_all();
+        pool->cv_work.notify_all();
+    }
+}
+
+pf_pool *pool_create(int device, int workers, double budget) {
+    PF_CHECK(workers >= 1 && workers <= 64, PF_ERR_INVALID, "a pool needs 1..64 workers");
+    PF_CUDA(cudaSetDevice(device));
+    pf_pool *pool = new pf_pool();
+    pool->device = device;
+    if (budget <= 0) {
+        size_t fr = 0, tot = 0;
+        PF_CUDA(cudaMemGetInfo(&fr, &tot));
+        budget = 0.9 * (double)fr;
+    }
+    pool->budget = budget;
+    try {
+        for (int w = 0; w < workers; ++w) {
+            pf_handle *h = nullptr;
+            if (pf_handle_create(device, &h) != PF_OK) throw Error(PF_ERR_CUDA, pf_last_error());
+            pool->handles.push_back(h);
+        }
+        for (int w = 0; w < workers; ++w) pool->threads.emplace_back(pool_worker, pool, w);
+    } catch (...) {
+        {
+            std::lock_guard<std::mutex> lock(pool->mu);
+            pool->stop = true;
+        }
+        pool->cv_work.notify_all();
+        for (auto &t : pool->threads) t.join();
+        for (auto h : pool->handles) pf_handle_destroy(h);
+        delete pool;
+        throw;
+    }
+    return pool;
+}
+
+void pool_destroy(pf_pool *pool) {
+    if (!pool) return;
+    {
+        std::lock_guard<std::mutex> lock(pool->mu);
+        for (auto &r : pool->queue) r->cancelled = true;
+        pool->stop = true;
+    }
+    pool->cv_work.notify_all();
+    for (auto &t : pool->threads) t.join();
+    for (auto h : pool->handles) pf_handle_destroy(h);
+    delete pool;
+}
+
+cudaStream_t pool_stream(pf_pool *pool, int worker) {
+    PF_CHECK(worker >= 0 && worker < (int)pool->handles.size(), PF_ERR_INVALID, "no such worker");
+    return pool->handles[worker]->stream;
+}
+
+static std::shared_ptr<PoolRequest> make_request(pf_pool *pool, pf_op *op, const pf_params *p, int s, int nev) {
+    PF_CHECK(op && p, PF_ERR_INVALID, "null argument");
+    PF_CHECK(op->h && op->h->device == pool->device, PF_ERR_INVALID, "operator and pool are on different devices");
+    PF_CHECK(s >= 1 && nev >= 1, PF_ERR_INVALID, "s and nev must be positive");
+    auto r = std::make_shared<PoolRequest>();
+    r->op = op;
+    r->params = *p;
+    r->s = s;
+    r->nev = nev;
+    r->footprint = solve_footprint(op, p, s, nev);
+    r->t_submit = Clock::now();
+    return r;
+}
+
+static void enqueue(pf_pool *pool, const std::shared_ptr<PoolRequest> &r) {
+    {
+        std::lock_guard<std::mutex> lock(pool->mu);
+        PF_CHECK(!pool->stop, PF_ERR_INVALID, "pool is shutting down");
+        r->id = pool->next_id++;
+        pool->requests[r->id] = r;
+        pool->queue.push_back(r);
+        ++pool->submitted;
+    }
+    pool->cv_work.notify_all();
+}
+
+int64_t pool_submit(pf_pool *pool, pf_op *op, const pf_params *p, int s, int nev, const double *x0,
+                    double *vecs_out, int vecs_mem) {
+    PF_CHECK(pool && x0, PF_ERR_INVALID, "null argument");
+    auto r = make_request(pool, op, p, s, nev);
+    PF_CHECK(!p->probes, PF_ERR_INVALID, "served requests draw their KPM probes from params.seed");
+    r->x0_copy.assign(x0, x0 + (size_t)op->dim * s);
+    r->x0 = r->x0_copy.data();
+    r->x0_mem = PF_MEM_HOST;
+    r->vals.assign(nev, 0.0);
+    r->vecs_out = vecs_out;
+    r->vecs_mem = vecs_mem;
+    enqueue(pool, r);
+    return r->id;
+}
+
+int pool_solve_batch(pf_pool *pool, int n, pf_op *const *ops, const pf_params *const *params, const int *s,
+                     const int *nev, const double *const *x0, int x0_mem, double *const *vals, double *const *vecs,
+                     int vecs_mem, pf_report *reports, int *nconv, std::string &first_error) {
+    PF_CHECK(pool && n >= 0 && (n == 0 || (ops && params && s && nev && x0 && vals && nconv)), PF_ERR_INVALID,
+             "null argument");
+    std::vector<std::shared_ptr<PoolRequest>> reqs;
+    for (int i = 0; i < n; ++i) {
+        auto r = make_request(pool, ops[i], params[i], s[i], nev[i]);
+        r->batch = true;
+        r->x0 = x0[i];
+        r->x0_mem = x0_mem;
+        r->vals_out = vals[i];
+        r->vecs_out = vecs ? vecs[i] : nullptr;
+        r->vecs_mem = vecs_mem;
+        r->rep_out = reports ? reports + i : nullptr;
+        r->nconv_out = nconv + i;
+        reqs.push_back(r);
+    }
+    for (auto &r : reqs) enqueue(pool, r);
+    int status = PF_OK;
+    std::unique_lock<std::mutex> lock(pool->mu);
+    for (auto &r : reqs) {
+        pool->cv_done.wait(lock, [&] { return r->state == PF_REQ_DONE || r->state == PF_REQ_FAILED; });
+        if (r->status != PF_OK && status == PF_OK) {
+            status = r->status;
+            first_error = r->error;
+        }
+        pool->requests.erase(r->id);
+    }
+    return status;
+}
+
+int pool_poll(pf_pool *pool, int64_t id) {
+    std::lock_guard<std::mutex> lock(pool->mu);
+    auto it = pool->requests.find(id);
+    PF_CHECK(it != pool->requests.end(), PF_ERR_INVALID, "unknown request");
+    return it->second->state;
+}
+
+int pool_fetch(pf_pool *pool, int64_t id, double timeout_s, double *vals, pf_report *rep, int *nconv,
+               std::string &error) {
+    std::unique_lock<std::mutex> lock(pool->mu);
+    auto it = pool->requests.find(id);
+    PF_CHECK(it != pool->requests.end(), PF_ERR_INVALID, "unknown request");
+    auto r = it->second;
+    PF_CHECK(!r->batch, PF_ERR_INVALID, "batch requests are collected by pf_pool_solve_batch");
+    PF_CHECK(!r->cancelled, PF_ERR_INVALID, "request was cancelled");
+    auto done = [&] { return r->state == PF_REQ_DONE || r->state == PF_REQ_FAILED; };
+    if (timeout_s < 0) pool->cv_done.wait(lock, done);
+    else if (!pool->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), done))
+        throw Error(PF_ERR_NUMERIC, "request not finished within the timeout");
+    pool->requests.erase(id);
+    if (r->status != PF_OK) {
+        error = r->error;
+        return r->status;
+    }
+    if (vals) std::copy(r->vals.begin(), r->vals.begin() + r->nconv, vals);
+    if (rep) *rep = r->rep;
+    if (nconv) *nconv = r->nconv;
+    return PF_OK;
+}
+
+void pool_cancel(pf_pool *pool, int64_t id) {
+    std::lock_guard<std::mutex> lock(pool->mu);
+    auto it = pool->requests.find(id);
+    PF_CHECK(it != pool->requests.end(), PF_ERR_INVALID, "unknown request");
+    auto r = it->second;
+    r->cancelled = true;
+    if (r->state == PF_REQ_QUEUED) {
+        pool->queue.erase(std::remove(pool->queue.begin(), pool->queue.end(), r), pool->queue.end());
+        pool->requests.erase(it);
+    } else if (r->state != PF_REQ_RUNNING) {
+        pool->requests.erase(it);
+    }
+    pool->cv_work.notify_all();
+}
+
+void pool_stats(pf_pool *pool, pf_pool_stats *st) {
+    std::lock_guard<std::mutex> lock(pool->mu);
+    std::memset(st, 0, sizeof(*st));
+    st->submitted = pool->submitted;
+    st->completed = pool->completed;
+    st->failed = pool->failed;
+    st->queued = (int64_t)pool->queue.size();
+    st->running = pool->running;
+    st->eigenpairs = pool->eigenpairs;
+    st->bytes_budget = pool->budget;
+    st->bytes_in_use = pool->in_use;
+    st->bytes_peak = pool->peak;
+    st->busy_seconds =
+        pool->busy + (pool->running > 0 ? std::chrono::duration<double>(Clock::now() - pool->busy_since).count() : 0.0);
+    std::vector<double> l = pool->latencies;
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double q) {
+            const double pos = q * (l.size() - 1);
+            const size_t i = (size_t)pos;
+            const double f = pos - i;
+            return i + 1 < l.size() ? l[i] * (1 - f) + l[i + 1] * f : l[i];
+        };
+        st->p50_latency = pct(0.50);
+        st->p99_latency = pct(0.99);
+        double m = 0;
+        for (double v : l) m += v;
+        st->mean_latency = m / l.size();
+    }
+}
+
+}  // namespace pf

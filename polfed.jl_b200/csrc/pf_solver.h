@@ -32,4 +32,20 @@ void solve(pf_op *op, const pf_params *p, int s, int nev, const double *x0, int 
 void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, double eigentol, double *Emin,
                      double *Emax);
 
+// request pool (pf_pool.cpp)
+double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev);
+pf_pool *pool_create(int device, int workers, double budget);
+void pool_destroy(pf_pool *pool);
+cudaStream_t pool_stream(pf_pool *pool, int worker);
+int64_t pool_submit(pf_pool *pool, pf_op *op, const pf_params *p, int s, int nev, const double *x0,
+                    double *vecs_out, int vecs_mem);
+int pool_solve_batch(pf_pool *pool, int n, pf_op *const *ops, const pf_params *const *params, const int *s,
+                     const int *nev, const double *const *x0, int x0_mem, double *const *vals, double *const *vecs,
+                     int vecs_mem, pf_report *reports, int *nconv, std::string &first_error);
+int pool_poll(pf_pool *pool, int64_t id);
+int pool_fetch(pf_pool *pool, int64_t id, double timeout_s, double *vals, pf_report *rep, int *nconv,
+               std::string &error);
+void pool_cancel(pf_pool *pool, int64_t id);
+void pool_stats(pf_pool *pool, pf_pool_stats *st);
+
 }  // namespace pf

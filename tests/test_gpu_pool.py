@@ -1,0 +1,133 @@
+"""The native request pool (pf_pool_*): batched and served solves.
+
+Every request in a pool runs the same solve as pf_solve on its own worker
+handle, so a problem must give the same eigenpairs whether it is solved
+alone or among others running at the same time: eigenvalues equal to 1e-10
+relative, each vector with an FP64 residual below the eigen tolerance.  The
+served path (submit / poll / result) must admit requests only while their
+footprints fit the HBM budget, keep FIFO order, release failed and cancelled
+requests, and report latency percentiles.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NEV = 8
+TARGET = ("rescaled", 0.5)
+EIGENTOL = 1e-9
+
+
+def _kw(pkg, seed):
+    return dict(fact=pkg.FactorizationConfig(eigentol=EIGENTOL, overestimate_iters=2.0),
+                dos=pkg.DoSConfig(N=64, R=16, seed=seed))
+
+
+def _problems(pkg, orc):
+    """Three operators of different kinds and sizes; two share one operator."""
+    rng = np.random.default_rng(5)
+    out = []
+    f = 5 * (2 * rng.random(12) - 1)
+    xxz = pkg.xxz_hamiltonian(12, 6, 1.0, 1.0, 0.0, fields=f)
+    out.append((xxz, orc.xxz_matrix(12, 6, 1.0, 1.0, f), 1))
+    f2 = 4 * (2 * rng.random(12) - 1)
+    j1j2 = pkg.j1j2_hamiltonian(12, 6, 1.0, 0.5, 1.0, 0.8, 0.0, fields=f2)
+    out.append((j1j2, orc.j1j2_matrix(12, 6, 1.0, 0.5, 1.0, 0.8, f2), 2))
+    fq, nq, cq, gq = pkg.qsun_parameters(7, 3, 0.75, rng=rng)
+    qsun = pkg.QSunOperator(7, 3, 1.0, cq, nq, fq, gq)
+    out.append((qsun, orc.qsun_matrix(7, 3, 1.0, cq, nq, fq, gq), 4))
+    out.append((xxz, out[0][1], 2))   # the XXZ operator again, with a block start
+    return out, rng
+
+
+def _x0(rng, D, s):
+    return rng.random(D) if s == 1 else rng.random((D, s))
+
+
+def _residuals_ok(H, vals, vecs):
+    for j in range(len(vals)):
+        v = vecs[:, j]
+        assert np.linalg.norm(H @ v - vals[j] * v) < EIGENTOL * 10
+
+
+def test_batch_matches_each_problem_alone(pkg, orc, cuda):
+    probs, rng = _problems(pkg, orc)
+    x0s = [_x0(rng, H.shape[0], s) for _, H, s in probs]
+    for op, _, s in probs:   # same step width alone and in the mix
+        pkg.autotune(op, s, "fp64")
+    alone = [pkg.polfed(op, x0, NEV, TARGET, **_kw(pkg, 11 + i)) for i, ((op, _, _), x0) in enumerate(zip(probs, x0s))]
+    with pkg.SolverPool(workers=4) as pool:
+        # solve_batch takes one parameter set; run the problems one seed at a time in a mix with the others
+        mixed = []
+        for i in range(len(probs)):
+            order = [i] + [j for j in range(len(probs)) if j != i]
+            res = pool.solve_batch([probs[j][0] for j in order], [x0s[j] for j in order], NEV, TARGET,
+                                   **_kw(pkg, 11 + i))
+            mixed.append(res[0])
+        st = pool.stats()
+    for (op, H, s), (va, Va), (vm, Vm) in zip(probs, alone, mixed):
+        assert len(va) == len(vm) and len(va) >= 1
+        assert np.max(np.abs(va - vm) / np.maximum(1, np.abs(va))) < 1e-10
+        _residuals_ok(H, vm, Vm)
+    assert st.completed == 4 * len(probs) and st.failed == 0
+    assert st.eigenpairs >= sum(len(v) for v, _ in mixed)
+
+
+def test_batch_with_device_inputs(pkg, orc, cuda):
+    probs, rng = _problems(pkg, orc)
+    hx = [_x0(rng, H.shape[0], s) for _, H, s in probs]
+    dx = []
+    for x in hx:
+        x2 = x.reshape(x.shape[0], -1)
+        t = pkg.col_major(x2.shape[0], x2.shape[1])
+        t.copy_(cuda.from_numpy(np.ascontiguousarray(x2)).to("cuda:0"))
+        dx.append(t if x.ndim == 2 else t[:, 0].contiguous())
+    ops = [p[0] for p in probs]
+    pool = pkg.solver_pool(3)
+    host = pool.solve_batch(ops, hx, NEV, TARGET, **_kw(pkg, 3))
+    dev = pool.solve_batch(ops, dx, NEV, TARGET, **_kw(pkg, 3))
+    for (op, H, s), (vh, _), (vd, Vd) in zip(probs, host, dev):
+        assert Vd.is_cuda
+        assert np.max(np.abs(vh - vd) / np.maximum(1, np.abs(vh))) < 1e-10
+        _residuals_ok(H, vd, Vd.cpu().numpy())
+
+
+def test_served_stream_respects_budget_and_order(pkg, orc, cuda):
+    probs, rng = _problems(pkg, orc)
+    op, H, s = probs[2]
+    fp = pkg.SolverPool.footprint(op, NEV, TARGET, s, **_kw(pkg, 0))
+    assert fp > 8 * H.shape[0] * NEV
+    # room for one request at a time although three workers are free
+    with pkg.SolverPool(workers=3, hbm_budget=1.5 * fp) as pool:
+        ids = [pool.submit(op, _x0(rng, H.shape[0], s), NEV, TARGET, **_kw(pkg, 20 + k)) for k in range(4)]
+        states = [pool.poll(r) for r in ids]
+        assert states[-1] == "queued"
+        res = [pool.result(r) for r in ids]
+        st = pool.stats()
+    for vals, vecs in res:
+        assert len(vals) >= 1
+        _residuals_ok(H, vals, vecs)
+    assert st.completed == 4 and st.queued == 0 and st.running == 0
+    assert st.bytes_peak <= 1.5 * fp + 1
+    assert st.bytes_in_use == 0
+    assert 0 < st.p50_latency <= st.p99_latency
+    assert st.busy_seconds > 0
+
+
+def test_failed_and_cancelled_requests_are_released(pkg, orc, cuda):
+    probs, rng = _problems(pkg, orc)
+    op, H, s = probs[0]
+    D = H.shape[0]
+    with pkg.SolverPool(workers=1) as pool:
+        bad = pool.submit(op, np.zeros(D), NEV, TARGET, **_kw(pkg, 1))      # zero start vector
+        good = pool.submit(op, _x0(rng, D, 1), NEV, TARGET, **_kw(pkg, 2))
+        dropped = pool.submit(op, _x0(rng, D, 1), NEV, TARGET, **_kw(pkg, 3))
+        pool.cancel(dropped)
+        with pytest.raises(pkg._lib.PolfedArgumentError, match="nonzero"):
+            pool.result(bad)
+        vals, vecs = pool.result(good)
+        _residuals_ok(H, vals, vecs)
+        with pytest.raises(pkg._lib.PolfedArgumentError, match="unknown request"):
+            pool.poll(dropped)
+        st = pool.stats()
+    assert st.failed == 1 and st.completed == 1 and st.submitted == 3

@@ -103,3 +103,20 @@ def test_qsun_parameters(pkg):
         pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, S=1.0)
     with pytest.raises(ValueError):
         pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, S=0.3)
+
+
+def test_pool_refuses_without_a_device_and_footprint_guards(pkg):
+    """With no CUDA device the pool is refused with a status (no host fallback),
+    and the footprint query rejects null arguments."""
+    import ctypes
+    import torch
+    from polfed_b200 import _lib
+    lib = pkg.load_library()
+    assert lib.pf_solve_footprint(None, None, 1, 1) == -1.0
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(_lib.PolfedError):
+        pkg.SolverPool(workers=2)
+    out = ctypes.c_void_p()
+    assert lib.pf_pool_create(0, 0, 0.0, ctypes.byref(out)) == _lib.PF_ERR_INVALID   # 0 workers
+    assert not out.value
