@@ -416,6 +416,202 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+# ------------------------------------------------ served stream and disorder batch
+SERVE = {"workload": "served stream: XXZ L=14..20 (Lup=L//2, W=5) and Quantum Sun L_grain=3, L_loc=10..15, "
+                     "eps~U[0.1,0.9], nev in {20,50,100,200}, s in {4,8,16}, Poisson arrivals",
+         "seed": 2025, "eigentol": 1e-10, "dos_N": 250, "dos_R": 300}
+DISORDER = {"workload": "disorder average: 256 x XXZ L=16 (D=12870) + 32 x XXZ L=18 (D=48620), Sz=0, "
+                        "Delta=1, W=3, nev=50, eps in {0.3,0.5,0.7}",
+            "seed": 31337, "eigentol": 1e-10, "dos_N": 250, "dos_R": 300, "nev": 50}
+
+
+def _serve_request(pkg, rng, device):
+    """One request of the mixed served stream (seeded)."""
+    import numpy as np
+    if rng.random() < 0.5:
+        L = int(rng.integers(14, 21))
+        op = pkg.xxz_hamiltonian(L, L // 2, 1.0, 1.0, 5.0, rng=rng, device=device)
+        name = f"xxz_L{L}"
+    else:
+        L_loc = int(rng.integers(10, 16))
+        op = pkg.qsun_hamiltonian(L_loc, 3, 1.0, 0.75, gamma=1.0, w=0.5, hz=1.0, zeta=0.2, rng=rng, device=device)
+        name = f"qsun_Lloc{L_loc}"
+    eps = float(rng.uniform(0.1, 0.9))
+    nev = int(rng.choice([20, 50, 100, 200]))
+    s = int(rng.choice([4, 8, 16]))
+    x0 = np.asfortranarray(rng.random((op.dim, s)))
+    return name, op, x0, eps, nev, s
+
+
+def run_serve(args, local_rank):
+    """A seeded Poisson request stream through the native request pool.
+    Requests are created and submitted at their arrival times; latency is
+    submit -> done (host clock, the pool's own record); throughput is the
+    converged pairs of all requests over the first arrival -> last completion."""
+    import numpy as np
+    import torch
+    import __graft_entry__ as ge
+    torch.cuda.set_device(local_rank)
+    pkg = ge.load_package()
+    pkg.load_library()
+    rng = np.random.default_rng(SERVE["seed"])
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=args.requests))
+    arrivals -= arrivals[0]
+    pool = pkg.SolverPool(workers=args.workers, device=local_rank)
+    # warm-up: one small request of each kind (library set-up, cuBLAS/cuSOLVER handles)
+    wrng = np.random.default_rng(1)
+    for _ in range(2):
+        name, op, x0, eps, nev, s = _serve_request(pkg, wrng, local_rank)
+        pool.result(pool.submit(op, x0, 20, ("rescaled", eps), dos=pkg.DoSConfig(N=64, R=16, seed=1)))
+    torch.cuda.synchronize()
+    base = pool.stats()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ids, meta = [], []
+    t0 = time.perf_counter()
+    for i in range(args.requests):
+        delay = t0 + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        name, op, x0, eps, nev, s = _serve_request(pkg, rng, local_rank)
+        rid = pool.submit(op, x0, nev, ("rescaled", eps), produce_report=True, vecs=False,
+                          dos=pkg.DoSConfig(N=SERVE["dos_N"], R=SERVE["dos_R"], seed=SERVE["seed"] + i),
+                          fact=pkg.FactorizationConfig(eigentol=SERVE["eigentol"]))
+        ids.append(rid)
+        meta.append((name, op, op.dim, nev, s, eps))
+    nconv, per = 0, []
+    for rid, (name, op, D, nev, s, eps) in zip(ids, meta):
+        vals, _, rep = pool.result(rid)
+        nconv += len(vals)
+        per.append({"model": name, "D": D, "nev": nev, "s": s, "eps": round(eps, 3), "converged": len(vals),
+                    "K": rep.spectral.order, "solve_s": round(rep.benchmark.stage_seconds["total"], 4)})
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    st = pool.stats()
+    pool.close()
+    lat = sorted(p["solve_s"] for p in per)
+    out = {
+        "metric": "converged eigenpairs/s at resid<=1e-10 (served stream)", "value": nconv / wall,
+        "unit": "eigenpairs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded request stream)",
+        "config": dict(SERVE, requests=args.requests, rate_per_s=args.rate, workers=args.workers),
+        "latency_s": {"p50": st.p50_latency, "p99": st.p99_latency, "mean": st.mean_latency,
+                      "note": "submit -> done, host clock, queueing included"},
+        "solve_seconds": {"p50": lat[len(lat) // 2], "max": lat[-1]},
+        "wall_seconds": wall, "busy_seconds": st.busy_seconds - base.busy_seconds,
+        "converged": nconv, "completed": st.completed - base.completed, "failed": st.failed - base.failed,
+        "hbm": {"budget_bytes": st.bytes_budget, "peak_admitted_bytes": st.bytes_peak},
+        "clocks": clocks, "requests": per,
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def _disorder_problems(pkg, device):
+    import numpy as np
+    probs = []
+    for i in range(288):
+        L = 16 if i < 256 else 18
+        rng = np.random.default_rng(DISORDER["seed"] + i)
+        op = pkg.xxz_hamiltonian(L, L // 2, 1.0, 1.0, 3.0, rng=rng, device=device)
+        probs.append((op, (0.3, 0.5, 0.7)[i % 3], rng))
+    return probs
+
+
+def run_disorder(args, local_rank):
+    """The disorder average: 288 realisations through the request pool, block
+    size per L picked by timing s in {4, 8, 16} on one realisation, against
+    the same realisations solved one at a time."""
+    import numpy as np
+    import torch
+    import __graft_entry__ as ge
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    pkg = ge.load_package()
+    pkg.load_library()
+    probs = _disorder_problems(pkg, local_rank)
+    kw = lambda seed: dict(fact=pkg.FactorizationConfig(eigentol=DISORDER["eigentol"]), vecs=False,
+                           dos=pkg.DoSConfig(N=DISORDER["dos_N"], R=DISORDER["dos_R"], seed=seed))
+    nev = DISORDER["nev"]
+    # block-size tuner (outside the timed region): converged pairs per second of one solve
+    best_s, tune = {}, {}
+    for L, i in ((16, 0), (18, 256)):
+        op = probs[i][0]
+        rates = {}
+        for s in (4, 8, 16):
+            x0 = np.random.default_rng(7).random((op.dim, s))
+            pkg.polfed(op, x0, nev, ("rescaled", 0.5), **kw(1))   # warm-up and step-width tuning
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            vals, _ = pkg.polfed(op, x0, nev, ("rescaled", 0.5), **kw(1))
+            torch.cuda.synchronize()
+            rates[s] = len(vals) / (time.perf_counter() - t)
+        best_s[L] = max(rates, key=rates.get)
+        tune[f"L{L}"] = {str(k): round(v, 2) for k, v in rates.items()}
+    x0s = []
+    for op, eps, rng in probs:
+        s = best_s[16 if op.dim == 12870 else 18]
+        x0s.append(np.asfortranarray(rng.random((op.dim, s))))
+    pool = pkg.SolverPool(workers=args.workers, device=local_rank)
+    streams = [torch.cuda.ExternalStream(st, device=dev) for st in pool.streams()]
+    tstream = torch.cuda.Stream(device=dev)
+
+    def timed_pool(idx):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(tstream)
+        for ws in streams:
+            ws.wait_event(e0)
+        nconv = 0
+        for eps in (0.3, 0.5, 0.7):   # one batch per target (one parameter set per batch)
+            sel = [i for i in idx if probs[i][1] == eps]
+            for vals, _ in pool.solve_batch([probs[i][0] for i in sel], [x0s[i] for i in sel], nev,
+                                            ("rescaled", eps), **kw(5)):
+                nconv += len(vals)
+        for ws in streams:
+            ev = torch.cuda.Event()
+            ev.record(ws)
+            tstream.wait_event(ev)
+        e1.record(tstream)
+        e1.synchronize()
+        return nconv, e0.elapsed_time(e1) * 1e-3
+
+    timed_pool(list(range(0, 288, 24)))   # warm-up
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    n_pool, t_pool = timed_pool(list(range(288)))
+    clocks = sampler.stop()
+    # the single-solve form: one at a time on the library's stream, every 4th realisation
+    from polfed_b200 import _lib
+    st = torch.cuda.ExternalStream(_lib.stream_of(_lib.handle(local_rank)), device=dev)
+    sub = list(range(0, 288, 4))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    n_single = 0
+    for i in sub:
+        vals, _ = pkg.polfed(probs[i][0], x0s[i], nev, ("rescaled", probs[i][1]), **kw(5))
+        n_single += len(vals)
+    e1.record(st)
+    e1.synchronize()
+    t_single = e0.elapsed_time(e1) * 1e-3
+    pool.close()
+    out = {
+        "metric": "converged eigenpairs/s at resid<=1e-10 (disorder batch)", "value": n_pool / t_pool,
+        "unit": "eigenpairs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic (seeded realisations)",
+        "config": dict(DISORDER, workers=args.workers, blocksize={f"L{k}": v for k, v in best_s.items()}),
+        "blocksize_tuning_pairs_per_s": tune,
+        "seconds": t_pool, "converged": n_pool,
+        "single_solve": {"value": n_single / t_single, "unit": "eigenpairs/s", "realisations": len(sub),
+                         "converged": n_single, "seconds": t_single},
+        "clocks": clocks,
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def profile_step():
     """Two order-30 Chebyshev filters on one realisation of the workload's
     operator (s = 8, FP64) with the autotuned step: a small, bounded case for
@@ -447,6 +643,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch", type=int, default=4, help="solves in flight together per step")
+    ap.add_argument("--serve", action="store_true", help="run the seeded Poisson request stream instead")
+    ap.add_argument("--disorder", action="store_true", help="run the 288-realisation disorder batch instead")
+    ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--rate", type=float, default=0.5, help="served stream arrivals per second")
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--profile-step", action="store_true",
                     help="only run two short Chebyshev filters on one realisation (a bounded case for ncu)")
     args = ap.parse_args()
@@ -458,6 +659,10 @@ def main():
         return run_reference(args, rank, world)
     if args.profile_step:
         return profile_step()
+    if args.serve:
+        return run_serve(args, local_rank)
+    if args.disorder:
+        return run_disorder(args, local_rank)
     if world > 1:
         import datetime
         import torch

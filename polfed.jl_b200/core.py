@@ -502,10 +502,7 @@ class SolverPool:
         out = []
         for i in range(n):
             k = nconv[i]
-            if want_vecs:
-                V = vecs[i][:, :k] if on_device else vecs[i][:, :k].copy()
-            else:
-                V = None
+            V = vecs[i][:, :k] if want_vecs else None   # a view: no second pass over D x nev
             res = (vals[i][:k].copy(), V)
             if want_rep:
                 res = res + (_make_report(reps[i], kind, val),)
