@@ -481,16 +481,25 @@ def run_serve(args, local_rank):
         meta.append((name, op, op.dim, nev, s, eps))
     nconv, per = 0, []
     for rid, (name, op, D, nev, s, eps) in zip(ids, meta):
-        vals, _, rep = pool.result(rid)
+        item = {"model": name, "D": D, "nev": nev, "s": s, "eps": round(eps, 3)}
+        try:
+            vals, _, rep = pool.result(rid)
+        except pkg._lib.PolfedError as e:
+            # the reference raises the same for an infeasible request (e.g. fewer
+            # states near the target than nev); the request fails, the stream goes on
+            item["error"] = str(e)
+            per.append(item)
+            continue
         nconv += len(vals)
-        per.append({"model": name, "D": D, "nev": nev, "s": s, "eps": round(eps, 3), "converged": len(vals),
-                    "K": rep.spectral.order, "solve_s": round(rep.benchmark.stage_seconds["total"], 4)})
+        item.update({"converged": len(vals), "K": rep.spectral.order,
+                     "solve_s": round(rep.benchmark.stage_seconds["total"], 4)})
+        per.append(item)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     st = pool.stats()
     pool.close()
-    lat = sorted(p["solve_s"] for p in per)
+    lat = sorted(p["solve_s"] for p in per if "solve_s" in p) or [0.0]
     out = {
         "metric": "converged eigenpairs/s at resid<=1e-10 (served stream)", "value": nconv / wall,
         "unit": "eigenpairs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
@@ -635,6 +644,85 @@ def profile_step():
     return 0
 
 
+STEP_CASES = [
+    # (name, constructor, s)
+    ("qsun_Lloc13_D65536", lambda pkg, rng: pkg.qsun_hamiltonian(13, 3, 1.0, 0.75, rng=rng), 8),
+    ("xxz_L16_D12870", lambda pkg, rng: pkg.xxz_hamiltonian(16, 8, 1.0, 1.0, 3.0, rng=rng), 16),
+    ("xxz_L20_D184756", lambda pkg, rng: pkg.xxz_hamiltonian(20, 10, 1.0, 1.0, 5.0, rng=rng), 16),
+    ("j1j2_L24_D2704156", lambda pkg, rng: pkg.j1j2_hamiltonian(24, 12, 1.0, 0.5, 1.0, 1.0, 1.0, rng=rng), 16),
+]
+
+
+def step_sweep(large_only=False):
+    """Per-step time of the Clenshaw recurrence step across sizes and
+    precisions: (t(K=40) - t(K=20)) / 20 from CUDA events on the library's
+    stream around pf_filter, so the layout copies and set-up cancel.
+    Algorithmic bytes per step 4 * D * s * w; fraction of the measured HBM
+    copy peak."""
+    import numpy as np
+    import torch
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+    from polfed_b200 import _lib
+    pkg.load_library()
+    peak, peak_kind = read_peaks()
+    st = torch.cuda.ExternalStream(_lib.stream_of(_lib.handle(0)), device="cuda:0")
+    cases = STEP_CASES[-1:] if large_only else STEP_CASES
+    for name, make, s in cases:
+        op = make(pkg, np.random.default_rng(3))
+        D = op.dim
+        for dt, tdt, w in (("fp64", torch.float64, 8), ("fp32", torch.float32, 4)):
+            width, _ = pkg.autotune(op, s, dt)
+            X = pkg.col_major(D, s, dtype=tdt)
+            X.copy_(torch.rand(D, s, dtype=tdt, device="cuda:0"))
+            Y = pkg.col_major(D, s, dtype=tdt)
+
+            def t_filter(K, reps=3):
+                c = np.cos(np.arange(K + 1) * 0.7) * 0.05
+                pkg.chebyshev_filter(op, Y, X, c, a=2.0 * s, b=0.0)   # warm-up
+                best = None
+                for _ in range(reps):
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    pkg.chebyshev_filter(op, Y, X, c, a=2.0 * s, b=0.0)
+                    e1.record(st)
+                    e1.synchronize()
+                    t = e0.elapsed_time(e1) * 1e-3
+                    best = t if best is None else min(best, t)
+                return best
+
+            per = (t_filter(40) - t_filter(20)) / 20
+            alg = 4.0 * D * s * w
+            print(json.dumps({"case": name, "D": D, "s": s, "dtype": dt, "width": width,
+                              "us_per_step": per * 1e6, "alg_bytes": alg, "achieved_gbs": alg / per / 1e9,
+                              "frac": alg / per / 1e9 / peak, "peak": peak, "peak_kind": peak_kind}), flush=True)
+            del X, Y
+    return 0
+
+
+def profile_step_large(dtype="fp64"):
+    """Two order-2 Chebyshev filters on the J1-J2 L=24 Sz=0 operator
+    (D = 2,704,156, s = 16): a bounded large-D case for ncu captures."""
+    import numpy as np
+    import torch
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+    name, make, s = STEP_CASES[-1]
+    op = make(pkg, np.random.default_rng(3))
+    tdt = torch.float64 if dtype == "fp64" else torch.float32
+    width, _ = pkg.autotune(op, s, dtype)
+    X = pkg.col_major(op.dim, s, dtype=tdt)
+    X.copy_(torch.rand(op.dim, s, dtype=tdt, device="cuda:0"))
+    Y = pkg.col_major(op.dim, s, dtype=tdt)
+    c = np.array([0.1, 0.2, 0.3])
+    for _ in range(2):
+        pkg.chebyshev_filter(op, Y, X, c, a=2.0 * s, b=0.0)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_step_large": True, "D": op.dim, "s": s, "dtype": dtype, "width": width}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -648,6 +736,10 @@ def main():
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=0.5, help="served stream arrivals per second")
     ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--step-sweep", action="store_true", help="time the Clenshaw step across sizes and precisions")
+    ap.add_argument("--large-only", action="store_true", help="with --step-sweep: only the J1-J2 L=24 case")
+    ap.add_argument("--profile-step-large", choices=["fp64", "fp32"], default=None,
+                    help="two order-2 filters on J1-J2 L=24 (a bounded large-D case for ncu)")
     ap.add_argument("--profile-step", action="store_true",
                     help="only run two short Chebyshev filters on one realisation (a bounded case for ncu)")
     args = ap.parse_args()
@@ -659,6 +751,10 @@ def main():
         return run_reference(args, rank, world)
     if args.profile_step:
         return profile_step()
+    if args.step_sweep:
+        return step_sweep(args.large_only)
+    if args.profile_step_large:
+        return profile_step_large(args.profile_step_large)
     if args.serve:
         return run_serve(args, local_rank)
     if args.disorder:

@@ -160,11 +160,18 @@ int pf_kpm_moments(pf_op *op, int dtype, double a, double b, int N, int R,
                    double *mu);
 
 /* Autotuner (no reference counterpart: the reference has no kernel variants).
- * Times every columns-per-thread width of the Clenshaw step kernel for block
- * width s and dtype on scratch blocks, keeps the fastest for this operator and
- * returns it in *width; times_ms[i] (optional, 5 entries) receives the
- * measured milliseconds per launch of widths 1, 2, 4, 8, 16 (0 if invalid). */
+ * Times every variant of the Clenshaw step kernel for block width s and dtype
+ * on scratch blocks -- 1, 2, 4, 8 or 16 columns per thread, and for chain
+ * operators with s in {4, 8, 16, 32} the warp-cooperative step (width
+ * PF_WIDTH_COOP: the s lanes of a warp share one row) -- keeps the fastest
+ * for this operator and returns it in *width; times_ms[i] (optional, 6
+ * entries) receives the measured milliseconds per launch of widths 1, 2, 4,
+ * 8, 16 and PF_WIDTH_COOP (0 where not offered). */
+#define PF_WIDTH_COOP 0
 int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms);
+/* Pin the step-kernel variant for (dtype, s) without timing (a width the
+ * autotuner could have chosen); later launches on this operator use it. */
+int pf_set_step_width(pf_op *op, int dtype, int s, int width);
 
 /* ----------------------------------------------------------- solving */
 typedef struct pf_params {

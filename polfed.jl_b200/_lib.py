@@ -26,13 +26,14 @@ KERNEL_IDS = {"Jackson": 0, "Lorentz": 1, "Fejer": 2, "LanczosK": 3, "WangZunger
 PF_PROBE_GAUSSIAN, PF_PROBE_RADEMACHER = 0, 1
 PF_PREC_FP64, PF_PREC_MIXED = 0, 1
 PF_REPORT_MAX_CHECKS = 128
+PF_WIDTH_COOP = 0
 
 EXPORTED = [
     "pf_abi_version", "pf_last_error", "pf_handle_create", "pf_handle_destroy", "pf_handle_stream",
     "pf_handle_synchronize", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_destroy",
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
-    "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind",
+    "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind", "pf_set_step_width",
     "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
 ]
@@ -135,6 +136,7 @@ def load():
                            ctypes.POINTER(pf_report), ctypes.POINTER(i32)]),
         "pf_lanczos_extrema": (i32, [vp, vp, i32, f64, f64, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
         "pf_autotune": (i32, [vp, i32, i32, ctypes.POINTER(i32), vp]),
+        "pf_set_step_width": (i32, [vp, i32, i32, i32]),
         "pf_pool_create": (i32, [i32, i32, f64, ctypes.POINTER(vp)]),
         "pf_pool_destroy": (i32, [vp]),
         "pf_pool_stream": (i32, [vp, i32, ctypes.POINTER(vp)]),

@@ -712,13 +712,22 @@ def kpm_moments(op: Operator, N: int, R: int, a: float = 1.0, b: float = 0.0, pr
 
 
 def autotune(op: Operator, s: int, dtype: str = "fp64"):
-    """Time every columns-per-thread width of the step kernel for block width
-    ``s``; the fastest is kept on the operator.  Returns (width, {width: ms})."""
+    """Time every variant of the step kernel for block width ``s`` (1..16
+    columns per thread, and width 0 = the warp-cooperative chain step where
+    offered); the fastest is kept on the operator.  Returns
+    (width, {width: ms})."""
     w = ctypes.c_int(0)
-    t = (ctypes.c_float * 5)()
+    t = (ctypes.c_float * 6)()
     dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
     _lib.check(_lib.load().pf_autotune(op.op, dt, int(s), ctypes.byref(w), ctypes.addressof(t)))
-    return w.value, {1 << i: t[i] for i in range(5) if t[i] > 0}
+    widths = [1, 2, 4, 8, 16, _lib.PF_WIDTH_COOP]
+    return w.value, {widths[i]: t[i] for i in range(6) if t[i] > 0}
+
+
+def set_step_width(op: Operator, s: int, width: int, dtype: str = "fp64"):
+    """Pin the step-kernel variant for block width ``s`` (see ``autotune``)."""
+    dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
+    _lib.check(_lib.load().pf_set_step_width(op.op, dt, int(s), int(width)))
 
 
 def basis_states(op: Operator, idx):

@@ -208,13 +208,34 @@ int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms) {
     std::vector<std::pair<int, float>> t;
     *width = pf::autotune_step(op, s, dtype, &t);
     if (times_ms) {
-        for (int i = 0; i < 5; ++i) times_ms[i] = 0.f;
+        for (int i = 0; i < 6; ++i) times_ms[i] = 0.f;
         for (auto &pr : t) {
-            int idx = 0;
-            while ((1 << idx) < pr.first) ++idx;
-            if (idx < 5) times_ms[idx] = pr.second;
+            int idx = 5;  // PF_WIDTH_COOP
+            if (pr.first != PF_WIDTH_COOP) {
+                idx = 0;
+                while ((1 << idx) < pr.first) ++idx;
+            }
+            if (idx < 6) times_ms[idx] = pr.second;
         }
     }
+    PF_API_END
+}
+
+int pf_set_step_width(pf_op *op, int dtype, int s, int width) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    PF_CHECK(dtype == PF_F64 || dtype == PF_F32, PF_ERR_INVALID, "dtype must be PF_F64 or PF_F32");
+    PF_CHECK(s >= 1, PF_ERR_INVALID, "s must be positive");
+    const int elem = dtype == PF_F64 ? 8 : 4;
+    if (width == PF_WIDTH_COOP) {
+        PF_CHECK(pf::coop_eligible(op, s, pf::StepFlags::Q | pf::StepFlags::P | pf::StepFlags::X), PF_ERR_INVALID,
+                 "the warp-cooperative step needs a chain operator and s in {4, 8, 16, 32}");
+    } else {
+        PF_CHECK(width >= 1 && (width & (width - 1)) == 0 && s % width == 0 && width * elem <= 64, PF_ERR_INVALID,
+                 "width must be a power of two dividing s with at most 64 bytes of columns");
+    }
+    std::lock_guard<std::mutex> lock(op->tune_mu);
+    op->tuned_width[std::make_pair(elem, s)] = width;
     PF_API_END
 }
 

@@ -71,6 +71,7 @@ struct ChainDesc {
     T hhalf[PF_MAX_SITES];         // h_i / 2            (h Sz with Sz = +-1/2)
     const uint32_t *states;        // D basis states (sector only)
     const uint32_t *rank_tab;      // chunked rank tables (sector only)
+    const T *diag;                 // D diagonal elements (k_chain_diag), or null
 };
 
 // Spin-1/2 Quantum Sun in the full space; grain = the low L_grain bits.
@@ -127,6 +128,8 @@ struct pf_op {
     pf::QSunDesc<float> qsun32;
     uint32_t *d_states = nullptr;
     uint32_t *d_rank_tab = nullptr;
+    double *d_diag64 = nullptr;       // chain diagonal in each precision (warp-cooperative step)
+    float *d_diag32 = nullptr;
     // owns d_states / d_rank_tab; shared with the views pf_op_bind makes on other handles
     std::shared_ptr<void> tables_owner;
     int smem_bytes = 0;               // dynamic shared memory of the step kernels
@@ -159,12 +162,17 @@ void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const
                  const T *x, T *out, double cx, double alpha, double beta, double inva,
                  double shift, int flags, double *dots);
 
-// Same with an explicit columns-per-thread width V (s % V == 0, V*sizeof(T) <= 64).
+// Same with an explicit columns-per-thread width V (s % V == 0, V*sizeof(T) <= 64),
+// or V == kCoopWidth: the warp-cooperative chain step (coop_eligible).
 template <typename T>
 void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p, const T *x, T *out,
                        double cx, double alpha, double beta, double inva, double shift, int flags, double *dots,
                        int V);
 int default_width(int s, int elem_bytes);
+constexpr int kCoopWidth = 0;
+bool coop_eligible(const pf_op *op, int s, int flags);
+// Diagonal of a chain operator in both precisions (same term order as the step kernels).
+void build_chain_diag(pf_op *op);
 // Times every columns-per-thread width of the Clenshaw step for (s, dtype) on
 // scratch blocks and records the fastest in op->tuned_width.  Returns it.
 int autotune_step(pf_op *op, int s, int dtype, std::vector<std::pair<int, float>> *timings);

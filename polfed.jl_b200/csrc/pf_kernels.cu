@@ -375,6 +375,105 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T, V>::value) k_step(const
     }
 }
 
+// ------------------------------------------------ warp-cooperative chain step
+// Diagonal of a chain row: fields in site order, then the Sz Sz term of every
+// bond in bond order -- the same sequence of additions chain_row performs, so
+// the stored diagonal equals the one the per-thread kernels compute.
+template <typename T>
+__device__ __forceinline__ T chain_diag(const ChainDesc<T> &d, uint32_t st) {
+    T dg = T(0);
+    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
+    for (int b = 0; b < d.nb; ++b) {
+        const uint32_t bm = d.bmask[b];
+        const uint32_t m = st & bm;
+        const bool differ = (m != 0u) && (m != bm);
+        dg += differ ? -d.jdq[b] : d.jdq[b];
+    }
+    return dg;
+}
+
+template <typename T>
+__global__ void k_chain_diag(const ChainDesc<T> d, uint32_t D, T *__restrict__ out) {
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < D; row += gridDim.x * blockDim.x) {
+        const uint32_t st = d.full ? row : __ldg(d.states + row);
+        out[row] = chain_diag<T>(d, st);
+    }
+}
+
+// One row per S lanes (S = s, a power of two <= 32), one column per lane.  The
+// lanes of a row split its bonds: lane l ranks the flipped states of bonds
+// l, l+S, l+2S, ...; one shuffle per bond hands the rank to every lane of the
+// row, and each lane gathers its own column.  A round issues S independent
+// gathers per lane with one register each, and the row's rank work is done
+// once instead of once per column group.  Gathers are accumulated in bond
+// order and the diagonal comes from k_chain_diag, so every output equals the
+// per-thread kernel's.  Shared memory: the bond masks (lane-indexed, so not
+// read from the kernel parameters), then the rank tables.
+template <typename T, int S, int FLAGS>
+__global__ void __launch_bounds__(kThreads) k_step_coop(const ChainDesc<T> d, const StepArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool HASQ = (FLAGS & StepFlags::Q) != 0;
+    constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
+    constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
+    uint32_t *sbm = reinterpret_cast<uint32_t *>(smem_raw);
+    uint32_t *tab = sbm + PF_MAX_BONDS;
+    if constexpr (HASQ) {
+        for (int i = threadIdx.x; i < d.nb; i += blockDim.x) sbm[i] = d.bmask[i];
+        if (!d.full) {
+            const int n = rank_table_entries(d.nchunks);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) tab[i] = __ldg(d.rank_tab + i);
+        }
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const int lr = lane & (S - 1);   // this lane's column
+    const int rb = lane & ~(S - 1);  // first lane of this lane's row
+    const uint64_t total = (uint64_t)a.D * S;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    // warp-uniform loop: every lane of a warp runs the same iterations (shuffles)
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < total; base += stride) {
+        const uint64_t t = base + lane;
+        const bool valid = t < total;
+        const uint32_t row = valid ? (uint32_t)(t / S) : 0u;
+        T acc = T(0);
+        if constexpr (HASQ) {
+            const uint32_t st = valid ? (d.full ? row : __ldg(d.states + row)) : 0u;
+            const T *qc = a.q + lr;
+            for (int b0 = 0; b0 < d.nb; b0 += S) {
+                uint32_t mine = 0xffffffffu;  // rank of this lane's flipped state, or inactive
+                const int b = b0 + lr;
+                if (valid && b < d.nb) {
+                    const uint32_t bm = sbm[b];
+                    const uint32_t m = st & bm;
+                    if (m != 0u && m != bm) mine = d.full ? (st ^ bm) : sector_rank(st ^ bm, tab, d.nchunks);
+                }
+                uint32_t r[S];
+                T g[S];
+#pragma unroll
+                for (int j = 0; j < S; ++j) {
+                    r[j] = __shfl_sync(0xffffffffu, mine, rb + j);
+                    g[j] = (r[j] != 0xffffffffu) ? __ldg(qc + (size_t)r[j] * S) : T(0);
+                }
+#pragma unroll
+                for (int j = 0; j < S; ++j)
+                    if (r[j] != 0xffffffffu) acc += d.jhalf[b0 + j] * g[j];
+            }
+        }
+        if (valid) {
+            const size_t off = (size_t)t;
+            T res = T(0);
+            if constexpr (HASX) res = a.cx * a.x[off];
+            if constexpr (HASQ) {
+                const T qo = a.q[off];
+                const T hq = (acc + d.diag[row] * qo) * a.inva - a.boa * qo;
+                res = res + a.alpha * hq;
+            }
+            if constexpr (HASP) res = res + a.beta * a.p[off];
+            a.out[off] = res;
+        }
+    }
+}
+
 static thread_local int64_t t_launches = 0;
 void count_launches(int64_t n) { t_launches += n; }
 int64_t thread_launches() { return t_launches; }
@@ -480,6 +579,66 @@ static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int fl
     }
 }
 
+bool coop_eligible(const pf_op *op, int s, int flags) {
+    return op->kind == OP_CHAIN && op->d_diag64 != nullptr && op->d_diag32 != nullptr &&
+           (s == 4 || s == 8 || s == 16 || s == 32) && (flags & StepFlags::DOTS) == 0;
+}
+
+template <typename T, int S, int FLAGS>
+static void launch_coop_one(pf_op *op, cudaStream_t st, const ChainDesc<T> &d, const StepArgs<T> &a) {
+    auto kern = k_step_coop<T, S, FLAGS>;
+    int smem = PF_MAX_BONDS * 4;
+    if ((FLAGS & StepFlags::Q) && !d.full) smem += rank_table_entries(d.nchunks) * 4;
+    if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int grid = grid_for(op->h, (int64_t)a.D * S, kThreads, blocks_per_sm((const void *)kern, smem));
+    kern<<<grid, kThreads, smem, st>>>(d, a);
+    PF_CUDA(cudaGetLastError());
+    count_launches(1);
+}
+
+template <typename T, int S>
+static void coop_flags(pf_op *op, cudaStream_t st, const ChainDesc<T> &d, const StepArgs<T> &a, int flags) {
+    using F = StepFlags;
+    switch (flags) {
+        case F::X: launch_coop_one<T, S, F::X>(op, st, d, a); break;
+        case F::Q: launch_coop_one<T, S, F::Q>(op, st, d, a); break;
+        case F::Q | F::X: launch_coop_one<T, S, F::Q | F::X>(op, st, d, a); break;
+        case F::Q | F::P: launch_coop_one<T, S, F::Q | F::P>(op, st, d, a); break;
+        case F::Q | F::P | F::X: launch_coop_one<T, S, F::Q | F::P | F::X>(op, st, d, a); break;
+        default: throw Error(PF_ERR_INVALID, "unsupported step flag combination");
+    }
+}
+
+template <typename T>
+static void launch_coop(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int flags) {
+    const ChainDesc<T> &d = chain_of<T>(op);
+    PF_CHECK(d.diag != nullptr, PF_ERR_INVALID, "chain diagonal missing");
+    switch (a.s) {
+        case 4: coop_flags<T, 4>(op, st, d, a, flags); break;
+        case 8: coop_flags<T, 8>(op, st, d, a, flags); break;
+        case 16: coop_flags<T, 16>(op, st, d, a, flags); break;
+        case 32: coop_flags<T, 32>(op, st, d, a, flags); break;
+        default: throw Error(PF_ERR_INVALID, "the warp-cooperative step needs s in {4, 8, 16, 32}");
+    }
+}
+
+void build_chain_diag(pf_op *op) {
+    PF_CHECK(op->kind == OP_CHAIN, PF_ERR_INVALID, "not a chain operator");
+    const uint64_t D = (uint64_t)op->dim;
+    if ((double)D * 12.0 > 4.0 * (double)(1ull << 30)) return;  // the cooperative step is not offered
+    PF_CUDA(cudaMalloc(&op->d_diag64, D * sizeof(double)));
+    PF_CUDA(cudaMalloc(&op->d_diag32, D * sizeof(float)));
+    cudaStream_t st = op->h->stream;
+    const int grid = grid_for(op->h, (int64_t)D, kThreads, 8);
+    k_chain_diag<double><<<grid, kThreads, 0, st>>>(op->chain64, (uint32_t)D, op->d_diag64);
+    k_chain_diag<float><<<grid, kThreads, 0, st>>>(op->chain32, (uint32_t)D, op->d_diag32);
+    PF_CUDA(cudaGetLastError());
+    count_launches(2);
+    PF_CUDA(cudaStreamSynchronize(st));
+    op->chain64.diag = op->d_diag64;
+    op->chain32.diag = op->d_diag32;
+}
+
 // Columns per thread: the widest power of two dividing s within one 64-byte
 // run by default, or the width the autotuner measured fastest for (s, dtype).
 int default_width(int s, int elem_bytes) {
@@ -495,17 +654,25 @@ void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q,
                        int V) {
     PF_CHECK(D == op->dim, PF_ERR_INVALID, "block height does not match the operator dimension");
     PF_CHECK(s >= 1, PF_ERR_INVALID, "block must have at least one column");
-    PF_CHECK(V >= 1 && s % V == 0 && V * (int)sizeof(T) <= 64, PF_ERR_INVALID, "invalid columns-per-thread width");
+    const bool coop = (V == kCoopWidth);
+    PF_CHECK(!coop || coop_eligible(op, s, flags), PF_ERR_INVALID,
+             "the warp-cooperative step needs a chain operator, s in {4, 8, 16, 32} and no fused dots");
+    PF_CHECK(coop || (V >= 1 && s % V == 0 && V * (int)sizeof(T) <= 64), PF_ERR_INVALID,
+             "invalid columns-per-thread width");
     StepArgs<T> a;
     a.D = (uint32_t)D;
     a.s = s;
-    a.G = s / V;
+    a.G = coop ? s : s / V;
     PF_CHECK((int64_t)D * a.G < (int64_t)0xffffffffLL, PF_ERR_UNSUPPORTED, "block too large for one launch");
     a.items = (uint32_t)(D * a.G);
     a.q = q; a.p = p; a.x = x; a.out = out;
     a.cx = (T)cx; a.alpha = (T)alpha; a.beta = (T)beta;
     a.inva = (T)inva; a.boa = (T)(shift * inva);
     a.partials = nullptr; a.counter = nullptr; a.dots = dots;
+    if (coop) {
+        launch_coop<T>(op, st, a, flags);
+        return;
+    }
     if (flags & StepFlags::DOTS)
         PF_CHECK(kThreads % a.G == 0, PF_ERR_UNSUPPORTED, "fused dots need s/V to divide 256");
     switch (V) {
@@ -535,6 +702,7 @@ void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const
         V = default_width(s, (int)sizeof(T));
         while (V > 1 && (V * (int)sizeof(T) > 32 || kThreads % (s / V) != 0)) V /= 2;
     }
+    if (V == kCoopWidth && !coop_eligible(op, s, flags)) V = default_width(s, (int)sizeof(T));
     launch_step_width<T>(op, st, D, s, q, p, x, out, cx, alpha, beta, inva, shift, flags, dots, V);
 }
 

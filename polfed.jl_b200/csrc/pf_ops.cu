@@ -130,20 +130,27 @@ pf_op *create_spin_chain(pf_handle *h, int L, int Lup, int nbonds, const int32_t
             std::vector<uint32_t> tab = build_rank_tables(nchunks);
             PF_CUDA(cudaMalloc(&op->d_rank_tab, tab.size() * sizeof(uint32_t)));
             PF_CUDA(cudaMemcpy(op->d_rank_tab, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-            uint32_t *tst = op->d_states, *trk = op->d_rank_tab;
-            const int dev = h->device;
-            op->tables_owner = std::shared_ptr<void>(nullptr, [tst, trk, dev](void *) {
-                cudaSetDevice(dev);
-                cudaFree(tst);
-                cudaFree(trk);
-            });
         }
         fill_chain(op->chain64, op);
         fill_chain(op->chain32, op);
+        build_chain_diag(op);
+        uint32_t *tst = op->d_states, *trk = op->d_rank_tab;
+        double *tdg = op->d_diag64;
+        float *tdf = op->d_diag32;
+        const int dev = h->device;
+        op->tables_owner = std::shared_ptr<void>(nullptr, [tst, trk, tdg, tdf, dev](void *) {
+            cudaSetDevice(dev);
+            cudaFree(tst);
+            cudaFree(trk);
+            cudaFree(tdg);
+            cudaFree(tdf);
+        });
     } catch (...) {
         if (!op->tables_owner) {
             if (op->d_states) cudaFree(op->d_states);
             if (op->d_rank_tab) cudaFree(op->d_rank_tab);
+            if (op->d_diag64) cudaFree(op->d_diag64);
+            if (op->d_diag32) cudaFree(op->d_diag32);
         }
         delete op;
         throw;
@@ -206,6 +213,8 @@ pf_op *bind_op(const pf_op *src, pf_handle *h) {
     op->qsun32 = src->qsun32;
     op->d_states = src->d_states;
     op->d_rank_tab = src->d_rank_tab;
+    op->d_diag64 = src->d_diag64;
+    op->d_diag32 = src->d_diag32;
     op->tables_owner = src->tables_owner;
     op->smem_bytes = src->smem_bytes;
     {

@@ -2,8 +2,10 @@
 //
 // The Clenshaw / KPM / apply step can give each thread 1..16 columns of a
 // row (more columns per thread amortise the per-row basis-state, diagonal
-// and flip-rank work; fewer raise occupancy and parallelism).  The best
-// width depends on the model, s, dtype and D, so it is measured: every
+// and flip-rank work; fewer raise occupancy and parallelism), or, for chain
+// operators, share each row among s lanes of a warp (width 0, the
+// warp-cooperative step).  The best choice depends on the model, s, dtype
+// and D, so it is measured: every
 // valid width runs the recurrence step (the filter's dominant launch) on
 // scratch blocks, timed with CUDA events on the handle's stream, and the
 // fastest is cached on the operator for all later launches.
@@ -36,8 +38,11 @@ static int tune_typed(pf_op *op, int s, std::vector<std::pair<int, float>> *timi
         const int reps = 20;
         // The recurrence b_k = c X + 2 Ht b_{k+1} - b_{k+2} with a norm-preserving
         // scaling (alpha = 0.5, beta = -0.25) keeps the scratch data bounded.
-        for (int V = 1; V <= vmax; V *= 2) {
-            if (s % V) continue;
+        std::vector<int> widths;
+        for (int V = 1; V <= vmax; V *= 2)
+            if (s % V == 0) widths.push_back(V);
+        if (coop_eligible(op, s, StepFlags::Q | StepFlags::P | StepFlags::X)) widths.push_back(kCoopWidth);
+        for (int V : widths) {
             for (int r = 0; r < 3; ++r)
                 launch_step_width<T>(op, st, D, s, q, p, x, p, 0.1, 0.5, -0.25, 0.05, 0.0,
                                      StepFlags::Q | StepFlags::P | StepFlags::X, nullptr, V);

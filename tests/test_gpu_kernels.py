@@ -144,6 +144,68 @@ def test_apply_fp32(pkg, orc, cuda, models, s):
         assert err < RTOL32, (name, err)
 
 
+@pytest.mark.parametrize("s", [4, 8, 16, 32])
+def test_coop_step_matches_per_thread_and_oracle(pkg, orc, cuda, models, s):
+    """The warp-cooperative chain step (width 0) against the per-thread step
+    and the oracle: apply, the rescaled apply, the diagonal (bit-exact) and a
+    K = 40 filter, in FP64 and FP32."""
+    rng = np.random.default_rng(100 + s)
+    for name, op, H in models:
+        if op.kind != "spin_chain":
+            continue
+        D = H.shape[0]
+        Ht = orc.CSROperator(H)
+        for dt, dts, tol in ((cuda.float64, "fp64", RTOL64), (cuda.float32, "fp32", RTOL32)):
+            per_thread = min(s, 64 // (8 if dts == "fp64" else 4))
+            X = rng.standard_normal((D, s))
+            out = {}
+            for width in (per_thread, 0):
+                pkg.set_step_width(op, s, width, dts)
+                Y = pkg.col_major(D, s, dtype=dt)
+                pkg.apply(op, Y, _dev(cuda, X, dt), a=2.5, b=-0.3)
+                out[width] = _host(Y).astype(np.float64)
+                ref = Ht.rescaled(X.astype(np.float64) if dts == "fp64" else X.astype(np.float32).astype(np.float64),
+                                  2.5, -0.3)
+                err = np.linalg.norm(out[width] - ref) / np.linalg.norm(ref)
+                assert err < tol, (name, s, dts, width, err)
+            diff = np.linalg.norm(out[0] - out[per_thread]) / np.linalg.norm(out[per_thread])
+            assert diff <= (1e-14 if dts == "fp64" else 1e-6), (name, s, dts, diff)
+            if dts == "fp64":
+                # diagonal from the stored array: exact
+                E = np.zeros((D, s))
+                cols = np.random.default_rng(s).choice(D, min(s, D), replace=False)
+                E[cols, np.arange(len(cols))] = 1.0
+                Y = pkg.col_major(D, s)
+                pkg.apply(op, Y, _dev(cuda, E, cuda.float64))
+                np.testing.assert_array_equal(_host(Y)[cols, np.arange(len(cols))], H.diagonal()[cols],
+                                              err_msg=name)
+                # a filter through the cooperative step
+                Emax = float(np.abs(H).sum(axis=1).max())
+                plan = orc.build_transform_plan(("rescaled", 0.31), 10, 1.0, 0.0, order=40)
+                coeffs = orc.filter_coefficients(plan)[:41]
+                Y = pkg.col_major(D, s)
+                pkg.chebyshev_filter(op, Y, _dev(cuda, X, cuda.float64), coeffs, a=1.01 * Emax, b=0.0)
+                ref = Ht.filter(X, 1.01 * Emax, 0.0, coeffs)
+                assert np.linalg.norm(_host(Y) - ref) / np.linalg.norm(ref) < RTOL64 * 10, name
+            pkg.set_step_width(op, s, per_thread, dts)   # leave the default variant for later tests
+
+
+def test_set_step_width_rejects_invalid_widths(pkg, cuda, models):
+    from polfed_b200 import _lib
+    chain = next(op for name, op, H in models if op.kind == "spin_chain")
+    qsun = next(op for name, op, H in models if op.kind != "spin_chain")
+    with pytest.raises(_lib.PolfedArgumentError):
+        pkg.set_step_width(qsun, 8, 0)          # cooperative step is for chain operators
+    with pytest.raises(_lib.PolfedArgumentError):
+        pkg.set_step_width(chain, 6, 0)         # s must be 4, 8, 16 or 32
+    with pytest.raises(_lib.PolfedArgumentError):
+        pkg.set_step_width(chain, 8, 3)         # not a power of two
+    with pytest.raises(_lib.PolfedArgumentError):
+        pkg.set_step_width(chain, 16, 16)       # 128 bytes of FP64 columns per thread
+    w, times = pkg.autotune(chain, 8, "fp64")
+    assert w in times and 0 in times            # the cooperative step was timed
+
+
 def test_clenshaw_step_formulas(pkg, orc, cuda, models):
     # vector_dispatch.jl:113-139 and optimization.jl:307-325:
     #   b1 = c X + 2 Ht b2 - b3,   Y = c0 X + Ht b1 - b2
