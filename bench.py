@@ -672,7 +672,7 @@ def step_sweep(large_only=False):
         op = make(pkg, np.random.default_rng(3))
         D = op.dim
         for dt, tdt, w in (("fp64", torch.float64, 8), ("fp32", torch.float32, 4)):
-            width, _ = pkg.autotune(op, s, dt)
+            width, tune = pkg.autotune(op, s, dt)
             X = pkg.col_major(D, s, dtype=tdt)
             X.copy_(torch.rand(D, s, dtype=tdt, device="cuda:0"))
             Y = pkg.col_major(D, s, dtype=tdt)
@@ -695,6 +695,7 @@ def step_sweep(large_only=False):
             per = (t_filter(40) - t_filter(20)) / 20
             alg = 4.0 * D * s * w
             print(json.dumps({"case": name, "D": D, "s": s, "dtype": dt, "width": width,
+                              "tune_us": {str(k): round(v * 1e3, 2) for k, v in tune.items()},
                               "us_per_step": per * 1e6, "alg_bytes": alg, "achieved_gbs": alg / per / 1e9,
                               "frac": alg / per / 1e9 / peak, "peak": peak, "peak_kind": peak_kind}), flush=True)
             del X, Y

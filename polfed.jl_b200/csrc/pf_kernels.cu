@@ -400,6 +400,28 @@ __global__ void k_chain_diag(const ChainDesc<T> d, uint32_t D, T *__restrict__ o
     }
 }
 
+// One round of the cooperative step: lane lr ranks the flip of bond b0 + lr,
+// the ranks are shuffled to every lane of the row (r[j] = rank of bond b0 + j,
+// or all ones when that bond does not flip the state) and each lane gathers
+// its column of every flipped neighbour.
+template <typename T, int S>
+__device__ __forceinline__ void coop_round(const ChainDesc<T> &d, const uint32_t *sbm, const uint32_t *tab,
+                                           uint32_t st, bool valid, int b0, int lr, int rb, const T *qc,
+                                           uint32_t (&r)[S], T (&g)[S]) {
+    uint32_t mine = 0xffffffffu;
+    const int b = b0 + lr;
+    if (valid && b < d.nb) {
+        const uint32_t bm = sbm[b];
+        const uint32_t m = st & bm;
+        if (m != 0u && m != bm) mine = d.full ? (st ^ bm) : sector_rank(st ^ bm, tab, d.nchunks);
+    }
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+        r[j] = __shfl_sync(0xffffffffu, mine, rb + j);
+        g[j] = (r[j] != 0xffffffffu) ? __ldg(qc + (size_t)r[j] * S) : T(0);
+    }
+}
+
 // One row per S lanes (S = s, a power of two <= 32), one column per lane.  The
 // lanes of a row split its bonds: lane l ranks the flipped states of bonds
 // l, l+S, l+2S, ...; one shuffle per bond hands the rank to every lane of the
@@ -435,44 +457,57 @@ __global__ void __launch_bounds__(kThreads) k_step_coop(const ChainDesc<T> d, co
         const uint64_t t = base + lane;
         const bool valid = t < total;
         const uint32_t row = valid ? (uint32_t)(t / S) : 0u;
+        // the row's own operands, diagonal and basis state are independent
+        // loads: issue them together, ahead of the gathers
+        T xo = T(0), qo = T(0), po = T(0), dgv = T(0);
+        uint32_t st = 0u;
+        if (valid) {
+            if constexpr (HASX) xo = a.x[t];
+            if constexpr (HASQ) {
+                qo = a.q[t];
+                dgv = d.diag[row];
+                st = d.full ? row : __ldg(d.states + row);
+            }
+            if constexpr (HASP) po = a.p[t];
+        }
         T acc = T(0);
         if constexpr (HASQ) {
-            const uint32_t st = valid ? (d.full ? row : __ldg(d.states + row)) : 0u;
             const T *qc = a.q + lr;
+            // rounds of S bonds, software-pipelined: round k+1's ranks and
+            // gathers are issued before round k is accumulated
+            uint32_t rc[S];
+            T gc[S];
+            coop_round<T, S>(d, sbm, tab, st, valid, 0, lr, rb, qc, rc, gc);
             for (int b0 = 0; b0 < d.nb; b0 += S) {
-                uint32_t mine = 0xffffffffu;  // rank of this lane's flipped state, or inactive
-                const int b = b0 + lr;
-                if (valid && b < d.nb) {
-                    const uint32_t bm = sbm[b];
-                    const uint32_t m = st & bm;
-                    if (m != 0u && m != bm) mine = d.full ? (st ^ bm) : sector_rank(st ^ bm, tab, d.nchunks);
-                }
-                uint32_t r[S];
-                T g[S];
-#pragma unroll
-                for (int j = 0; j < S; ++j) {
-                    r[j] = __shfl_sync(0xffffffffu, mine, rb + j);
-                    g[j] = (r[j] != 0xffffffffu) ? __ldg(qc + (size_t)r[j] * S) : T(0);
-                }
+                uint32_t rn[S];
+                T gn[S];
+                const bool more = b0 + S < d.nb;   // warp-uniform
+                if (more) coop_round<T, S>(d, sbm, tab, st, valid, b0 + S, lr, rb, qc, rn, gn);
 #pragma unroll
                 for (int j = 0; j < S; ++j)
-                    if (r[j] != 0xffffffffu) acc += d.jhalf[b0 + j] * g[j];
+                    if (rc[j] != 0xffffffffu) acc += d.jhalf[b0 + j] * gc[j];
+                if (more) {
+#pragma unroll
+                    for (int j = 0; j < S; ++j) {
+                        rc[j] = rn[j];
+                        gc[j] = gn[j];
+                    }
+                }
             }
         }
         if (valid) {
-            const size_t off = (size_t)t;
             T res = T(0);
-            if constexpr (HASX) res = a.cx * a.x[off];
+            if constexpr (HASX) res = a.cx * xo;
             if constexpr (HASQ) {
-                const T qo = a.q[off];
-                const T hq = (acc + d.diag[row] * qo) * a.inva - a.boa * qo;
+                const T hq = (acc + dgv * qo) * a.inva - a.boa * qo;
                 res = res + a.alpha * hq;
             }
-            if constexpr (HASP) res = res + a.beta * a.p[off];
-            a.out[off] = res;
+            if constexpr (HASP) res = res + a.beta * po;
+            a.out[t] = res;
         }
     }
 }
+
 
 static thread_local int64_t t_launches = 0;
 void count_launches(int64_t n) { t_launches += n; }
