@@ -79,6 +79,7 @@ int pf_handle_create(int device, pf_handle **out) {
 int pf_handle_destroy(pf_handle *h) {
     PF_API_BEGIN
     if (!h) return PF_OK;
+    if (h->aux) pf_handle_destroy(h->aux);
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->blas) cublasDestroy(h->blas);

@@ -115,6 +115,10 @@ struct pf_handle {
     double *red_partials = nullptr;   // deterministic reduction partials
     size_t red_partials_len = 0;
     unsigned int *red_counter = nullptr;
+    // second handle of the same device for work that runs beside this one's
+    // (the two extremal Lanczos probes); created on first use
+    pf_handle *aux = nullptr;
+    std::mutex aux_mu;
 };
 
 struct pf_op {

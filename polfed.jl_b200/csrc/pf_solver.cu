@@ -3,6 +3,9 @@
 // and FP64 residuals.  Reference: Polfed.jl (see each function's citation).
 #include "pf_internal.h"
 #include "pf_solver.h"
+
+#include <exception>
+#include <thread>
 #include "pf_spectral.h"
 
 #include <algorithm>
@@ -588,21 +591,67 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
 // Emin / Emax by two scalar Lanczos probes on H (Plan.jl:136-168,
 // Lanczos.jl:183-212): which = :SR then :LR, howmany 1, tol 1e-14,
 // eigentol 1e-8 (the lanczos() defaults), mapvals = H.
+static pf_handle *aux_handle(pf_handle *h) {
+    std::lock_guard<std::mutex> lock(h->aux_mu);
+    if (!h->aux) {
+        pf_handle *a = nullptr;
+        if (pf_handle_create(h->device, &a) != PF_OK) throw Error(PF_ERR_CUDA, pf_last_error());
+        h->aux = a;
+    }
+    return h->aux;
+}
+
 static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, double tol, double eigentol, double *Emin,
                                 double *Emax, double *stage_acc) {
     const int64_t D = op->dim;
-    BlockMap happly = [&](const double *X, double *Y) {
-        launch_step<double>(op, op->h->stream, D, 1, X, nullptr, nullptr, Y, 0, 1.0, 0, 1.0, 0.0, StepFlags::Q, nullptr);
+    // The :SR probe runs here and the :LR probe at the same time on the
+    // auxiliary handle (its own stream, cuBLAS and cuSOLVER): both only read
+    // v0, so each gives exactly what it gives alone.
+    pf_handle *ah = aux_handle(op->h);
+    std::unique_ptr<pf_op, void (*)(pf_op *)> view(bind_op(op, ah), destroy_op);
+    cudaEvent_t ready = nullptr;
+    PF_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    PF_CUDA(cudaEventRecord(ready, op->h->stream));
+    PF_CUDA(cudaStreamWaitEvent(ah->stream, ready, 0));
+    auto probe = [&](pf_op *o, int which, double *out) {
+        BlockMap happly = [&](const double *X, double *Y) {
+            launch_step<double>(o, o->h->stream, D, 1, X, nullptr, nullptr, Y, 0, 1.0, 0, 1.0, 0.0, StepFlags::Q,
+                                nullptr);
+        };
+        double dummy[10] = {0};
+        LanczosOut lo;
+        lanczos(o, 1, 1, maxdim, tol, eigentol, which, 1, v0_dev, happly, lo, stage_acc ? dummy : nullptr);
+        PF_CHECK(lo.nconv >= 1, PF_ERR_NUMERIC, "Failed to estimate extremal eigenvalue with Lanczos.");
+        *out = which == PF_WHICH_SR ? lo.vals.front() : lo.vals.back();
     };
-    double dummy[10] = {0};
-    for (int w = 0; w < 2; ++w) {
-        LanczosOut o;
-        lanczos(op, 1, 1, maxdim, tol, eigentol, w == 0 ? PF_WHICH_SR : PF_WHICH_LR, 1, v0_dev, happly, o,
-                stage_acc ? dummy : nullptr);
-        PF_CHECK(o.nconv >= 1, PF_ERR_NUMERIC, "Failed to estimate extremal eigenvalue with Lanczos.");
-        if (w == 0) *Emin = o.vals.front();
-        else *Emax = o.vals.back();
+    std::exception_ptr aux_err;
+    int64_t aux_launches = 0;
+    double hi = 0.0;
+    std::thread t([&] {
+        try {
+            PF_CUDA(cudaSetDevice(ah->device));
+            AllocStream guard(ah->stream);
+            const int64_t before = thread_launches();
+            probe(view.get(), PF_WHICH_LR, &hi);
+            aux_launches = thread_launches() - before;
+        } catch (...) {
+            aux_err = std::current_exception();
+        }
+    });
+    std::exception_ptr err;
+    double lo = 0.0;
+    try {
+        probe(op, PF_WHICH_SR, &lo);
+    } catch (...) {
+        err = std::current_exception();
     }
+    t.join();
+    cudaEventDestroy(ready);
+    count_launches(aux_launches);
+    if (err) std::rethrow_exception(err);
+    if (aux_err) std::rethrow_exception(aux_err);
+    *Emin = lo;
+    *Emax = hi;
 }
 
 void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, double eigentol, double *Emin,
