@@ -429,7 +429,9 @@ __device__ __forceinline__ void coop_round(const ChainDesc<T> &d, const uint32_t
 // gathers per lane with one register each, and the row's rank work is done
 // once instead of once per column group.  Gathers are accumulated in bond
 // order and the diagonal comes from k_chain_diag, so every output equals the
-// per-thread kernel's.  Shared memory: the bond masks (lane-indexed, so not
+// per-thread kernel's.  One-column lanes issue 4- or 8-byte gathers, so the
+// variant pays where latency, not load-instruction throughput, bounds the
+// step: small D.  Shared memory: the bond masks (lane-indexed, so not
 // read from the kernel parameters), then the rank tables.
 template <typename T, int S, int FLAGS>
 __global__ void __launch_bounds__(kThreads) k_step_coop(const ChainDesc<T> d, const StepArgs<T> a) {
@@ -473,26 +475,13 @@ __global__ void __launch_bounds__(kThreads) k_step_coop(const ChainDesc<T> d, co
         T acc = T(0);
         if constexpr (HASQ) {
             const T *qc = a.q + lr;
-            // rounds of S bonds, software-pipelined: round k+1's ranks and
-            // gathers are issued before round k is accumulated
-            uint32_t rc[S];
-            T gc[S];
-            coop_round<T, S>(d, sbm, tab, st, valid, 0, lr, rb, qc, rc, gc);
             for (int b0 = 0; b0 < d.nb; b0 += S) {
-                uint32_t rn[S];
-                T gn[S];
-                const bool more = b0 + S < d.nb;   // warp-uniform
-                if (more) coop_round<T, S>(d, sbm, tab, st, valid, b0 + S, lr, rb, qc, rn, gn);
+                uint32_t r[S];
+                T g[S];
+                coop_round<T, S>(d, sbm, tab, st, valid, b0, lr, rb, qc, r, g);
 #pragma unroll
                 for (int j = 0; j < S; ++j)
-                    if (rc[j] != 0xffffffffu) acc += d.jhalf[b0 + j] * gc[j];
-                if (more) {
-#pragma unroll
-                    for (int j = 0; j < S; ++j) {
-                        rc[j] = rn[j];
-                        gc[j] = gn[j];
-                    }
-                }
+                    if (r[j] != 0xffffffffu) acc += d.jhalf[b0 + j] * g[j];
             }
         }
         if (valid) {
