@@ -87,6 +87,7 @@ int pf_handle_destroy(pf_handle *h) {
     if (h->scratch) cudaFree(h->scratch);
     if (h->red_partials) cudaFree(h->red_partials);
     if (h->red_counter) cudaFree(h->red_counter);
+    if (h->pinned) cudaFreeHost(h->pinned);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     PF_API_END

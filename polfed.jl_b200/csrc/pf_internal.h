@@ -119,6 +119,11 @@ struct pf_handle {
     // (the two extremal Lanczos probes); created on first use
     pf_handle *aux = nullptr;
     std::mutex aux_mu;
+    // page-locked staging for the solver's small host<->device transfers
+    // (pageable copies are staged by the driver synchronously and serialise
+    // concurrent solves); grown on demand
+    void *pinned = nullptr;
+    size_t pinned_bytes = 0;
 };
 
 struct pf_op {

@@ -317,6 +317,21 @@ struct LanczosOut {
 
 using BlockMap = std::function<void(const double *X, double *Y)>;  // RI D x s, on h->stream
 
+// The handle's page-locked staging area, at least n doubles.  Growing it
+// waits for the handle's stream, so no copy in flight uses the old area.
+static double *pinned_scratch(pf_handle *h, size_t n) {
+    const size_t bytes = n * sizeof(double);
+    if (h->pinned_bytes < bytes) {
+        sync(h);
+        if (h->pinned) cudaFreeHost(h->pinned);
+        h->pinned = nullptr;
+        h->pinned_bytes = 0;
+        PF_CUDA(cudaMallocHost(&h->pinned, bytes));
+        h->pinned_bytes = bytes;
+    }
+    return static_cast<double *>(h->pinned);
+}
+
 static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
                     int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
                     double *stage_acc) {
@@ -342,6 +357,17 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     const double one = 1.0, zero = 0.0, mone = -1.0;
     const int ldb = maxdim;  // row stride of the basis
     StageClock clk(st, stage_acc);
+    // staging regions; each is rewritten only after a sync(h) that follows
+    // the copy which last used it
+    const size_t ss = (size_t)s * s;
+    double *pin = pinned_scratch(h, 5 * ss + (size_t)maxdim * maxdim + (size_t)maxdim * (s + 3) + 8);
+    double *pinA = pin, *pinG = pinA + ss, *pinR = pinG + ss, *pinO1 = pinR + ss, *pinO2 = pinO1 + ss;
+    double *pinT = pinO2 + ss;                          // maxdim x maxdim
+    double *pinLam = pinT + (size_t)maxdim * maxdim;    // maxdim
+    double *pinTail = pinLam + maxdim;                  // s x maxdim
+    double *pinE = pinTail + (size_t)s * maxdim;        // maxdim
+    double *pinRes = pinE + maxdim;                     // maxdim
+    int *pinInfo = reinterpret_cast<int *>(pinRes + maxdim);
 
     auto append = [&](const double *src, int col) {
         PF_CUDA(cudaMemcpy2DAsync(basis.p + col, (size_t)ldb * sizeof(double), src, (size_t)s * sizeof(double),
@@ -350,8 +376,9 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     // alpha = V^T W (s x s, column-major) -> host, upper-triangle symmetrised
     auto overlap = [&](const double *Vb, const double *Wb) {
         PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, Vb, s, Wb, s, &zero, smallA.p, s));
-        PF_CUDA(cudaMemcpyAsync(hA.data(), smallA.p, (size_t)s * s * sizeof(double), cudaMemcpyDeviceToHost, st));
+        PF_CUDA(cudaMemcpyAsync(pinA, smallA.p, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
         sync(h);
+        std::memcpy(hA.data(), pinA, ss * sizeof(double));
         for (int j = 0; j < s; ++j)
             for (int i = j + 1; i < s; ++i) hA[i + j * s] = hA[j + i * s];  // Hermitian(alpha): upper
     };
@@ -363,12 +390,14 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
         for (int pass = 0; pass < 2 && ok; ++pass) {
             PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, smallA.p, s));
             std::vector<double> hG((size_t)s * s), Rp;
-            PF_CUDA(cudaMemcpyAsync(hG.data(), smallA.p, (size_t)s * s * sizeof(double), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(pinG, smallA.p, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
             sync(h);
+            std::memcpy(hG.data(), pinG, ss * sizeof(double));
             for (int j = 0; j < s; ++j)
                 for (int i = j + 1; i < s; ++i) hG[i + j * s] = hG[j + i * s];
             if (!host_cholesky(hG, s, Rp)) { ok = false; break; }
-            PF_CUDA(cudaMemcpyAsync(smallB.p, Rp.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
+            std::memcpy(pinR, Rp.data(), ss * sizeof(double));
+            PF_CUDA(cudaMemcpyAsync(smallB.p, pinR, ss * sizeof(double), cudaMemcpyHostToDevice, st));
             // W^T <- R^{-T} W^T  (i.e. W <- W R^{-1})
             PF_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, s,
                                   (int)D, &one, smallB.p, s, W, s));
@@ -405,7 +434,8 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     overlap(vlast, r);
     for (int j = 0; j < s; ++j)
         for (int i = 0; i < s; ++i) T[(size_t)i + (size_t)j * maxdim] = hA[i + j * s];
-    PF_CUDA(cudaMemcpyAsync(smallA.p, hA.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
+    std::memcpy(pinO1, hA.data(), ss * sizeof(double));
+    PF_CUDA(cudaMemcpyAsync(smallA.p, pinO1, ss * sizeof(double), cudaMemcpyHostToDevice, st));
     // r^T -= alpha^T x0^T
     PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, smallA.p, s, vlast, s, &one, r, s));
     int numiter = 1;
@@ -448,8 +478,10 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
         cudaEvent_t e3 = clk.mark();
         clk.add(2, e2, e3);
         // 4 orthogonalization: r -= vlast alpha + vprev beta^T  (orthogonalization.jl:31-33)
-        PF_CUDA(cudaMemcpyAsync(smallA.p, hA.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
-        PF_CUDA(cudaMemcpyAsync(smallB.p, beta_last.data(), (size_t)s * s * sizeof(double), cudaMemcpyHostToDevice, st));
+        std::memcpy(pinO1, hA.data(), ss * sizeof(double));
+        std::memcpy(pinO2, beta_last.data(), ss * sizeof(double));
+        PF_CUDA(cudaMemcpyAsync(smallA.p, pinO1, ss * sizeof(double), cudaMemcpyHostToDevice, st));
+        PF_CUDA(cudaMemcpyAsync(smallB.p, pinO2, ss * sizeof(double), cudaMemcpyHostToDevice, st));
         PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, smallA.p, s, vlast, s, &one, r, s));
         PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, s, (int)D, s, &mone, smallB.p, s, vprev, s, &one, r, s));
         cudaEvent_t e4 = clk.mark();
@@ -471,22 +503,22 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
         numiter += 1;
         if (nextcheck == numiter || numiter >= maxiter) {
             // projected matrix, upper triangle is authoritative (Hermitian view)
-            std::vector<double> Tk((size_t)k * k);
+            double *Tk = pinT;
             for (int j = 0; j < k; ++j)
                 for (int i = 0; i < k; ++i) {
                     const int a = std::min(i, j), b2 = std::max(i, j);
                     Tk[(size_t)i + (size_t)j * k] = T[(size_t)a + (size_t)b2 * maxdim];
                 }
-            PF_CUDA(cudaMemcpyAsync(dT.p, Tk.data(), Tk.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            PF_CUDA(cudaMemcpyAsync(dT.p, Tk, (size_t)k * k * sizeof(double), cudaMemcpyHostToDevice, st));
             PF_CUSOLVER(cusolverDnDsyevd(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, dT.p, k, dW.p,
                                          dwork.p, lwork, dinfo.p));
-            std::vector<double> lam(k), tail((size_t)s * k);
-            int info = 0;
-            PF_CUDA(cudaMemcpyAsync(lam.data(), dW.p, k * sizeof(double), cudaMemcpyDeviceToHost, st));
-            PF_CUDA(cudaMemcpy2DAsync(tail.data(), s * sizeof(double), dT.p + (k - s), (size_t)k * sizeof(double),
+            PF_CUDA(cudaMemcpyAsync(pinLam, dW.p, k * sizeof(double), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpy2DAsync(pinTail, s * sizeof(double), dT.p + (k - s), (size_t)k * sizeof(double),
                                       s * sizeof(double), k, cudaMemcpyDeviceToHost, st));
-            PF_CUDA(cudaMemcpyAsync(&info, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(pinInfo, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             sync(h);
+            std::vector<double> lam(pinLam, pinLam + k), tail(pinTail, pinTail + (size_t)s * k);
+            const int info = *pinInfo;
             PF_CHECK(info == 0, PF_ERR_NUMERIC, "projected eigenproblem failed to converge");
             std::vector<int> idx(k);
             std::iota(idx.begin(), idx.end(), 0);
@@ -531,10 +563,10 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
                                         StepFlags::Q, nullptr);
                     launch_coldots<double>(h, st, D, conv, out.vecs.p, HV.p, E.p);
                     launch_colresid(h, st, D, conv, HV.p, out.vecs.p, E.p, res2.p);
-                    std::vector<double> hE(conv), hr(conv);
-                    PF_CUDA(cudaMemcpyAsync(hE.data(), E.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
-                    PF_CUDA(cudaMemcpyAsync(hr.data(), res2.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
+                    PF_CUDA(cudaMemcpyAsync(pinE, E.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
+                    PF_CUDA(cudaMemcpyAsync(pinRes, res2.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
                     sync(h);
+                    std::vector<double> hE(pinE, pinE + conv), hr(pinRes, pinRes + conv);
                     int ec = 0;
                     bool counting = true;
                     double maxe = 0.0;
