@@ -522,11 +522,10 @@ void ensure_reduction(pf_handle *h, size_t n) {
     }
 }
 
-// Resident CTAs per SM of a kernel instance (occupancy calculator, cached).
+// Resident CTAs per SM of a kernel instance (occupancy calculator, cached per
+// host thread so concurrent solves do not contend on a lock every launch).
 static int blocks_per_sm(const void *kern, int smem) {
-    static std::mutex mu;
-    static std::map<std::pair<const void *, int>, int> cache;
-    std::lock_guard<std::mutex> lock(mu);
+    thread_local std::map<std::pair<const void *, int>, int> cache;
     auto key = std::make_pair(kern, smem);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
