@@ -109,6 +109,13 @@ int pf_op_spin_chain_create(pf_handle *h, int L, int Lup, int nbonds, const int3
 int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup,
                       const int32_t *nbr, const double *fields, const double *grain,
                       pf_op **out);
+/* A real symmetric sparse matrix (polfed(mat, ...), PolfedCore.jl:153-184,
+ * whose operator is mul!(Y, mat, X)): CSR with 0-based row pointers
+ * indptr[D + 1] (indptr[0] = 0, indptr[D] = nnz, non-decreasing), column
+ * indices in [0, D) and values, host arrays copied.  Symmetry is the
+ * caller's contract, as in the reference.  D < 2^31. */
+int pf_op_csr_create(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                     const double *values, pf_op **out);
 /* A view of op that runs on handle h (same device).  It shares op's device
  * tables, so several host threads can solve concurrently, each on its own
  * handle / stream.  Destroy views and the original in any order; the tables
@@ -252,7 +259,10 @@ int pf_solve(pf_op *op, const pf_params *params, int s, int nev,
  * A request is admitted when a worker is free and its estimated device
  * footprint fits in what `hbm_budget` (bytes; 0 = 90 % of free memory at
  * creation) leaves; otherwise it waits in FIFO order.  Requests run the
- * same solve as pf_solve and give the same result alone or in a mix. */
+ * same solve as pf_solve and give the same result alone or in a mix.  Each
+ * request takes its own view of its operator when it is submitted (device
+ * tables and tuned step widths shared), so an operator may be destroyed as
+ * soon as the submitting call returns. */
 typedef struct pf_pool pf_pool;
 
 typedef struct pf_pool_stats {

@@ -34,6 +34,7 @@ EXPORTED = [
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
     "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind", "pf_set_step_width",
+    "pf_op_csr_create",
     "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
 ]
@@ -121,6 +122,7 @@ def load():
         "pf_op_spin_chain_create": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_qsun_create": (i32, [vp, i32, i32, f64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_destroy": (i32, [vp]),
+        "pf_op_csr_create": (i32, [vp, i64, i64, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_bind": (i32, [vp, vp, ctypes.POINTER(vp)]),
         "pf_op_dim": (i64, [vp]),
         "pf_basis_unrank": (i32, [vp, i64, vp, vp]),

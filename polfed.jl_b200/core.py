@@ -26,7 +26,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from .models import Operator
+from .models import Operator, as_operator
 
 # ------------------------------------------------------------------ configs
 
@@ -266,7 +266,9 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
            precision: str = "fp64", vecs: bool = True):
     """POLFED on the B200 (PolfedCore.jl:194-263).
 
-    ``x0`` is D (scalar Lanczos) or D x s (block Lanczos): a host array, or a
+    ``op`` is a model operator or a real symmetric matrix (scipy.sparse, a
+    CSR triple or dense; PolfedCore.jl:153-184).  ``x0`` is D (scalar
+    Lanczos) or D x s (block Lanczos): a host array, or a
     column-major float64 CUDA tensor (then the eigenvectors are returned as a
     column-major CUDA tensor and never leave HBM).  A non-normalised /
     non-orthonormal start is replaced by a normalised copy, as the reference
@@ -278,6 +280,7 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
     dos = dos or DoSConfig()
     if howmany < 1:
         raise ValueError("howmany must be positive")
+    op = as_operator(op)   # polfed(mat, ...): a sparse or dense matrix runs as a CSR operator
     D = op.dim
     on_device = _is_cuda_tensor(x0)
     if on_device:
@@ -461,6 +464,7 @@ class SolverPool:
         n = len(ops)
         if n == 0:
             return []
+        ops = [as_operator(o, self.device) for o in ops]
         mapping, transform, fact, dos, precision, want_rep, want_vecs = _solve_kwargs(kwargs)
         on_device = _is_cuda_tensor(x0s[0])
         if any(_is_cuda_tensor(x) != on_device for x in x0s):
@@ -511,6 +515,7 @@ class SolverPool:
 
     def submit(self, op: Operator, x0, howmany: int, target, **kwargs) -> int:
         """Queue one solve; returns its request id.  ``x0`` is copied."""
+        op = as_operator(op, self.device)
         mapping, transform, fact, dos, precision, want_rep, want_vecs = _solve_kwargs(kwargs)
         if op.device != self.device:
             raise ValueError("operator and pool are on different devices")
@@ -523,7 +528,9 @@ class SolverPool:
         _lib.check(_lib.load().pf_pool_submit(self._pool, op.op, ctypes.byref(p), s, int(howmany), x.ctypes.data,
                                               V.ctypes.data if want_vecs else None, _lib.PF_MEM_HOST,
                                               ctypes.byref(rid)))
-        self._pending[rid.value] = (V, int(howmany), want_rep, kind, val)
+        # the operator stays referenced until the result is collected: the
+        # worker binds it when the request starts and updates its tuning after
+        self._pending[rid.value] = (V, int(howmany), want_rep, kind, val, op)
         return rid.value
 
     def poll(self, request: int) -> str:
@@ -535,7 +542,7 @@ class SolverPool:
     def result(self, request: int, timeout: Optional[float] = None):
         """Wait for a request and return its ``polfed`` result tuple; raises the
         request's error if it failed (the request is released either way)."""
-        V, howmany, want_rep, kind, val = self._pending[request]
+        V, howmany, want_rep, kind, val, _op = self._pending[request]
         vals = np.zeros(howmany)
         rep = _lib.pf_report()
         n = ctypes.c_int()
@@ -580,6 +587,7 @@ def polfed_batch(ops, x0s, howmany: int, target, *, workers: int = 4, **kwargs):
         raise ValueError("one x0 per operator is required")
     if not ops:
         return []
+    ops = [as_operator(o) for o in ops]
     return solver_pool(max(1, workers), ops[0].device).solve_batch(ops, x0s, howmany, target, **kwargs)
 
 

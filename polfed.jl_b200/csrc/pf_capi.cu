@@ -124,6 +124,14 @@ int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const dou
     PF_API_END
 }
 
+int pf_op_csr_create(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                     const double *values, pf_op **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    *out = pf::create_csr(h, D, nnz, indptr, indices, values);
+    PF_API_END
+}
+
 int pf_op_bind(const pf_op *op, pf_handle *h, pf_op **out) {
     PF_API_BEGIN
     PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");

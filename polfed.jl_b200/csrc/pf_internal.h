@@ -85,7 +85,17 @@ struct QSunDesc {
     T grain[PF_MAX_GRAIN * PF_MAX_GRAIN];  // row-major dg x dg
 };
 
-enum OpKind { OP_CHAIN = 0, OP_QSUN = 1 };
+// A user-supplied real symmetric sparse matrix in CSR form (row pointers,
+// column indices and values per row, any column order; the diagonal is an
+// ordinary entry).
+template <typename T>
+struct CsrDesc {
+    const int64_t *indptr;   // D + 1
+    const int32_t *indices;  // nnz
+    const T *values;         // nnz
+};
+
+enum OpKind { OP_CHAIN = 0, OP_QSUN = 1, OP_CSR = 2 };
 
 // Number of entries of the chunked rank table for an L-bit sector:
 // chunk c (bits 8c..8c+7) holds (8c+1) x 256 entries.
@@ -135,6 +145,9 @@ struct pf_op {
     pf::ChainDesc<float> chain32;
     pf::QSunDesc<double> qsun64;
     pf::QSunDesc<float> qsun32;
+    pf::CsrDesc<double> csr64{};
+    pf::CsrDesc<float> csr32{};
+    int64_t nnz = 0;
     uint32_t *d_states = nullptr;
     uint32_t *d_rank_tab = nullptr;
     double *d_diag64 = nullptr;       // chain diagonal in each precision (warp-cooperative step)

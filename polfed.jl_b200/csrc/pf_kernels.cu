@@ -190,6 +190,40 @@ __device__ __forceinline__ void qsun_row(const QSunDesc<T> &d, const T *smem_t, 
     }
 }
 
+// CSR row (a user matrix): the entries of the row in storage order, gathered
+// in unrolled batches of U like the matrix-free rows; the diagonal is an
+// ordinary entry, so diag = 0.
+template <typename T, int V, bool HASQ>
+__device__ __forceinline__ void csr_row(const CsrDesc<T> &d, uint32_t row, int s, int c0, const T *__restrict__ q,
+                                        T (&acc)[V], T &diag) {
+    diag = T(0);
+    if constexpr (HASQ) {
+        constexpr int U = Batch<T, V>::U;
+        const int64_t b = __ldg(d.indptr + row), e = __ldg(d.indptr + row + 1);
+        const T *qc = q + c0;
+        for (int64_t p0 = b; p0 < e; p0 += U) {
+            int32_t col[U];
+            T val[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (p0 + u < e) {
+                    col[u] = __ldg(d.indices + p0 + u);
+                    val[u] = __ldg(d.values + p0 + u);
+                }
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (p0 + u < e) g[u] = ldp<T, V>(qc + (size_t)col[u] * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (p0 + u < e) {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] += val[u] * g[u].v[v];
+                }
+        }
+    }
+}
+
 template <typename T>
 struct StepArgs {
     uint32_t D;
@@ -215,6 +249,10 @@ struct DescTraits<ChainDesc<T>> {
 template <typename T>
 struct DescTraits<QSunDesc<T>> {
     static constexpr int kind = OP_QSUN;
+};
+template <typename T>
+struct DescTraits<CsrDesc<T>> {
+    static constexpr int kind = OP_CSR;
 };
 
 constexpr int kThreads = 256;
@@ -260,7 +298,7 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T, V>::value) k_step(const
             uint32_t *t = reinterpret_cast<uint32_t *>(smem_raw);
             for (int i = threadIdx.x; i < n; i += blockDim.x) t[i] = __ldg(d.rank_tab + i);
         }
-    } else {
+    } else if constexpr (DescTraits<Desc>::kind == OP_QSUN) {
         T *sm = reinterpret_cast<T *>(smem_raw);
         const int gs = d.dg + 1;
         for (int i = threadIdx.x; i < d.dg * d.dg; i += blockDim.x) sm[(i / d.dg) * gs + (i % d.dg)] = d.grain[i];
@@ -294,8 +332,10 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T, V>::value) k_step(const
         T diag;
         if constexpr (DescTraits<Desc>::kind == OP_CHAIN)
             chain_row<T, V, HASQ>(d, tab, row, a.s, c0, a.q, acc, diag);
-        else
+        else if constexpr (DescTraits<Desc>::kind == OP_QSUN)
             qsun_row<T, V, HASQ>(d, smem_t, row, a.s, c0, a.q, acc, diag);
+        else
+            csr_row<T, V, HASQ>(d, row, a.s, c0, a.q, acc, diag);
         Pack<T, V> res;
 #pragma unroll
         for (int v = 0; v < V; ++v) res.v[v] = T(0);
@@ -584,6 +624,13 @@ const QSunDesc<double> &qsun_of<double>(pf_op *op) { return op->qsun64; }
 template <>
 const QSunDesc<float> &qsun_of<float>(pf_op *op) { return op->qsun32; }
 
+template <typename T>
+static const CsrDesc<T> &csr_of(pf_op *op);
+template <>
+const CsrDesc<double> &csr_of<double>(pf_op *op) { return op->csr64; }
+template <>
+const CsrDesc<float> &csr_of<float>(pf_op *op) { return op->csr32; }
+
 template <typename T, int V>
 static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int flags) {
     int smem = 0;
@@ -594,10 +641,14 @@ static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int fl
         if ((flags & StepFlags::Q) && !d.full) smem = rank_table_entries(d.nchunks) * 4;
         if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
         dispatch_flags<T, V>(op, st, d, a, flags, smem);
-    } else {
+    } else if (op->kind == OP_QSUN) {
         const QSunDesc<T> &d = qsun_of<T>(op);
         smem = QSunSmem<T>::bytes(d.dg);
         if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
+        dispatch_flags<T, V>(op, st, d, a, flags, smem);
+    } else {
+        const CsrDesc<T> &d = csr_of<T>(op);
+        if (flags & StepFlags::DOTS) smem = dots_smem;
         dispatch_flags<T, V>(op, st, d, a, flags, smem);
     }
 }

@@ -193,6 +193,61 @@ pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double
     return op;
 }
 
+pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                  const double *values) {
+    PF_CHECK(h != nullptr, PF_ERR_INVALID, "null handle");
+    PF_CHECK(D >= 1 && D < ((int64_t)1 << 31), PF_ERR_UNSUPPORTED, "matrix dimension must be in [1, 2^31)");
+    PF_CHECK(nnz >= 0 && indptr && (nnz == 0 || (indices && values)), PF_ERR_INVALID, "null CSR array");
+    PF_CHECK(indptr[0] == 0 && indptr[D] == nnz, PF_ERR_INVALID, "indptr must start at 0 and end at nnz");
+    for (int64_t i = 0; i < D; ++i)
+        PF_CHECK(indptr[i + 1] >= indptr[i], PF_ERR_INVALID, "indptr must be non-decreasing");
+    for (int64_t p = 0; p < nnz; ++p) {
+        PF_CHECK(indices[p] >= 0 && (int64_t)indices[p] < D, PF_ERR_INVALID, "column index out of range");
+        PF_CHECK(std::isfinite(values[p]), PF_ERR_INVALID, "non-finite matrix entry");
+    }
+    PF_CUDA(cudaSetDevice(h->device));
+    pf_op *op = new pf_op();
+    op->h = h;
+    op->kind = OP_CSR;
+    op->dim = D;
+    op->nnz = nnz;
+    int64_t *dptr = nullptr;
+    int32_t *didx = nullptr;
+    double *dv64 = nullptr;
+    float *dv32 = nullptr;
+    try {
+        std::vector<float> v32(values, values + nnz);
+        PF_CUDA(cudaMalloc(&dptr, (D + 1) * sizeof(int64_t)));
+        PF_CUDA(cudaMalloc(&didx, std::max<int64_t>(nnz, 1) * sizeof(int32_t)));
+        PF_CUDA(cudaMalloc(&dv64, std::max<int64_t>(nnz, 1) * sizeof(double)));
+        PF_CUDA(cudaMalloc(&dv32, std::max<int64_t>(nnz, 1) * sizeof(float)));
+        PF_CUDA(cudaMemcpy(dptr, indptr, (D + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+        if (nnz > 0) {
+            PF_CUDA(cudaMemcpy(didx, indices, nnz * sizeof(int32_t), cudaMemcpyHostToDevice));
+            PF_CUDA(cudaMemcpy(dv64, values, nnz * sizeof(double), cudaMemcpyHostToDevice));
+            PF_CUDA(cudaMemcpy(dv32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
+        }
+        const int dev = h->device;
+        op->tables_owner = std::shared_ptr<void>(nullptr, [dptr, didx, dv64, dv32, dev](void *) {
+            cudaSetDevice(dev);
+            cudaFree(dptr);
+            cudaFree(didx);
+            cudaFree(dv64);
+            cudaFree(dv32);
+        });
+    } catch (...) {
+        if (dptr) cudaFree(dptr);
+        if (didx) cudaFree(didx);
+        if (dv64) cudaFree(dv64);
+        if (dv32) cudaFree(dv32);
+        delete op;
+        throw;
+    }
+    op->csr64 = {dptr, didx, dv64};
+    op->csr32 = {dptr, didx, dv32};
+    return op;
+}
+
 void destroy_op(pf_op *op) {
     if (!op) return;
     delete op;  // the device tables go with the last operator sharing them
@@ -211,6 +266,9 @@ pf_op *bind_op(const pf_op *src, pf_handle *h) {
     op->chain32 = src->chain32;
     op->qsun64 = src->qsun64;
     op->qsun32 = src->qsun32;
+    op->csr64 = src->csr64;
+    op->csr32 = src->csr32;
+    op->nnz = src->nnz;
     op->d_states = src->d_states;
     op->d_rank_tab = src->d_rank_tab;
     op->d_diag64 = src->d_diag64;

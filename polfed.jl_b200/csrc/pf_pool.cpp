@@ -27,6 +27,10 @@ using Clock = std::chrono::steady_clock;
 
 struct PoolRequest {
     int64_t id = 0;
+    // the request's own view of the caller's operator (taken at submit; it
+    // shares the device tables and the tuned step widths of that moment), so
+    // the caller may destroy its operator as soon as the call returns
+    std::unique_ptr<pf_op, void (*)(pf_op *)> own{nullptr, destroy_op};
     pf_op *op = nullptr;
     pf_params params{};
     int s = 1, nev = 1;
@@ -119,12 +123,6 @@ static void pool_worker(pf_pool *pool, int w) {
             double *vals = req->batch ? req->vals_out : req->vals.data();
             solve(view, &req->params, req->s, req->nev, req->x0, req->x0_mem, vals, req->vecs_out, req->vecs_mem,
                   &req->rep, &req->nconv);
-            {
-                // keep the autotuned step width on the caller's operator for later requests
-                std::lock_guard<std::mutex> lk(req->op->tune_mu);
-                std::lock_guard<std::mutex> lv(view->tune_mu);
-                for (auto &kv : view->tuned_width) req->op->tuned_width.insert(kv);
-            }
         } catch (const Error &e) {
             status = e.code;
             err = e.what();
@@ -215,7 +213,8 @@ static std::shared_ptr<PoolRequest> make_request(pf_pool *pool, pf_op *op, const
     PF_CHECK(op->h && op->h->device == pool->device, PF_ERR_INVALID, "operator and pool are on different devices");
     PF_CHECK(s >= 1 && nev >= 1, PF_ERR_INVALID, "s and nev must be positive");
     auto r = std::make_shared<PoolRequest>();
-    r->op = op;
+    r->own.reset(bind_op(op, op->h));
+    r->op = r->own.get();
     r->params = *p;
     r->s = s;
     r->nev = nev;

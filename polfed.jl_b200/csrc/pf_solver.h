@@ -11,6 +11,8 @@ pf_op *create_spin_chain(pf_handle *h, int L, int Lup, int nbonds, const int32_t
                          const double *Delta, const double *fields);
 pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup, const int32_t *nbr,
                    const double *fields, const double *grain);
+pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                  const double *values);
 void destroy_op(pf_op *op);
 pf_op *bind_op(const pf_op *src, pf_handle *h);
 void *handle_scratch(pf_handle *h, size_t bytes);

@@ -198,6 +198,58 @@ class QSunOperator(Operator):
         return out.value
 
 
+class SparseOperator(Operator):
+    """A real symmetric sparse matrix as the operator of ``polfed(mat, ...)``
+    (PolfedCore.jl:153-184, whose operator is ``mul!(Y, mat, X)``).  ``mat``
+    is anything with ``tocsr()`` (a scipy.sparse matrix), a CSR triple
+    ``(indptr, indices, values)`` of a square matrix, or a dense 2-D array.
+    Symmetry is the caller's contract, as in the reference."""
+
+    kind = "csr"
+
+    def __init__(self, mat, device: int = 0):
+        super().__init__(device)
+        if hasattr(mat, "tocsr"):
+            m = mat.tocsr()
+            if m.shape[0] != m.shape[1]:
+                raise ValueError(f"the matrix must be square; got {m.shape}")
+            indptr, indices, values = m.indptr, m.indices, m.data
+        elif isinstance(mat, tuple) and len(mat) == 3:
+            indptr, indices, values = mat
+        else:
+            a = np.asarray(mat)
+            if a.ndim != 2 or a.shape[0] != a.shape[1]:
+                raise ValueError(f"the matrix must be square; got shape {a.shape}")
+            rows, cols = np.nonzero(a)
+            indptr = np.searchsorted(rows, np.arange(a.shape[0] + 1))
+            indices, values = cols, a[rows, cols]
+        if np.iscomplexobj(values):
+            raise ValueError("Complex GPU arrays are not supported yet. Current GPU kernels are real-only. "
+                             "Use CPU arrays for complex matrices/operators.")
+        self.indptr = np.ascontiguousarray(indptr, dtype=np.int64)
+        self.indices = np.ascontiguousarray(indices, dtype=np.int32)
+        self.values = np.ascontiguousarray(values, dtype=np.float64)
+        if self.indptr.ndim != 1 or len(self.indptr) < 2:
+            raise ValueError("indptr must hold D + 1 row pointers")
+        if len(self.indices) != len(self.values) or self.indptr[-1] != len(self.values):
+            raise ValueError("indices and values must hold indptr[-1] entries")
+
+    def _create(self) -> int:
+        D = len(self.indptr) - 1
+        nnz = len(self.values)
+        idx = self.indices if nnz else np.zeros(1, np.int32)
+        val = self.values if nnz else np.zeros(1)
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().pf_op_csr_create(self.handle, D, nnz, self.indptr.ctypes.data, idx.ctypes.data,
+                                                val.ctypes.data, ctypes.byref(out)))
+        return out.value
+
+
+def as_operator(mat, device: int = 0) -> Operator:
+    """An Operator as is; a matrix (sparse, CSR triple or dense) as a SparseOperator."""
+    return mat if isinstance(mat, Operator) else SparseOperator(mat, device=device)
+
+
 def xxz_hamiltonian(L: int, Lup: int, J: float, Delta: float, W: float, *, boundary: str = "periodic",
                     field: float = 0.0, fields=None, rng=None, device: int = 0) -> SpinChainOperator:
     """XXZ chain (SpinHalfChains.jl:74-99)."""

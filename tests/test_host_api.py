@@ -120,3 +120,23 @@ def test_pool_refuses_without_a_device_and_footprint_guards(pkg):
     out = ctypes.c_void_p()
     assert lib.pf_pool_create(0, 0, 0.0, ctypes.byref(out)) == _lib.PF_ERR_INVALID   # 0 workers
     assert not out.value
+
+
+def test_sparse_operator_host_validation(pkg):
+    """Matrix input is checked on the host before any device work: square,
+    real (the reference rejects complex GPU input, PolfedCore.jl:160-162),
+    consistent CSR arrays; a dense matrix becomes the same CSR as scipy's."""
+    import scipy.sparse as sp
+    with pytest.raises(ValueError, match="square"):
+        pkg.SparseOperator(np.zeros((3, 4)))
+    with pytest.raises(ValueError, match="Complex GPU arrays"):
+        pkg.SparseOperator(sp.csr_matrix(np.eye(3) * 1j))
+    with pytest.raises(ValueError):
+        pkg.SparseOperator((np.array([0, 1]), np.array([0, 0]), np.array([1.0])))
+    A = sp.random(40, 40, density=0.2, random_state=3)
+    A = (A + A.T).tocsr()
+    A.sort_indices()
+    d = pkg.SparseOperator(A.toarray())
+    np.testing.assert_array_equal(d.indptr, A.indptr)
+    np.testing.assert_array_equal(d.indices, A.indices)
+    np.testing.assert_array_equal(d.values, A.data)
