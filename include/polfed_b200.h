@@ -205,7 +205,7 @@ typedef struct pf_params {
     int    precision;            /* PF_PREC_FP64 */
     int    reorth_passes;        /* 1 = FullRO of the reference; 2 = CGS2 */
     int    extrema_maxdim;       /* 1000 (Plan.jl:143,160) */
-    int    refine;               /* MIXED only: FP64 refinement passes for unconverged pairs */
+    int    refine;               /* reserved (read by nothing): no FP64 refinement pass is implemented */
     int    autotune;             /* 1: time the step-kernel variants once per (op, s, dtype) */
 } pf_params;
 
