@@ -280,9 +280,14 @@ typedef struct pf_pool_stats {
 
 int pf_pool_create(int device, int workers, double hbm_budget, pf_pool **out);
 int pf_pool_destroy(pf_pool *pool);   /* waits for running requests */
-/* The CUDA stream (cudaStream_t) of worker w, for callers that order their own
- * work or timing events against the pool's solves. */
+/* The CUDA streams (cudaStream_t) of the pool: index w < workers is worker
+ * w's default-priority stream, workers + w its high-priority stream; for
+ * callers that order their own work or timing events against the solves. */
 int pf_pool_stream(pf_pool *pool, int worker, void **stream);
+/* Requests on operators of dimension <= dim (default 65536; 0: none) run on
+ * the workers' high-priority streams, so their short launches are dispatched
+ * ahead of the queued launches of larger solves.  Results are unchanged. */
+int pf_pool_set_priority_dim(pf_pool *pool, int64_t dim);
 /* Estimated device bytes of one solve (what admission charges). */
 double pf_solve_footprint(const pf_op *op, const pf_params *params, int s, int nev);
 /* Solve n problems concurrently; arrays of length n (params may repeat one

@@ -412,12 +412,20 @@ class SolverPool:
     of requests.  Every request runs the same solve as ``polfed`` and gives
     the same result whether it runs alone or among others."""
 
-    def __init__(self, workers: int = 4, device: int = 0, hbm_budget: Optional[float] = None):
+    def __init__(self, workers: int = 4, device: int = 0, hbm_budget: Optional[float] = None,
+                 priority_dim: Optional[int] = None):
         self.device = device
         h = ctypes.c_void_p()
         _lib.check(_lib.load().pf_pool_create(device, int(workers), float(hbm_budget or 0.0), ctypes.byref(h)))
         self._pool = h
         self._pending: dict = {}
+        if priority_dim is not None:
+            self.set_priority_dim(priority_dim)
+
+    def set_priority_dim(self, dim: int):
+        """Requests with operator dimension <= ``dim`` (default 65536; 0: none)
+        run on high-priority streams; results are unchanged."""
+        _lib.check(_lib.load().pf_pool_set_priority_dim(self._pool, int(dim)))
 
     def close(self):
         if self._pool is not None and self._pool.value:
@@ -445,7 +453,8 @@ class SolverPool:
         return _lib.load().pf_solve_footprint(op.op, ctypes.byref(p), int(s), int(howmany))
 
     def streams(self):
-        """The workers' CUDA stream handles (integers), one per worker."""
+        """The pool's CUDA stream handles (integers): each worker's default-
+        and high-priority stream."""
         out, w = [], 0
         while True:
             st = ctypes.c_void_p()

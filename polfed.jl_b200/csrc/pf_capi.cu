@@ -11,6 +11,9 @@
 namespace pf {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &msg) { g_last_error = msg; }
+// Stream priority for handles created by this thread (the pool and the
+// auxiliary handles set it around their pf_handle_create calls).
+thread_local int t_new_handle_priority = 0;
 }  // namespace pf
 
 #define PF_API_BEGIN try {
@@ -58,7 +61,8 @@ int pf_handle_create(int device, pf_handle **out) {
     h->device = device;
     h->num_sms = prop.multiProcessorCount;
     try {
-        PF_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->priority = pf::t_new_handle_priority;
+        PF_CUDA(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, h->priority));
         PF_CUBLAS(cublasCreate(&h->blas));
         PF_CUBLAS(cublasSetStream(h->blas, h->stream));
         PF_CUSOLVER(cusolverDnCreate(&h->solver));
@@ -309,6 +313,12 @@ int pf_pool_stream(pf_pool *pool, int worker, void **stream) {
     PF_API_BEGIN
     PF_CHECK(pool && stream, PF_ERR_INVALID, "null argument");
     *stream = (void *)pf::pool_stream(pool, worker);
+    PF_API_END
+}
+
+int pf_pool_set_priority_dim(pf_pool *pool, int64_t dim) {
+    PF_API_BEGIN
+    pf::pool_set_priority_dim(pool, dim);
     PF_API_END
 }
 

@@ -116,6 +116,7 @@ __host__ __device__ inline int rank_table_offset(int c) {
 struct pf_handle {
     int device = 0;
     int num_sms = 148;
+    int priority = 0;                 // CUDA stream priority (lower = more urgent)
     cudaStream_t stream = nullptr;
     cublasHandle_t blas = nullptr;
     cusolverDnHandle_t solver = nullptr;

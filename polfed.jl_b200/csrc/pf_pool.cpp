@@ -49,7 +49,7 @@ struct PoolRequest {
     int status = PF_OK;
     std::string error;
     double footprint = 0.0;
-    bool cancelled = false, batch = false;
+    bool cancelled = false, batch = false, urgent = false;
     Clock::time_point t_submit, t_done;
 };
 
@@ -57,7 +57,9 @@ struct PoolRequest {
 
 struct pf_pool {
     int device = 0;
-    std::vector<pf_handle *> handles;
+    std::vector<pf_handle *> handles;   // one per worker, default stream priority
+    std::vector<pf_handle *> urgent;    // one per worker, the device's highest stream priority
+    int64_t priority_dim = 65536;       // requests with D <= this run on the urgent handles
     std::vector<std::thread> threads;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -88,7 +90,6 @@ double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev) {
 }
 
 static void pool_worker(pf_pool *pool, int w) {
-    pf_handle *h = pool->handles[w];
     cudaSetDevice(pool->device);
     while (true) {
         std::shared_ptr<PoolRequest> req;
@@ -110,11 +111,15 @@ static void pool_worker(pf_pool *pool, int w) {
                 pool->cv_work.notify_all();
                 continue;
             }
+            req->urgent = req->op->dim <= pool->priority_dim;
             pool->in_use += req->footprint;
             pool->peak = std::max(pool->peak, pool->in_use);
             if (pool->running++ == 0) pool->busy_since = Clock::now();
             req->state = PF_REQ_RUNNING;
         }
+        // small solves on the high-priority stream: their short launches are
+        // dispatched ahead of queued launches of larger solves (same results)
+        pf_handle *h = req->urgent ? pool->urgent[w] : pool->handles[w];
         int status = PF_OK;
         std::string err;
         pf_op *view = nullptr;
@@ -170,10 +175,18 @@ pf_pool *pool_create(int device, int workers, double budget) {
     }
     pool->budget = budget;
     try {
+        int least = 0, greatest = 0;
+        PF_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         for (int w = 0; w < workers; ++w) {
             pf_handle *h = nullptr;
             if (pf_handle_create(device, &h) != PF_OK) throw Error(PF_ERR_CUDA, pf_last_error());
             pool->handles.push_back(h);
+            const int saved = t_new_handle_priority;
+            t_new_handle_priority = greatest;
+            const int st = pf_handle_create(device, &h);
+            t_new_handle_priority = saved;
+            if (st != PF_OK) throw Error(PF_ERR_CUDA, pf_last_error());
+            pool->urgent.push_back(h);
         }
         for (int w = 0; w < workers; ++w) pool->threads.emplace_back(pool_worker, pool, w);
     } catch (...) {
@@ -184,6 +197,7 @@ pf_pool *pool_create(int device, int workers, double budget) {
         pool->cv_work.notify_all();
         for (auto &t : pool->threads) t.join();
         for (auto h : pool->handles) pf_handle_destroy(h);
+        for (auto h : pool->urgent) pf_handle_destroy(h);
         delete pool;
         throw;
     }
@@ -200,12 +214,20 @@ void pool_destroy(pf_pool *pool) {
     pool->cv_work.notify_all();
     for (auto &t : pool->threads) t.join();
     for (auto h : pool->handles) pf_handle_destroy(h);
+    for (auto h : pool->urgent) pf_handle_destroy(h);
     delete pool;
 }
 
+void pool_set_priority_dim(pf_pool *pool, int64_t dim) {
+    PF_CHECK(pool && dim >= 0, PF_ERR_INVALID, "invalid argument");
+    std::lock_guard<std::mutex> lock(pool->mu);
+    pool->priority_dim = dim;
+}
+
 cudaStream_t pool_stream(pf_pool *pool, int worker) {
-    PF_CHECK(worker >= 0 && worker < (int)pool->handles.size(), PF_ERR_INVALID, "no such worker");
-    return pool->handles[worker]->stream;
+    const int W = (int)pool->handles.size();
+    PF_CHECK(worker >= 0 && worker < 2 * W, PF_ERR_INVALID, "no such worker stream");
+    return worker < W ? pool->handles[worker]->stream : pool->urgent[worker - W]->stream;
 }
 
 static std::shared_ptr<PoolRequest> make_request(pf_pool *pool, pf_op *op, const pf_params *p, int s, int nev) {

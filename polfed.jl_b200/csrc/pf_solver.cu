@@ -627,7 +627,11 @@ static pf_handle *aux_handle(pf_handle *h) {
     std::lock_guard<std::mutex> lock(h->aux_mu);
     if (!h->aux) {
         pf_handle *a = nullptr;
-        if (pf_handle_create(h->device, &a) != PF_OK) throw Error(PF_ERR_CUDA, pf_last_error());
+        const int saved = t_new_handle_priority;
+        t_new_handle_priority = h->priority;   // the probes run as urgently as their solve
+        const int st = pf_handle_create(h->device, &a);
+        t_new_handle_priority = saved;
+        if (st != PF_OK) throw Error(PF_ERR_CUDA, pf_last_error());
         h->aux = a;
     }
     return h->aux;

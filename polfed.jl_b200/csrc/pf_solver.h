@@ -34,11 +34,14 @@ void solve(pf_op *op, const pf_params *p, int s, int nev, const double *x0, int 
 void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, double eigentol, double *Emin,
                      double *Emax);
 
+extern thread_local int t_new_handle_priority;
+
 // request pool (pf_pool.cpp)
 double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev);
 pf_pool *pool_create(int device, int workers, double budget);
 void pool_destroy(pf_pool *pool);
 cudaStream_t pool_stream(pf_pool *pool, int worker);
+void pool_set_priority_dim(pf_pool *pool, int64_t dim);
 int64_t pool_submit(pf_pool *pool, pf_op *op, const pf_params *p, int s, int nev, const double *x0,
                     double *vecs_out, int vecs_mem);
 int pool_solve_batch(pf_pool *pool, int n, pf_op *const *ops, const pf_params *const *params, const int *s,
