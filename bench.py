@@ -458,6 +458,7 @@ def run_serve(args, local_rank):
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=args.requests))
     arrivals -= arrivals[0]
     pool = pkg.SolverPool(workers=args.workers, device=local_rank)
+    pool.set_admission(args.admission)
     # warm-up: one small request of each kind (library set-up, cuBLAS/cuSOLVER handles)
     wrng = np.random.default_rng(1)
     for _ in range(2):
@@ -504,7 +505,8 @@ def run_serve(args, local_rank):
         "metric": "converged eigenpairs/s at resid<=1e-10 (served stream)", "value": nconv / wall,
         "unit": "eigenpairs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64",
         "data": "synthetic (seeded request stream)",
-        "config": dict(SERVE, requests=args.requests, rate_per_s=args.rate, workers=args.workers),
+        "config": dict(SERVE, requests=args.requests, rate_per_s=args.rate, workers=args.workers,
+                       admission=args.admission),
         "latency_s": {"p50": st.p50_latency, "p99": st.p99_latency, "mean": st.mean_latency,
                       "note": "submit -> done, host clock, queueing included"},
         "solve_seconds": {"p50": lat[len(lat) // 2], "max": lat[-1]},
@@ -737,6 +739,8 @@ def main():
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--rate", type=float, default=0.5, help="served stream arrivals per second")
     ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--admission", choices=["fifo", "shortest"], default="fifo",
+                    help="served stream admission order")
     ap.add_argument("--step-sweep", action="store_true", help="time the Clenshaw step across sizes and precisions")
     ap.add_argument("--large-only", action="store_true", help="with --step-sweep: only the J1-J2 L=24 case")
     ap.add_argument("--profile-step-large", choices=["fp64", "fp32"], default=None,

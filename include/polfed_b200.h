@@ -288,6 +288,13 @@ int pf_pool_stream(pf_pool *pool, int worker, void **stream);
  * the workers' high-priority streams, so their short launches are dispatched
  * ahead of the queued launches of larger solves.  Results are unchanged. */
 int pf_pool_set_priority_dim(pf_pool *pool, int64_t dim);
+/* Admission order.  PF_ADMIT_FIFO (default): arrival order.  PF_ADMIT_SHORTEST:
+ * the fitting request of least expected work D^2 (20.427 s + 1.696 nev) / nev
+ * first, except that a request queued for max_wait_s seconds goes first in
+ * arrival order and nothing overtakes it (no request waits forever). */
+#define PF_ADMIT_FIFO     0
+#define PF_ADMIT_SHORTEST 1
+int pf_pool_set_admission(pf_pool *pool, int policy, double max_wait_s);
 /* Estimated device bytes of one solve (what admission charges). */
 double pf_solve_footprint(const pf_op *op, const pf_params *params, int s, int nev);
 /* Solve n problems concurrently; arrays of length n (params may repeat one

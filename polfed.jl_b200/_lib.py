@@ -37,9 +37,10 @@ EXPORTED = [
     "pf_op_csr_create",
     "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
-    "pf_pool_set_priority_dim",
+    "pf_pool_set_priority_dim", "pf_pool_set_admission",
 ]
 PF_REQ_QUEUED, PF_REQ_RUNNING, PF_REQ_DONE, PF_REQ_FAILED = 0, 1, 2, 3
+PF_ADMIT_FIFO, PF_ADMIT_SHORTEST = 0, 1
 
 
 class PolfedError(RuntimeError):
@@ -144,6 +145,7 @@ def load():
         "pf_pool_destroy": (i32, [vp]),
         "pf_pool_stream": (i32, [vp, i32, ctypes.POINTER(vp)]),
         "pf_pool_set_priority_dim": (i32, [vp, i64]),
+        "pf_pool_set_admission": (i32, [vp, i32, f64]),
         "pf_solve_footprint": (f64, [vp, ctypes.POINTER(pf_params), i32, i32]),
         "pf_pool_solve_batch": (i32, [vp, i32, vp, vp, vp, vp, vp, i32, vp, vp, i32, vp, vp]),
         "pf_pool_submit": (i32, [vp, vp, ctypes.POINTER(pf_params), i32, i32, vp, vp, i32, ctypes.POINTER(i64)]),

@@ -422,6 +422,13 @@ class SolverPool:
         if priority_dim is not None:
             self.set_priority_dim(priority_dim)
 
+    def set_admission(self, policy: str = "fifo", max_wait: float = 30.0):
+        """Admission order: "fifo" (arrival order, the default) or "shortest"
+        (least expected work first; a request queued ``max_wait`` seconds goes
+        first and is not overtaken)."""
+        pol = {"fifo": _lib.PF_ADMIT_FIFO, "shortest": _lib.PF_ADMIT_SHORTEST}[policy]
+        _lib.check(_lib.load().pf_pool_set_admission(self._pool, pol, float(max_wait)))
+
     def set_priority_dim(self, dim: int):
         """Requests with operator dimension <= ``dim`` (default 65536; 0: none)
         run on high-priority streams; results are unchanged."""

@@ -316,6 +316,12 @@ int pf_pool_stream(pf_pool *pool, int worker, void **stream) {
     PF_API_END
 }
 
+int pf_pool_set_admission(pf_pool *pool, int policy, double max_wait_s) {
+    PF_API_BEGIN
+    pf::pool_set_admission(pool, policy, max_wait_s);
+    PF_API_END
+}
+
 int pf_pool_set_priority_dim(pf_pool *pool, int64_t dim) {
     PF_API_BEGIN
     pf::pool_set_priority_dim(pool, dim);

@@ -49,6 +49,7 @@ struct PoolRequest {
     int status = PF_OK;
     std::string error;
     double footprint = 0.0;
+    double cost = 0.0;                  // expected solve work (admission order)
     bool cancelled = false, batch = false, urgent = false;
     Clock::time_point t_submit, t_done;
 };
@@ -60,6 +61,8 @@ struct pf_pool {
     std::vector<pf_handle *> handles;   // one per worker, default stream priority
     std::vector<pf_handle *> urgent;    // one per worker, the device's highest stream priority
     int64_t priority_dim = 65536;       // requests with D <= this run on the urgent handles
+    int admission = PF_ADMIT_FIFO;
+    double max_wait = 30.0;             // PF_ADMIT_SHORTEST: seconds after which a request goes in arrival order
     std::vector<std::thread> threads;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -89,23 +92,59 @@ double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev) {
     return bytes;
 }
 
+// Expected work of a solve: the filter order grows like D / nev, a step costs
+// D * s, and the Krylov budget is (20.427 s + 1.696 nev) columns
+// (PolfedDefaults.jl:61-62), so work ~ D^2 (20.427 s + 1.696 nev) / nev.
+static double expected_cost(const pf_op *op, int s, int nev) {
+    const double D = (double)op->dim;
+    return D * D * (20.427 * s + 1.696 * nev) / std::max(nev, 1);
+}
+
+// Index in the queue of the request to start now, or -1.  A request larger
+// than the whole budget still runs alone.  FIFO: the head only.  SHORTEST:
+// cancelled entries and requests that waited max_wait seconds first, in
+// arrival order (nothing overtakes an aged request), otherwise the fitting
+// request of least expected cost (earliest among equals).
+static long pick_request(pf_pool *pool) {
+    auto fits = [&](const std::shared_ptr<PoolRequest> &r) {
+        return pool->in_use + r->footprint <= pool->budget || pool->running == 0;
+    };
+    if (pool->queue.empty()) return -1;
+    if (pool->admission == PF_ADMIT_FIFO) {
+        const auto &head = pool->queue.front();
+        return (head->cancelled || fits(head)) ? 0 : -1;
+    }
+    const auto now = Clock::now();
+    for (size_t i = 0; i < pool->queue.size(); ++i) {
+        const auto &r = pool->queue[i];
+        if (r->cancelled) return (long)i;
+        if (std::chrono::duration<double>(now - r->t_submit).count() >= pool->max_wait) return fits(r) ? (long)i : -1;
+    }
+    long best = -1;
+    for (size_t i = 0; i < pool->queue.size(); ++i) {
+        const auto &r = pool->queue[i];
+        if (fits(r) && (best < 0 || r->cost < pool->queue[(size_t)best]->cost)) best = (long)i;
+    }
+    return best;
+}
+
 static void pool_worker(pf_pool *pool, int w) {
     cudaSetDevice(pool->device);
     while (true) {
         std::shared_ptr<PoolRequest> req;
         {
             std::unique_lock<std::mutex> lock(pool->mu);
+            long pick = -1;
             pool->cv_work.wait(lock, [&] {
                 if (pool->stop) return true;
-                if (pool->queue.empty()) return false;
-                const auto &head = pool->queue.front();
-                // strict FIFO; a request larger than the whole budget still runs alone
-                return head->cancelled || pool->in_use + head->footprint <= pool->budget || pool->running == 0;
+                pick = pick_request(pool);
+                return pick >= 0;
             });
             if (pool->stop && pool->queue.empty()) return;
-            if (pool->queue.empty()) continue;
-            req = pool->queue.front();
-            pool->queue.pop_front();
+            if (pool->stop) pick = 0;   // shutting down: every queued entry is cancelled
+            if (pick < 0 || pool->queue.empty()) continue;
+            req = pool->queue[(size_t)pick];
+            pool->queue.erase(pool->queue.begin() + pick);
             if (req->cancelled) {
                 pool->requests.erase(req->id);
                 pool->cv_work.notify_all();
@@ -218,6 +257,17 @@ void pool_destroy(pf_pool *pool) {
     delete pool;
 }
 
+void pool_set_admission(pf_pool *pool, int policy, double max_wait) {
+    PF_CHECK(pool && (policy == PF_ADMIT_FIFO || policy == PF_ADMIT_SHORTEST) && max_wait >= 0, PF_ERR_INVALID,
+             "invalid admission policy");
+    {
+        std::lock_guard<std::mutex> lock(pool->mu);
+        pool->admission = policy;
+        pool->max_wait = max_wait;
+    }
+    pool->cv_work.notify_all();
+}
+
 void pool_set_priority_dim(pf_pool *pool, int64_t dim) {
     PF_CHECK(pool && dim >= 0, PF_ERR_INVALID, "invalid argument");
     std::lock_guard<std::mutex> lock(pool->mu);
@@ -241,6 +291,7 @@ static std::shared_ptr<PoolRequest> make_request(pf_pool *pool, pf_op *op, const
     r->s = s;
     r->nev = nev;
     r->footprint = solve_footprint(op, p, s, nev);
+    r->cost = expected_cost(op, s, nev);
     r->t_submit = Clock::now();
     return r;
 }

@@ -42,6 +42,7 @@ pf_pool *pool_create(int device, int workers, double budget);
 void pool_destroy(pf_pool *pool);
 cudaStream_t pool_stream(pf_pool *pool, int worker);
 void pool_set_priority_dim(pf_pool *pool, int64_t dim);
+void pool_set_admission(pf_pool *pool, int policy, double max_wait);
 int64_t pool_submit(pf_pool *pool, pf_op *op, const pf_params *p, int s, int nev, const double *x0,
                     double *vecs_out, int vecs_mem);
 int pool_solve_batch(pf_pool *pool, int n, pf_op *const *ops, const pf_params *const *params, const int *s,

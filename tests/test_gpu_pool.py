@@ -131,3 +131,23 @@ def test_failed_and_cancelled_requests_are_released(pkg, orc, cuda):
             pool.poll(dropped)
         st = pool.stats()
     assert st.failed == 1 and st.completed == 1 and st.submitted == 3
+
+
+def test_shortest_first_admission_lets_small_requests_pass(pkg, orc, cuda):
+    """PF_ADMIT_SHORTEST: behind a running request, a later small request
+    starts before an earlier large one; the large one still completes."""
+    rng = np.random.default_rng(21)
+    small = pkg.xxz_hamiltonian(12, 6, 1.0, 1.0, 5.0, rng=rng)       # D = 924
+    large = pkg.xxz_hamiltonian(16, 8, 1.0, 1.0, 5.0, rng=rng)       # D = 12870
+    kw = _kw(pkg, 4)
+    with pkg.SolverPool(workers=1) as pool:
+        pool.set_admission("shortest", max_wait=600.0)
+        blocker = pool.submit(large, rng.random(large.dim), NEV, TARGET, **kw)
+        big = pool.submit(large, rng.random(large.dim), NEV, TARGET, **kw)
+        little = pool.submit(small, rng.random(small.dim), NEV, TARGET, **kw)
+        pool.result(blocker)
+        vals, _ = pool.result(little)
+        assert pool.poll(big) in ("queued", "running")   # overtaken by the small request
+        assert len(vals) >= 1
+        vb, _ = pool.result(big)
+        assert len(vb) >= 1
