@@ -485,9 +485,13 @@ def run_serve(args, local_rank):
         item = {"model": name, "D": D, "nev": nev, "s": s, "eps": round(eps, 3)}
         try:
             vals, _, rep = pool.result(rid)
+        except pkg._lib.PolfedRejected as e:
+            # infeasible: fewer than nev states within reach of the target (the
+            # reference raises the same bisection error); rejected, not failed
+            item["rejected"] = str(e)
+            per.append(item)
+            continue
         except pkg._lib.PolfedError as e:
-            # the reference raises the same for an infeasible request (e.g. fewer
-            # states near the target than nev); the request fails, the stream goes on
             item["error"] = str(e)
             per.append(item)
             continue
@@ -512,6 +516,7 @@ def run_serve(args, local_rank):
         "solve_seconds": {"p50": lat[len(lat) // 2], "max": lat[-1]},
         "wall_seconds": wall, "busy_seconds": st.busy_seconds - base.busy_seconds,
         "converged": nconv, "completed": st.completed - base.completed, "failed": st.failed - base.failed,
+        "rejected": st.rejected - base.rejected,
         "hbm": {"budget_bytes": st.bytes_budget, "peak_admitted_bytes": st.bytes_peak},
         "clocks": clocks, "requests": per,
     }

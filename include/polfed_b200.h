@@ -6,6 +6,8 @@
  * torch type crosses this boundary; arrays are plain pointers plus sizes.
  * A handle owns one CUDA stream plus workspaces; handles are independent and
  * may be used from different host threads, but one handle is not re-entrant.
+ * Every entry point returns with the calling thread's current CUDA device
+ * unchanged (work runs on the handle's device whatever is current).
  *
  * Matrix-shaped arguments are column-major with a leading dimension, like a
  * Julia CuArray / Array.  "device" pointers are CUDA global memory on the
@@ -271,15 +273,31 @@ typedef struct pf_pool_stats {
     double  bytes_budget, bytes_in_use, bytes_peak;
     double  p50_latency, p99_latency, mean_latency;  /* seconds, submit -> done */
     double  busy_seconds;          /* wall time with at least one request running */
+    int64_t rejected;              /* infeasible requests (see PF_REQ_REJECTED) */
 } pf_pool_stats;
 
-#define PF_REQ_QUEUED  0
-#define PF_REQ_RUNNING 1
-#define PF_REQ_DONE    2
-#define PF_REQ_FAILED  3
+#define PF_REQ_QUEUED   0
+#define PF_REQ_RUNNING  1
+#define PF_REQ_DONE     2
+#define PF_REQ_FAILED   3
+/* The request cannot be met: the density of states holds fewer than nev
+ * states within reach of its target, so the interval bisection has no
+ * bracket (the reference raises the same error, Bisection.jl:18-40).  It is
+ * found in the planning stage, before any Lanczos work; pf_pool_fetch returns
+ * PF_ERR_NUMERIC with the reference's message. */
+#define PF_REQ_REJECTED 4
 
 int pf_pool_create(int device, int workers, double hbm_budget, pf_pool **out);
-int pf_pool_destroy(pf_pool *pool);   /* waits for running requests */
+/* Stop the pool without freeing it: queued requests fail with
+ * PF_ERR_INVALID ("pool destroyed ..."), threads blocked in pf_pool_fetch /
+ * pf_pool_wait / pf_pool_solve_batch are woken, running requests finish, and
+ * later submissions are refused.  Finished requests can still be fetched. */
+int pf_pool_shutdown(pf_pool *pool);
+/* pf_pool_shutdown, then free the pool once no thread is inside pf_pool_fetch,
+ * pf_pool_wait or pf_pool_solve_batch.  No call may start on the pool once
+ * pf_pool_destroy has been called (callers whose threads may still be about
+ * to call in use pf_pool_shutdown first and destroy after they are done). */
+int pf_pool_destroy(pf_pool *pool);
 /* The CUDA streams (cudaStream_t) of the pool: index w < workers is worker
  * w's default-priority stream, workers + w its high-priority stream; for
  * callers that order their own work or timing events against the solves. */
@@ -313,9 +331,17 @@ int pf_pool_submit(pf_pool *pool, pf_op *op, const pf_params *params, int s, int
 int pf_pool_poll(pf_pool *pool, int64_t request, int *state);
 /* Wait for (timeout_s < 0: indefinitely) and collect a finished request: vals
  * (nev doubles, host), report (may be NULL), *nconv; the request is released.
- * A failed request returns its error status. */
+ * A failed or rejected request returns its error status, and *nconv is then
+ * -PF_REQ_FAILED or -PF_REQ_REJECTED. */
 int pf_pool_fetch(pf_pool *pool, int64_t request, double timeout_s, double *vals, pf_report *report,
                   int *nconv);
+/* Wait (timeout_s < 0: indefinitely) until the request has finished, without
+ * collecting it; *state is its PF_REQ_* state when the wait ends. */
+int pf_pool_wait(pf_pool *pool, int64_t request, double timeout_s, int *state);
+/* Seconds since the pool was created at which the request was submitted,
+ * started and finished (times[3]; -1 for what has not happened yet).  Valid
+ * until the request is fetched, cancelled or collected. */
+int pf_pool_request_times(pf_pool *pool, int64_t request, double *times);
 /* Drop a queued request (a running one finishes and is then discarded). */
 int pf_pool_cancel(pf_pool *pool, int64_t request);
 int pf_pool_get_stats(pf_pool *pool, pf_pool_stats *stats);

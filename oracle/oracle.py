@@ -576,8 +576,14 @@ def make_rho(mu, N, kernel="Jackson"):
     kf = get_kernel(kernel)
     coeffs = np.array([kf(i, N) * mu[i] * (2 - (i == 0)) for i in range(N)])
 
+    # The quadrature of getbounds_from_dos integrates up to x = +-1 exactly,
+    # where 1/sqrt(1 - x^2) is infinite; nodes that round onto +-1 are moved
+    # to the nearest double inside (-1, 1), as the library's rho does, so the
+    # integrand stays finite.
+    xm = np.nextafter(1.0, 0.0)
+
     def rho(x):
-        x = np.asarray(x, dtype=np.float64)
+        x = np.clip(np.asarray(x, dtype=np.float64), -xm, xm)
         return clenshaw_coeffs_scalar(coeffs, x) / (np.pi * np.sqrt(1 - x ** 2))
     return rho
 
@@ -824,6 +830,31 @@ class PolfedResult:
     mu: np.ndarray
     info: LanczosInfo
     matvecs: int
+
+
+def plan_only(op, x0, howmany, target, *, Emin=None, Emax=None, order=None, left=None, right=None,
+              cutoff=0.17, normalization=1.0, order_safety_factor=0.97, N=250, kernel="Jackson",
+              probes=None):
+    """The planning stage of ``polfed`` alone (PolfedCore.jl:194-263 up to
+    definetransformation!): Emin / Emax probes, KPM DoS, interval and order.
+    Returns a PolfedResult without eigenpairs (vals, vecs, info empty)."""
+    x0 = prepare_initial_state(x0)
+    v0 = x0 if x0.ndim == 1 else x0[:, 0]
+    if Emin is None:
+        Emin = float(lanczos(op.apply, v0, 1, which="SR", maxdim=1000)[0][0])
+    if Emax is None:
+        Emax = float(lanczos(op.apply, v0, 1, which="LR", maxdim=1000)[0][-1])
+    a = (Emax - Emin) / 2
+    b = (Emax + Emin) / 2
+    plan = build_transform_plan(target, howmany, a, b, left=left, right=right, order=order,
+                                cutoff=cutoff, normalization=normalization, osf=order_safety_factor)
+    mu = dos_moments(op, a, b, N, probes)
+    rho = make_rho(mu, N, kernel)
+    getbounds(plan, a, b, rho, "mean")
+    getorderofexpansion(plan)
+    coeffs = filter_coefficients(plan)
+    return PolfedResult(np.zeros(0), np.zeros((op.D, 0)), Emin, Emax, a, b, plan.target, plan.left,
+                        plan.right, plan.order, coeffs, mu, LanczosInfo(), 0)
 
 
 def polfed(op, x0, howmany, target, *, Emin=None, Emax=None, order=None, left=None,

@@ -37,9 +37,10 @@ EXPORTED = [
     "pf_op_csr_create",
     "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
-    "pf_pool_set_priority_dim", "pf_pool_set_admission",
+    "pf_pool_set_priority_dim", "pf_pool_set_admission", "pf_pool_request_times",
+    "pf_pool_wait", "pf_pool_shutdown",
 ]
-PF_REQ_QUEUED, PF_REQ_RUNNING, PF_REQ_DONE, PF_REQ_FAILED = 0, 1, 2, 3
+PF_REQ_QUEUED, PF_REQ_RUNNING, PF_REQ_DONE, PF_REQ_FAILED, PF_REQ_REJECTED = 0, 1, 2, 3, 4
 PF_ADMIT_FIFO, PF_ADMIT_SHORTEST = 0, 1
 
 
@@ -53,6 +54,11 @@ class PolfedError(RuntimeError):
 
 class PolfedArgumentError(PolfedError, ValueError):
     """PF_ERR_INVALID: the reference raises ArgumentError / DimensionMismatch here."""
+
+
+class PolfedRejected(PolfedError):
+    """A served request that cannot be met: fewer than ``howmany`` states lie
+    within reach of its target (the reference's bisection error)."""
 
 
 class pf_params(ctypes.Structure):
@@ -98,7 +104,7 @@ class pf_pool_stats(ctypes.Structure):
         ("queued", ctypes.c_int64), ("running", ctypes.c_int64), ("eigenpairs", ctypes.c_int64),
         ("bytes_budget", ctypes.c_double), ("bytes_in_use", ctypes.c_double), ("bytes_peak", ctypes.c_double),
         ("p50_latency", ctypes.c_double), ("p99_latency", ctypes.c_double), ("mean_latency", ctypes.c_double),
-        ("busy_seconds", ctypes.c_double),
+        ("busy_seconds", ctypes.c_double), ("rejected", ctypes.c_int64),
     ]
 
 
@@ -153,6 +159,9 @@ def load():
         "pf_pool_fetch": (i32, [vp, i64, f64, vp, ctypes.POINTER(pf_report), ctypes.POINTER(i32)]),
         "pf_pool_cancel": (i32, [vp, i64]),
         "pf_pool_get_stats": (i32, [vp, ctypes.POINTER(pf_pool_stats)]),
+        "pf_pool_request_times": (i32, [vp, i64, vp]),
+        "pf_pool_wait": (i32, [vp, i64, f64, ctypes.POINTER(i32)]),
+        "pf_pool_shutdown": (i32, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import threading
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -398,6 +399,7 @@ class PoolStats:
     p99_latency: float
     mean_latency: float
     busy_seconds: float
+    rejected: int
 
 
 class SolverPool:
@@ -419,24 +421,54 @@ class SolverPool:
         _lib.check(_lib.load().pf_pool_create(device, int(workers), float(hbm_budget or 0.0), ctypes.byref(h)))
         self._pool = h
         self._pending: dict = {}
+        # native calls in flight from any Python thread; close() frees the pool
+        # only after the last of them has returned
+        self._cv = threading.Condition()
+        self._active = 0
+        self._closed = False
         if priority_dim is not None:
             self.set_priority_dim(priority_dim)
+
+    def _native(self, name, *args):
+        """Call pf_pool_<name>(pool, *args) so that close() cannot free the
+        pool under it; returns the status."""
+        with self._cv:
+            if self._closed or self._pool is None:
+                raise _lib.PolfedArgumentError(_lib.PF_ERR_INVALID, "pool is closed")
+            self._active += 1
+            pool = self._pool
+        try:
+            return getattr(_lib.load(), "pf_pool_" + name)(pool, *args)
+        finally:
+            with self._cv:
+                self._active -= 1
+                self._cv.notify_all()
 
     def set_admission(self, policy: str = "fifo", max_wait: float = 30.0):
         """Admission order: "fifo" (arrival order, the default) or "shortest"
         (least expected work first; a request queued ``max_wait`` seconds goes
         first and is not overtaken)."""
         pol = {"fifo": _lib.PF_ADMIT_FIFO, "shortest": _lib.PF_ADMIT_SHORTEST}[policy]
-        _lib.check(_lib.load().pf_pool_set_admission(self._pool, pol, float(max_wait)))
+        _lib.check(self._native("set_admission", pol, float(max_wait)))
 
     def set_priority_dim(self, dim: int):
         """Requests with operator dimension <= ``dim`` (default 65536; 0: none)
         run on high-priority streams; results are unchanged."""
-        _lib.check(_lib.load().pf_pool_set_priority_dim(self._pool, int(dim)))
+        _lib.check(self._native("set_priority_dim", int(dim)))
 
     def close(self):
-        if self._pool is not None and self._pool.value:
-            _lib.check(_lib.load().pf_pool_destroy(self._pool))
+        """Stop the pool: queued requests fail ("pool destroyed"), threads
+        waiting for them return, running requests finish; then free it."""
+        with self._cv:
+            if self._closed or self._pool is None or not self._pool.value:
+                self._closed = True
+                return
+            self._closed = True
+            pool = self._pool
+        _lib.check(_lib.load().pf_pool_shutdown(pool))
+        with self._cv:
+            self._cv.wait_for(lambda: self._active == 0)
+        _lib.check(_lib.load().pf_pool_destroy(pool))
         self._pool = None
         self._pending.clear()
 
@@ -465,7 +497,7 @@ class SolverPool:
         out, w = [], 0
         while True:
             st = ctypes.c_void_p()
-            if _lib.load().pf_pool_stream(self._pool, w, ctypes.byref(st)) != _lib.PF_OK:
+            if self._native("stream", w, ctypes.byref(st)) != _lib.PF_OK:
                 return out
             out.append(st.value or 0)
             w += 1
@@ -516,8 +548,7 @@ class SolverPool:
         a_V = (P * n)(*vptr) if want_vecs else None
         reps = (_lib.pf_report * n)()
         nconv = (ctypes.c_int * n)()
-        _lib.check(_lib.load().pf_pool_solve_batch(self._pool, n, a_ops, a_par, a_s, a_nev, a_x, mem,
-                                                   a_v, a_V, mem, reps, nconv))
+        _lib.check(self._native("solve_batch", n, a_ops, a_par, a_s, a_nev, a_x, mem, a_v, a_V, mem, reps, nconv))
         del keep
         out = []
         for i in range(n):
@@ -541,19 +572,35 @@ class SolverPool:
         p, _, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
         V = np.zeros((op.dim, howmany), order="F") if want_vecs else None
         rid = ctypes.c_int64()
-        _lib.check(_lib.load().pf_pool_submit(self._pool, op.op, ctypes.byref(p), s, int(howmany), x.ctypes.data,
-                                              V.ctypes.data if want_vecs else None, _lib.PF_MEM_HOST,
-                                              ctypes.byref(rid)))
+        _lib.check(self._native("submit", op.op, ctypes.byref(p), s, int(howmany), x.ctypes.data,
+                                V.ctypes.data if want_vecs else None, _lib.PF_MEM_HOST, ctypes.byref(rid)))
         # the operator stays referenced until the result is collected: the
         # worker binds it when the request starts and updates its tuning after
         self._pending[rid.value] = (V, int(howmany), want_rep, kind, val, op)
         return rid.value
 
     def poll(self, request: int) -> str:
-        """"queued", "running", "done" or "failed"."""
+        """"queued", "running", "done", "failed" or "rejected" (the target
+        cannot hold ``howmany`` states; ``result`` raises the reference's
+        bisection error)."""
         st = ctypes.c_int()
-        _lib.check(_lib.load().pf_pool_poll(self._pool, int(request), ctypes.byref(st)))
-        return ("queued", "running", "done", "failed")[st.value]
+        _lib.check(self._native("poll", int(request), ctypes.byref(st)))
+        return ("queued", "running", "done", "failed", "rejected")[st.value]
+
+    def wait(self, request: int, timeout: Optional[float] = None) -> str:
+        """Wait until the request has finished (or ``timeout`` seconds pass)
+        without collecting it; returns its state as ``poll`` does."""
+        state = ctypes.c_int()
+        _lib.check(self._native("wait", int(request), -1.0 if timeout is None else float(timeout),
+                                ctypes.byref(state)))
+        return ("queued", "running", "done", "failed", "rejected")[state.value]
+
+    def times(self, request: int):
+        """(submitted, started, finished) in seconds since the pool was
+        created; -1 for what has not happened yet.  Valid until ``result``."""
+        t = (ctypes.c_double * 3)()
+        _lib.check(self._native("request_times", int(request), t))
+        return tuple(t)
 
     def result(self, request: int, timeout: Optional[float] = None):
         """Wait for a request and return its ``polfed`` result tuple; raises the
@@ -562,10 +609,12 @@ class SolverPool:
         vals = np.zeros(howmany)
         rep = _lib.pf_report()
         n = ctypes.c_int()
-        st = _lib.load().pf_pool_fetch(self._pool, int(request), -1.0 if timeout is None else float(timeout),
-                                       vals.ctypes.data, ctypes.byref(rep), ctypes.byref(n))
+        st = self._native("fetch", int(request), -1.0 if timeout is None else float(timeout), vals.ctypes.data,
+                          ctypes.byref(rep), ctypes.byref(n))
         if not (st == _lib.PF_ERR_NUMERIC and b"timeout" in _lib.load().pf_last_error()):
             self._pending.pop(request, None)
+        if st != _lib.PF_OK and n.value == -_lib.PF_REQ_REJECTED:
+            raise _lib.PolfedRejected(st, _lib.load().pf_last_error().decode(errors="replace"))
         _lib.check(st)
         k = n.value
         res = (vals[:k].copy(), V[:, :k].copy() if V is not None else None)
@@ -574,12 +623,12 @@ class SolverPool:
         return res
 
     def cancel(self, request: int):
-        _lib.check(_lib.load().pf_pool_cancel(self._pool, int(request)))
+        _lib.check(self._native("cancel", int(request)))
         self._pending.pop(request, None)
 
     def stats(self) -> PoolStats:
         st = _lib.pf_pool_stats()
-        _lib.check(_lib.load().pf_pool_get_stats(self._pool, ctypes.byref(st)))
+        _lib.check(self._native("get_stats", ctypes.byref(st)))
         return PoolStats(**{f: getattr(st, f) for f, _ in st._fields_})
 
 

@@ -16,7 +16,25 @@ void set_last_error(const std::string &msg) { g_last_error = msg; }
 thread_local int t_new_handle_priority = 0;
 }  // namespace pf
 
-#define PF_API_BEGIN try {
+// Every entry point leaves the calling thread's current CUDA device as it
+// found it (the library switches to a handle's device internally), so a
+// caller working on another GPU is not moved.
+struct DeviceRestore {
+    int dev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            dev = -1;
+            cudaGetLastError();
+        }
+    }
+    ~DeviceRestore() {
+        if (dev >= 0) cudaSetDevice(dev);
+    }
+};
+
+#define PF_API_BEGIN      \
+    DeviceRestore pf_dev_restore_; \
+    try {
 #define PF_API_END                                              \
     return PF_OK;                                               \
     }                                                           \
@@ -309,6 +327,12 @@ int pf_pool_destroy(pf_pool *pool) {
     PF_API_END
 }
 
+int pf_pool_shutdown(pf_pool *pool) {
+    PF_API_BEGIN
+    pf::pool_shutdown(pool);
+    PF_API_END
+}
+
 int pf_pool_stream(pf_pool *pool, int worker, void **stream) {
     PF_API_BEGIN
     PF_CHECK(pool && stream, PF_ERR_INVALID, "null argument");
@@ -371,6 +395,20 @@ int pf_pool_cancel(pf_pool *pool, int64_t request) {
     PF_API_BEGIN
     PF_CHECK(pool, PF_ERR_INVALID, "null pool");
     pf::pool_cancel(pool, request);
+    PF_API_END
+}
+
+int pf_pool_wait(pf_pool *pool, int64_t request, double timeout_s, int *state) {
+    PF_API_BEGIN
+    PF_CHECK(pool && state, PF_ERR_INVALID, "null argument");
+    *state = pf::pool_wait(pool, request, timeout_s);
+    PF_API_END
+}
+
+int pf_pool_request_times(pf_pool *pool, int64_t request, double *times) {
+    PF_API_BEGIN
+    PF_CHECK(pool && times, PF_ERR_INVALID, "null argument");
+    pf::pool_request_times(pool, request, times);
     PF_API_END
 }
 

@@ -50,8 +50,8 @@ struct PoolRequest {
     std::string error;
     double footprint = 0.0;
     double cost = 0.0;                  // expected solve work (admission order)
-    bool cancelled = false, batch = false, urgent = false;
-    Clock::time_point t_submit, t_done;
+    bool cancelled = false, batch = false, urgent = false, started = false;
+    Clock::time_point t_submit, t_start, t_done;
 };
 
 }  // namespace pf
@@ -69,14 +69,23 @@ struct pf_pool {
     std::deque<std::shared_ptr<pf::PoolRequest>> queue;
     std::unordered_map<int64_t, std::shared_ptr<pf::PoolRequest>> requests;
     double budget = 0.0, in_use = 0.0, peak = 0.0;
-    int64_t next_id = 1, submitted = 0, completed = 0, failed = 0, running = 0, eigenpairs = 0;
+    int64_t next_id = 1, submitted = 0, completed = 0, failed = 0, rejected = 0, running = 0, eigenpairs = 0;
     std::vector<double> latencies;
     double busy = 0.0;
-    pf::Clock::time_point busy_since;
+    pf::Clock::time_point busy_since, t_created;
     bool stop = false;
+    int waiters = 0;                    // threads blocked in fetch / solve_batch (destroy waits for them)
 };
 
 namespace pf {
+
+// Device memory a handle may still grow after creation (library workspaces,
+// its auxiliary handle); the default HBM budget keeps this much per handle free.
+constexpr size_t kHandleReserveBytes = size_t(96) << 20;
+
+static bool finished(int state) {
+    return state == PF_REQ_DONE || state == PF_REQ_FAILED || state == PF_REQ_REJECTED;
+}
 
 double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev) {
     const double D = (double)op->dim;
@@ -140,8 +149,7 @@ static void pool_worker(pf_pool *pool, int w) {
                 pick = pick_request(pool);
                 return pick >= 0;
             });
-            if (pool->stop && pool->queue.empty()) return;
-            if (pool->stop) pick = 0;   // shutting down: every queued entry is cancelled
+            if (pool->stop) return;   // pool_destroy has already failed every queued request
             if (pick < 0 || pool->queue.empty()) continue;
             req = pool->queue[(size_t)pick];
             pool->queue.erase(pool->queue.begin() + pick);
@@ -151,6 +159,8 @@ static void pool_worker(pf_pool *pool, int w) {
                 continue;
             }
             req->urgent = req->op->dim <= pool->priority_dim;
+            req->started = true;
+            req->t_start = Clock::now();
             pool->in_use += req->footprint;
             pool->peak = std::max(pool->peak, pool->in_use);
             if (pool->running++ == 0) pool->busy_since = Clock::now();
@@ -160,6 +170,7 @@ static void pool_worker(pf_pool *pool, int w) {
         // dispatched ahead of queued launches of larger solves (same results)
         pf_handle *h = req->urgent ? pool->urgent[w] : pool->handles[w];
         int status = PF_OK;
+        bool infeasible = false;
         std::string err;
         pf_op *view = nullptr;
         try {
@@ -170,6 +181,7 @@ static void pool_worker(pf_pool *pool, int w) {
         } catch (const Error &e) {
             status = e.code;
             err = e.what();
+            infeasible = e.infeasible;
         } catch (const std::exception &e) {
             status = PF_ERR_CUDA;
             err = e.what();
@@ -183,7 +195,9 @@ static void pool_worker(pf_pool *pool, int w) {
             req->t_done = Clock::now();
             req->status = status;
             req->error = err;
-            req->state = status == PF_OK ? PF_REQ_DONE : PF_REQ_FAILED;
+            // an infeasible request (fewer than nev states within reach of its
+            // target, the reference's bisection error) is rejected, not failed
+            req->state = status == PF_OK ? PF_REQ_DONE : (infeasible ? PF_REQ_REJECTED : PF_REQ_FAILED);
             if (status == PF_OK) {
                 ++pool->completed;
                 pool->eigenpairs += req->nconv;
@@ -192,6 +206,8 @@ static void pool_worker(pf_pool *pool, int w) {
                     if (req->rep_out) *req->rep_out = req->rep;
                     if (req->nconv_out) *req->nconv_out = req->nconv;
                 }
+            } else if (infeasible) {
+                ++pool->rejected;
             } else {
                 ++pool->failed;
             }
@@ -207,12 +223,7 @@ pf_pool *pool_create(int device, int workers, double budget) {
     PF_CUDA(cudaSetDevice(device));
     pf_pool *pool = new pf_pool();
     pool->device = device;
-    if (budget <= 0) {
-        size_t fr = 0, tot = 0;
-        PF_CUDA(cudaMemGetInfo(&fr, &tot));
-        budget = 0.9 * (double)fr;
-    }
-    pool->budget = budget;
+    pool->t_created = Clock::now();
     try {
         int least = 0, greatest = 0;
         PF_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -227,6 +238,16 @@ pf_pool *pool_create(int device, int workers, double budget) {
             if (st != PF_OK) throw Error(PF_ERR_CUDA, pf_last_error());
             pool->urgent.push_back(h);
         }
+        if (budget <= 0) {
+            // read after the handles exist; each of the 2 W handles later grows
+            // library workspaces and an auxiliary handle of its own, so keep a
+            // reserve for those out of the budget
+            size_t fr = 0, tot = 0;
+            PF_CUDA(cudaMemGetInfo(&fr, &tot));
+            const double reserve = 2.0 * workers * double(kHandleReserveBytes);
+            budget = std::max(0.0, 0.9 * ((double)fr - reserve));
+        }
+        pool->budget = budget;
         for (int w = 0; w < workers; ++w) pool->threads.emplace_back(pool_worker, pool, w);
     } catch (...) {
         {
@@ -243,15 +264,38 @@ pf_pool *pool_create(int device, int workers, double budget) {
     return pool;
 }
 
-void pool_destroy(pf_pool *pool) {
+void pool_shutdown(pf_pool *pool) {
     if (!pool) return;
     {
+        // queued requests never run: they fail with "pool destroyed", and
+        // threads waiting for them in fetch / solve_batch are woken
         std::lock_guard<std::mutex> lock(pool->mu);
-        for (auto &r : pool->queue) r->cancelled = true;
+        if (pool->stop) return;
+        for (auto &r : pool->queue) {
+            r->state = PF_REQ_FAILED;
+            r->status = PF_ERR_INVALID;
+            r->error = "pool destroyed before the request started";
+            r->t_done = Clock::now();
+            ++pool->failed;
+        }
+        pool->queue.clear();
         pool->stop = true;
     }
     pool->cv_work.notify_all();
-    for (auto &t : pool->threads) t.join();
+    pool->cv_done.notify_all();
+    for (auto &t : pool->threads) t.join();   // running requests finish
+    pool->threads.clear();
+}
+
+void pool_destroy(pf_pool *pool) {
+    if (!pool) return;
+    pool_shutdown(pool);
+    {
+        // no thread may still be inside fetch / wait / solve_batch when the pool goes
+        std::unique_lock<std::mutex> lock(pool->mu);
+        pool->cv_done.notify_all();
+        pool->cv_done.wait(lock, [&] { return pool->waiters == 0; });
+    }
     for (auto h : pool->handles) pf_handle_destroy(h);
     for (auto h : pool->urgent) pf_handle_destroy(h);
     delete pool;
@@ -344,14 +388,17 @@ int pool_solve_batch(pf_pool *pool, int n, pf_op *const *ops, const pf_params *c
     for (auto &r : reqs) enqueue(pool, r);
     int status = PF_OK;
     std::unique_lock<std::mutex> lock(pool->mu);
+    ++pool->waiters;
     for (auto &r : reqs) {
-        pool->cv_done.wait(lock, [&] { return r->state == PF_REQ_DONE || r->state == PF_REQ_FAILED; });
+        pool->cv_done.wait(lock, [&] { return finished(r->state); });
         if (r->status != PF_OK && status == PF_OK) {
             status = r->status;
             first_error = r->error;
         }
         pool->requests.erase(r->id);
     }
+    --pool->waiters;
+    pool->cv_done.notify_all();
     return status;
 }
 
@@ -370,13 +417,18 @@ int pool_fetch(pf_pool *pool, int64_t id, double timeout_s, double *vals, pf_rep
     auto r = it->second;
     PF_CHECK(!r->batch, PF_ERR_INVALID, "batch requests are collected by pf_pool_solve_batch");
     PF_CHECK(!r->cancelled, PF_ERR_INVALID, "request was cancelled");
-    auto done = [&] { return r->state == PF_REQ_DONE || r->state == PF_REQ_FAILED; };
+    auto done = [&] { return finished(r->state); };
+    ++pool->waiters;
+    bool ok = true;
     if (timeout_s < 0) pool->cv_done.wait(lock, done);
-    else if (!pool->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), done))
-        throw Error(PF_ERR_NUMERIC, "request not finished within the timeout");
+    else ok = pool->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), done);
+    --pool->waiters;
+    pool->cv_done.notify_all();
+    if (!ok) throw Error(PF_ERR_NUMERIC, "request not finished within the timeout");
     pool->requests.erase(id);
     if (r->status != PF_OK) {
         error = r->error;
+        if (nconv) *nconv = -r->state;
         return r->status;
     }
     if (vals) std::copy(r->vals.begin(), r->vals.begin() + r->nconv, vals);
@@ -400,12 +452,39 @@ void pool_cancel(pf_pool *pool, int64_t id) {
     pool->cv_work.notify_all();
 }
 
+int pool_wait(pf_pool *pool, int64_t id, double timeout_s) {
+    std::unique_lock<std::mutex> lock(pool->mu);
+    auto it = pool->requests.find(id);
+    PF_CHECK(it != pool->requests.end(), PF_ERR_INVALID, "unknown request");
+    auto r = it->second;
+    PF_CHECK(!r->cancelled, PF_ERR_INVALID, "request was cancelled");
+    auto done = [&] { return finished(r->state); };
+    ++pool->waiters;
+    if (timeout_s < 0) pool->cv_done.wait(lock, done);
+    else pool->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), done);
+    --pool->waiters;
+    pool->cv_done.notify_all();
+    return r->state;
+}
+
+void pool_request_times(pf_pool *pool, int64_t id, double *times) {
+    std::lock_guard<std::mutex> lock(pool->mu);
+    auto it = pool->requests.find(id);
+    PF_CHECK(it != pool->requests.end(), PF_ERR_INVALID, "unknown request");
+    const auto &r = it->second;
+    auto since = [&](Clock::time_point t) { return std::chrono::duration<double>(t - pool->t_created).count(); };
+    times[0] = since(r->t_submit);
+    times[1] = r->started ? since(r->t_start) : -1.0;
+    times[2] = finished(r->state) ? since(r->t_done) : -1.0;
+}
+
 void pool_stats(pf_pool *pool, pf_pool_stats *st) {
     std::lock_guard<std::mutex> lock(pool->mu);
     std::memset(st, 0, sizeof(*st));
     st->submitted = pool->submitted;
     st->completed = pool->completed;
     st->failed = pool->failed;
+    st->rejected = pool->rejected;
     st->queued = (int64_t)pool->queue.size();
     st->running = pool->running;
     st->eigenpairs = pool->eigenpairs;

@@ -40,6 +40,7 @@ extern thread_local int t_new_handle_priority;
 double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev);
 pf_pool *pool_create(int device, int workers, double budget);
 void pool_destroy(pf_pool *pool);
+void pool_shutdown(pf_pool *pool);
 cudaStream_t pool_stream(pf_pool *pool, int worker);
 void pool_set_priority_dim(pf_pool *pool, int64_t dim);
 void pool_set_admission(pf_pool *pool, int policy, double max_wait);
@@ -53,5 +54,7 @@ int pool_fetch(pf_pool *pool, int64_t id, double timeout_s, double *vals, pf_rep
                std::string &error);
 void pool_cancel(pf_pool *pool, int64_t id);
 void pool_stats(pf_pool *pool, pf_pool_stats *st);
+void pool_request_times(pf_pool *pool, int64_t id, double *times);
+int pool_wait(pf_pool *pool, int64_t id, double timeout_s);
 
 }  // namespace pf

@@ -62,7 +62,12 @@ Dos::Dos(const std::vector<double> &mu, int N, int kernel) : N_(N) {
     for (int i = 0; i < N; ++i) coeffs_[i] = kernel_weight(kernel, i, N) * mu[i] * (2.0 - (i == 0 ? 1.0 : 0.0));
 }
 
+// Quadrature nodes that round onto x = +-1 (getbounds_from_dos integrates up
+// to the spectrum's edges) are moved to the nearest double inside (-1, 1), so
+// the 1/sqrt(1 - x^2) weight stays finite.
 double Dos::operator()(double x) const {
+    const double xm = std::nextafter(1.0, 0.0);
+    x = std::min(std::max(x, -xm), xm);
     return cheb_clenshaw(coeffs_.data(), N_ - 1, x) / (M_PI * std::sqrt(1.0 - x * x));
 }
 
@@ -157,7 +162,14 @@ void bounds_from_dos(TransformState &t, const Dos &rho) {
         const double n = quadgk([&](double x) { return rho(x); }, lo, hi, 1e-12, 1e-12, 10000000L);
         return n >= t.howmany ? -1 : +1;
     };
-    const double d = bisection(f, 0.0, 1.0, 1e-8, 500);
+    double d = 0.0;
+    try {
+        d = bisection(f, 0.0, 1.0, 1e-8, 500);
+    } catch (Error &e) {
+        // no interval around the target holds howmany states: the request is infeasible
+        e.infeasible = true;
+        throw;
+    }
     bound_fns(0, t.target, d, t.left, t.right);
 }
 

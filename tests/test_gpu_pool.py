@@ -133,21 +133,94 @@ def test_failed_and_cancelled_requests_are_released(pkg, orc, cuda):
     assert st.failed == 1 and st.completed == 1 and st.submitted == 3
 
 
-def test_shortest_first_admission_lets_small_requests_pass(pkg, orc, cuda):
-    """PF_ADMIT_SHORTEST: behind a running request, a later small request
-    starts before an earlier large one; the large one still completes."""
+def _blocked_pool_order(pkg, policy, max_wait):
+    """One worker: a blocker runs, then an earlier large and a later small
+    request wait; returns the two waiting requests' start times (seconds)."""
     rng = np.random.default_rng(21)
     small = pkg.xxz_hamiltonian(12, 6, 1.0, 1.0, 5.0, rng=rng)       # D = 924
     large = pkg.xxz_hamiltonian(16, 8, 1.0, 1.0, 5.0, rng=rng)       # D = 12870
     kw = _kw(pkg, 4)
     with pkg.SolverPool(workers=1) as pool:
-        pool.set_admission("shortest", max_wait=600.0)
+        pool.set_admission(policy, max_wait=max_wait)
         blocker = pool.submit(large, rng.random(large.dim), NEV, TARGET, **kw)
         big = pool.submit(large, rng.random(large.dim), NEV, TARGET, **kw)
         little = pool.submit(small, rng.random(small.dim), NEV, TARGET, **kw)
+        assert pool.poll(big) == "queued" and pool.poll(little) == "queued"
         pool.result(blocker)
-        vals, _ = pool.result(little)
-        assert pool.poll(big) in ("queued", "running")   # overtaken by the small request
-        assert len(vals) >= 1
+        tb, tl = None, None
+        for rid in (big, little):
+            pool.wait(rid)
+        tb, tl = pool.times(big), pool.times(little)
         vb, _ = pool.result(big)
-        assert len(vb) >= 1
+        vl, _ = pool.result(little)
+    assert len(vb) >= 1 and len(vl) >= 1
+    assert tb[0] < tl[0]                     # submitted in this order
+    assert tb[1] >= 0 and tl[1] >= 0 and tb[2] >= tb[1] and tl[2] >= tl[1]
+    return tb[1], tl[1]
+
+
+def test_shortest_first_admission_lets_small_requests_pass(pkg, orc, cuda):
+    """PF_ADMIT_SHORTEST: behind a running request, a later small request
+    starts before an earlier large one."""
+    t_big, t_little = _blocked_pool_order(pkg, "shortest", 600.0)
+    assert t_little < t_big
+
+
+def test_aged_requests_keep_arrival_order(pkg, orc, cuda):
+    """PF_ADMIT_SHORTEST with max_wait = 0: every queued request has aged, so
+    arrival order comes back (the large request starts first)."""
+    t_big, t_little = _blocked_pool_order(pkg, "shortest", 0.0)
+    assert t_big < t_little
+
+
+def test_fifo_admission_keeps_arrival_order(pkg, orc, cuda):
+    t_big, t_little = _blocked_pool_order(pkg, "fifo", 30.0)
+    assert t_big < t_little
+
+
+def test_infeasible_request_is_rejected(pkg, orc, cuda):
+    """A request whose target cannot hold howmany states (here more states
+    than the whole space) is rejected with the reference's bisection error,
+    counted apart from failures; the pool goes on serving."""
+    probs, rng = _problems(pkg, orc)
+    op, H, s = probs[0]
+    D = H.shape[0]
+    with pkg.SolverPool(workers=1) as pool:
+        bad = pool.submit(op, _x0(rng, D, 1), D + 5, TARGET, **_kw(pkg, 1))
+        good = pool.submit(op, _x0(rng, D, 1), NEV, TARGET, **_kw(pkg, 2))
+        assert pool.wait(bad) == "rejected"
+        with pytest.raises(pkg._lib.PolfedRejected, match="opposite signs"):
+            pool.result(bad)
+        vals, vecs = pool.result(good)
+        _residuals_ok(H, vals, vecs)
+        st = pool.stats()
+    assert st.rejected == 1 and st.failed == 0 and st.completed == 1
+
+
+def test_destroy_wakes_waiting_threads(pkg, orc, cuda):
+    """Closing a pool while another thread waits for a queued request fails
+    that request ("pool destroyed") and returns the waiting thread."""
+    import threading
+    import time
+    rng = np.random.default_rng(8)
+    op = pkg.xxz_hamiltonian(16, 8, 1.0, 1.0, 5.0, rng=rng)       # D = 12870: the first solve takes a while
+    D = op.dim
+    pool = pkg.SolverPool(workers=1)
+    pool.submit(op, rng.random(D), NEV, TARGET, **_kw(pkg, 1))
+    queued = [pool.submit(op, rng.random(D), NEV, TARGET, **_kw(pkg, 2 + k)) for k in range(3)]
+    outcome = {}
+
+    def waiter():
+        try:
+            pool.result(queued[-1])
+            outcome["r"] = "done"
+        except pkg._lib.PolfedError as e:
+            outcome["r"] = str(e)
+
+    t = threading.Thread(target=waiter)
+    t.start()
+    time.sleep(0.5)                  # the waiter is now blocked in the native fetch
+    pool.close()
+    t.join(timeout=120)
+    assert not t.is_alive()
+    assert "pool destroyed" in outcome["r"] or "pool is closed" in outcome["r"], outcome
