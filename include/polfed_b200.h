@@ -170,17 +170,33 @@ int pf_kpm_moments(pf_op *op, int dtype, double a, double b, int N, int R,
 
 /* Autotuner (no reference counterpart: the reference has no kernel variants).
  * Times every variant of the Clenshaw step kernel for block width s and dtype
- * on scratch blocks -- 1, 2, 4, 8 or 16 columns per thread, and for chain
- * operators with s in {4, 8, 16, 32} the warp-cooperative step (width
- * PF_WIDTH_COOP: the s lanes of a warp share one row) -- keeps the fastest
- * for this operator and returns it in *width; times_ms[i] (optional, 6
- * entries) receives the measured milliseconds per launch of widths 1, 2, 4,
- * 8, 16 and PF_WIDTH_COOP (0 where not offered). */
+ * on scratch blocks -- 1, 2, 4, 8 or 16 columns per thread, each with five
+ * (gather batch, register cap) profiles (and, for the Quantum Sun, the
+ * asynchronous-gather profile of pf_set_step_variant), and for chain operators with s in
+ * {4, 8, 16, 32} the warp-cooperative step (width PF_WIDTH_COOP: the s lanes
+ * of a warp share one row) -- keeps the fastest for this operator and returns
+ * its width in *width; times_ms[i] (optional, 6 entries) receives the
+ * measured milliseconds per launch of the fastest profile of widths 1, 2, 4,
+ * 8, 16 and PF_WIDTH_COOP (0 where not offered).  Every variant computes the
+ * same sums in the same order.  The choice is also written to a persistent
+ * cache ($POLFED_B200_TUNE_CACHE, else ~/.cache/polfed_b200/step_variants.json)
+ * that pf_solve consults before timing. */
 #define PF_WIDTH_COOP 0
 int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms);
+/* The step-kernel variant in use for (dtype, s): columns per thread (0: the
+ * warp-cooperative step), gathers issued per batch and the resident CTAs per
+ * SM it is compiled for (its register cap). */
+int pf_step_variant(pf_op *op, int dtype, int s, int *width, int *gather_batch, int *ctas_per_sm);
 /* Pin the step-kernel variant for (dtype, s) without timing (a width the
  * autotuner could have chosen); later launches on this operator use it. */
 int pf_set_step_width(pf_op *op, int dtype, int s, int width);
+/* Same with a profile: 0 = the width's default gather batch and register cap,
+ * 1..4 = (8 gathers, 2 CTAs/SM), (8, 3), (4, 4), (8, 4); 5 = Quantum Sun
+ * operators only, with 16- or 32-byte column segments: every gather of a row
+ * issued at once as an asynchronous global-to-shared copy; 6 = Quantum Sun
+ * operators only: each CTA stages a tile of 2^t consecutive rows in shared
+ * memory and serves the grain block and the low outer-bit flips from it. */
+int pf_set_step_variant(pf_op *op, int dtype, int s, int width, int profile);
 
 /* ----------------------------------------------------------- solving */
 typedef struct pf_params {
@@ -274,6 +290,10 @@ typedef struct pf_pool_stats {
     double  p50_latency, p99_latency, mean_latency;  /* seconds, submit -> done */
     double  busy_seconds;          /* wall time with at least one request running */
     int64_t rejected;              /* infeasible requests (see PF_REQ_REJECTED) */
+    /* the filter engine's batched step launches: number, summed kernel time
+     * (CUDA events, seconds), algorithmic bytes moved (streams x D x s x
+     * element size per instance-step) and instance-steps served */
+    double  filter_launches, filter_seconds, filter_bytes, filter_instance_steps;
 } pf_pool_stats;
 
 #define PF_REQ_QUEUED   0
@@ -302,6 +322,14 @@ int pf_pool_destroy(pf_pool *pool);
  * w's default-priority stream, workers + w its high-priority stream; for
  * callers that order their own work or timing events against the solves. */
 int pf_pool_stream(pf_pool *pool, int worker, void **stream);
+/* Batched filtering (default off): the Clenshaw steps of every request in
+ * flight run as one multi-instance launch per step on the pool's engine
+ * stream (continuous batching: a filter joins at the next step after it is
+ * submitted and leaves after its own final sum).  Each instance computes
+ * exactly the rows and sums of the per-solve kernel.  Off: every request runs
+ * its own graph-captured filter on its worker stream.  Applies to requests
+ * that start after the call. */
+int pf_pool_set_batching(pf_pool *pool, int on);
 /* Requests on operators of dimension <= dim (default 65536; 0: none) run on
  * the workers' high-priority streams, so their short launches are dispatched
  * ahead of the queued launches of larger solves.  Results are unchanged. */

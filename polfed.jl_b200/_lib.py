@@ -38,7 +38,7 @@ EXPORTED = [
     "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
     "pf_pool_set_priority_dim", "pf_pool_set_admission", "pf_pool_request_times",
-    "pf_pool_wait", "pf_pool_shutdown",
+    "pf_pool_wait", "pf_pool_shutdown", "pf_pool_set_batching", "pf_step_variant", "pf_set_step_variant",
 ]
 PF_REQ_QUEUED, PF_REQ_RUNNING, PF_REQ_DONE, PF_REQ_FAILED, PF_REQ_REJECTED = 0, 1, 2, 3, 4
 PF_ADMIT_FIFO, PF_ADMIT_SHORTEST = 0, 1
@@ -105,6 +105,8 @@ class pf_pool_stats(ctypes.Structure):
         ("bytes_budget", ctypes.c_double), ("bytes_in_use", ctypes.c_double), ("bytes_peak", ctypes.c_double),
         ("p50_latency", ctypes.c_double), ("p99_latency", ctypes.c_double), ("mean_latency", ctypes.c_double),
         ("busy_seconds", ctypes.c_double), ("rejected", ctypes.c_int64),
+        ("filter_launches", ctypes.c_double), ("filter_seconds", ctypes.c_double),
+        ("filter_bytes", ctypes.c_double), ("filter_instance_steps", ctypes.c_double),
     ]
 
 
@@ -147,6 +149,8 @@ def load():
         "pf_lanczos_extrema": (i32, [vp, vp, i32, f64, f64, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
         "pf_autotune": (i32, [vp, i32, i32, ctypes.POINTER(i32), vp]),
         "pf_set_step_width": (i32, [vp, i32, i32, i32]),
+        "pf_set_step_variant": (i32, [vp, i32, i32, i32, i32]),
+        "pf_step_variant": (i32, [vp, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "pf_pool_create": (i32, [i32, i32, f64, ctypes.POINTER(vp)]),
         "pf_pool_destroy": (i32, [vp]),
         "pf_pool_stream": (i32, [vp, i32, ctypes.POINTER(vp)]),
@@ -162,6 +166,7 @@ def load():
         "pf_pool_request_times": (i32, [vp, i64, vp]),
         "pf_pool_wait": (i32, [vp, i64, f64, ctypes.POINTER(i32)]),
         "pf_pool_shutdown": (i32, [vp]),
+        "pf_pool_set_batching": (i32, [vp, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

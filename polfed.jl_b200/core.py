@@ -400,6 +400,10 @@ class PoolStats:
     mean_latency: float
     busy_seconds: float
     rejected: int
+    filter_launches: float
+    filter_seconds: float
+    filter_bytes: float
+    filter_instance_steps: float
 
 
 class SolverPool:
@@ -450,6 +454,12 @@ class SolverPool:
         first and is not overtaken)."""
         pol = {"fifo": _lib.PF_ADMIT_FIFO, "shortest": _lib.PF_ADMIT_SHORTEST}[policy]
         _lib.check(self._native("set_admission", pol, float(max_wait)))
+
+    def set_batching(self, on: bool = True):
+        """Batched filtering (default off): the Clenshaw steps of all requests
+        in flight share one multi-instance launch per step.  Off: each request
+        runs its own graph-captured filter.  Results are the same either way."""
+        _lib.check(self._native("set_batching", 1 if on else 0))
 
     def set_priority_dim(self, dim: int):
         """Requests with operator dimension <= ``dim`` (default 65536; 0: none)
@@ -797,10 +807,23 @@ def autotune(op: Operator, s: int, dtype: str = "fp64"):
     return w.value, {widths[i]: t[i] for i in range(6) if t[i] > 0}
 
 
-def set_step_width(op: Operator, s: int, width: int, dtype: str = "fp64"):
-    """Pin the step-kernel variant for block width ``s`` (see ``autotune``)."""
+def step_variant(op: Operator, s: int, dtype: str = "fp64"):
+    """The step-kernel variant in use for block width ``s``: (columns per
+    thread, gathers per batch, resident CTAs per SM); width 0 is the
+    warp-cooperative chain step."""
+    w, u, mb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
     dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
-    _lib.check(_lib.load().pf_set_step_width(op.op, dt, int(s), int(width)))
+    _lib.check(_lib.load().pf_step_variant(op.op, dt, int(s), ctypes.byref(w), ctypes.byref(u), ctypes.byref(mb)))
+    return w.value, u.value, mb.value
+
+
+def set_step_width(op: Operator, s: int, width: int, dtype: str = "fp64", profile: int = 0):
+    """Pin the step-kernel variant for block width ``s`` (see ``autotune``):
+    ``width`` columns per thread (0: the warp-cooperative chain step) and a
+    (gather batch, register cap) ``profile`` 0..4, or 5 (Quantum Sun only: all
+    of a row's gathers as asynchronous global-to-shared copies)."""
+    dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
+    _lib.check(_lib.load().pf_set_step_variant(op.op, dt, int(s), int(width), int(profile)))
 
 
 def basis_states(op: Operator, idx):

@@ -238,18 +238,54 @@ int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms) {
     PF_API_BEGIN
     PF_CHECK(op && width, PF_ERR_INVALID, "null argument");
     std::vector<std::pair<int, float>> t;
-    *width = pf::autotune_step(op, s, dtype, &t);
+    const int code = pf::autotune_step(op, s, dtype, &t);
+    *width = code == PF_WIDTH_COOP ? PF_WIDTH_COOP : pf::variant_width(code);
     if (times_ms) {
         for (int i = 0; i < 6; ++i) times_ms[i] = 0.f;
         for (auto &pr : t) {
             int idx = 5;  // PF_WIDTH_COOP
             if (pr.first != PF_WIDTH_COOP) {
+                const int w = pf::variant_width(pr.first);
                 idx = 0;
-                while ((1 << idx) < pr.first) ++idx;
+                while ((1 << idx) < w) ++idx;
             }
-            if (idx < 6) times_ms[idx] = pr.second;
+            // the fastest profile of each width
+            if (idx < 6 && (times_ms[idx] == 0.f || pr.second < times_ms[idx])) times_ms[idx] = pr.second;
         }
     }
+    PF_API_END
+}
+
+int pf_step_variant(pf_op *op, int dtype, int s, int *width, int *gather_batch, int *ctas_per_sm) {
+    PF_API_BEGIN
+    PF_CHECK(op && width && gather_batch && ctas_per_sm, PF_ERR_INVALID, "null argument");
+    PF_CHECK(dtype == PF_F64 || dtype == PF_F32, PF_ERR_INVALID, "dtype must be PF_F64 or PF_F32");
+    PF_CHECK(s >= 1, PF_ERR_INVALID, "s must be positive");
+    const int elem = dtype == PF_F64 ? 8 : 4;
+    int code = pf::default_width(s, elem);
+    {
+        std::lock_guard<std::mutex> lock(op->tune_mu);
+        auto it = op->tuned_width.find(std::make_pair(elem, s));
+        if (it != op->tuned_width.end()) code = it->second;
+    }
+    pf::variant_params(code, elem, width, gather_batch, ctas_per_sm);
+    PF_API_END
+}
+
+int pf_set_step_variant(pf_op *op, int dtype, int s, int width, int profile) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    PF_CHECK(profile >= 0 && profile <= pf::kStepProfiles, PF_ERR_INVALID, "profile must be in 0..6");
+    PF_CHECK(width != PF_WIDTH_COOP || profile == 0, PF_ERR_INVALID, "the warp-cooperative step has no profiles");
+    PF_CHECK(profile != pf::kProfileAsync || pf::qsun_async_eligible(op, s, width, dtype == PF_F64 ? 8 : 4),
+             PF_ERR_INVALID,
+             "asynchronous gathers (profile 5) need a Quantum Sun operator and 16- or 32-byte column segments");
+    PF_CHECK(profile != pf::kProfileTile || pf::qsun_tile_eligible(op, s, width, dtype == PF_F64 ? 8 : 4),
+             PF_ERR_INVALID, "row tiles (profile 6) need a Quantum Sun operator with at least 2^8 states");
+    const int st = pf_set_step_width(op, dtype, s, width);
+    if (st != PF_OK) return st;
+    std::lock_guard<std::mutex> lock(op->tune_mu);
+    op->tuned_width[std::make_pair(dtype == PF_F64 ? 8 : 4, s)] = pf::variant_code(width, profile);
     PF_API_END
 }
 
@@ -343,6 +379,12 @@ int pf_pool_stream(pf_pool *pool, int worker, void **stream) {
 int pf_pool_set_admission(pf_pool *pool, int policy, double max_wait_s) {
     PF_API_BEGIN
     pf::pool_set_admission(pool, policy, max_wait_s);
+    PF_API_END
+}
+
+int pf_pool_set_batching(pf_pool *pool, int on) {
+    PF_API_BEGIN
+    pf::pool_set_batching(pool, on);
     PF_API_END
 }
 

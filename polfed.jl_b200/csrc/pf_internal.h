@@ -116,6 +116,7 @@ __host__ __device__ inline int rank_table_offset(int c) {
 }  // namespace pf
 
 // ------------------------------------------------------------ opaque handles
+struct pf_engine;
 struct pf_handle {
     int device = 0;
     int num_sms = 148;
@@ -133,6 +134,9 @@ struct pf_handle {
     // (the two extremal Lanczos probes); created on first use
     pf_handle *aux = nullptr;
     std::mutex aux_mu;
+    // filter engine of the pool this handle works for (not owned); null: the
+    // handle runs its own graph-captured filters
+    pf_engine *engine = nullptr;
     // page-locked staging for the solver's small host<->device transfers
     // (pageable copies are staged by the driver synchronously and serialise
     // concurrent solves); grown on demand
@@ -158,6 +162,10 @@ struct pf_op {
     float *d_diag32 = nullptr;
     // owns d_states / d_rank_tab; shared with the views pf_op_bind makes on other handles
     std::shared_ptr<void> tables_owner;
+    // device copies of the descriptors, read by the multi-instance step kernel
+    // of the filter engine; shared with views
+    void *d_desc64 = nullptr, *d_desc32 = nullptr;
+    std::shared_ptr<void> multi_owner;
     int smem_bytes = 0;               // dynamic shared memory of the step kernels
     // autotuned columns-per-thread of the step kernel, keyed by (element bytes, s)
     std::mutex tune_mu;
@@ -196,12 +204,33 @@ void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q,
                        int V);
 int default_width(int s, int elem_bytes);
 constexpr int kCoopWidth = 0;
+// A step-kernel variant code: columns per thread V (bits 0-7) and a profile
+// (bits 8+; 0 = default gather batch and register cap, 1..kStepProfiles =
+// the tuned (batch, resident CTAs) pairs (8,2) (8,3) (4,4) (8,4), 5 =
+// asynchronous gathers and 6 = shared-memory row tiles, both Quantum Sun
+// only), or kCoopWidth for the warp-cooperative chain step.
+constexpr int kStepProfiles = 6;
+// Profile 5: the Quantum Sun step with asynchronous (cp.async) row gathers;
+// profile 6: the Quantum Sun step over shared-memory tiles of 2^t rows.
+constexpr int kProfileAsync = 5;
+constexpr int kProfileTile = 6;
+bool qsun_async_eligible(const pf_op *op, int s, int V, int elem);
+bool qsun_tile_eligible(const pf_op *op, int s, int V, int elem);
+constexpr int variant_code(int V, int profile) { return V | (profile << 8); }
+constexpr int variant_width(int code) { return code & 0xff; }
+constexpr int variant_profile(int code) { return code >> 8; }
 bool coop_eligible(const pf_op *op, int s, int flags);
 // Diagonal of a chain operator in both precisions (same term order as the step kernels).
 void build_chain_diag(pf_op *op);
 // Times every columns-per-thread width of the Clenshaw step for (s, dtype) on
 // scratch blocks and records the fastest in op->tuned_width.  Returns it.
 int autotune_step(pf_op *op, int s, int dtype, std::vector<std::pair<int, float>> *timings);
+extern thread_local bool t_refuse_spilling;
+// Take the variant for (s, dtype) from the persistent tuning cache, if it holds
+// one for this device, model and size; returns whether it did.
+bool cached_step_variant(pf_op *op, int s, int dtype);
+// (gather batch U, resident CTAs per SM) of a variant code for element size elem.
+void variant_params(int code, int elem, int *V, int *U, int *MB);
 
 // RI <-> column-major conversion, optional precision change.
 template <typename TS, typename TD>

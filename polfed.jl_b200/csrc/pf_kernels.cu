@@ -25,6 +25,7 @@
 //     of (outer bit, grain bit) with value g0 c_j / 4, plus the dense grain
 //     block on the low L_grain bits (held in shared memory).
 #include "pf_internal.h"
+#include "pf_rows.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -32,197 +33,6 @@
 #include <mutex>
 
 namespace pf {
-
-template <typename T, int V>
-struct alignas(sizeof(T) * V) Pack {
-    T v[V];
-};
-
-template <typename T, int V>
-__device__ __forceinline__ Pack<T, V> ldp(const T *p) {
-    return *reinterpret_cast<const Pack<T, V> *>(p);
-}
-template <typename T, int V>
-__device__ __forceinline__ void stp(T *p, const Pack<T, V> &v) {
-    *reinterpret_cast<Pack<T, V> *>(p) = v;
-}
-
-// ------------------------------------------------------------ sector rank
-__device__ __forceinline__ uint32_t sector_rank(uint32_t st, const uint32_t *tab, int nchunks) {
-    uint32_t r = 0;
-    int p = 0;
-    int off = 0;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        if (c < nchunks) {
-            uint32_t byte = (st >> (8 * c)) & 0xffu;
-            r += tab[off + p * 256 + (int)byte];
-            p += __popc(byte);
-            off += (8 * c + 1) * 256;
-        }
-    }
-    return r;
-}
-
-// ------------------------------------------------------------ row models
-// Each returns (through acc / diag) the off-diagonal gather sum and the
-// diagonal element of row `row` for columns c0..c0+V-1.
-
-// Gathers are issued in unrolled batches of U independent loads so that each
-// thread keeps several L2/HBM requests in flight (the loop bodies have no
-// load-to-load dependence); accumulation follows the reference's term order.
-// U shrinks as the per-thread column count V grows, to bound registers.
-template <typename T, int V>
-struct Batch {
-    static constexpr int bytes = V * (int)sizeof(T);
-    static constexpr int U = bytes >= 64 ? 2 : (bytes >= 16 ? 4 : 8);
-};
-
-// Resident CTAs per SM the step kernel is compiled for: caps registers so
-// enough warps stay resident to cover L2 latency with independent gathers
-// (with no cap the 64-byte-per-thread variants took 170 registers, one CTA
-// per SM, 8 warps -- latency-bound).
-template <typename T, int V>
-struct MinBlocks {
-    static constexpr int bytes = V * (int)sizeof(T);
-    static constexpr int value = bytes >= 32 ? 2 : 3;
-};
-
-template <typename T, int V, bool HASQ>
-__device__ __forceinline__ void chain_row(const ChainDesc<T> &d, const uint32_t *tab, uint32_t row,
-                                          int s, int c0, const T *__restrict__ q, T (&acc)[V],
-                                          T &diag) {
-    constexpr int U = Batch<T, V>::U;
-    const uint32_t st = d.full ? row : __ldg(d.states + row);
-    T dg = T(0);
-    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
-    const T *qc = q + c0;
-    for (int b0 = 0; b0 < d.nb; b0 += U) {
-        uint32_t r2[U];
-        bool act[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int b = b0 + u;
-            act[u] = false;
-            r2[u] = 0u;
-            if (b < d.nb) {
-                const uint32_t bm = d.bmask[b];
-                const uint32_t m = st & bm;
-                const bool differ = (m != 0u) && (m != bm);
-                dg += differ ? -d.jdq[b] : d.jdq[b];
-                act[u] = differ;
-                if (HASQ && differ) {
-                    const uint32_t st2 = st ^ bm;
-                    r2[u] = d.full ? st2 : sector_rank(st2, tab, d.nchunks);
-                }
-            }
-        }
-        if constexpr (HASQ) {
-            Pack<T, V> g[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (act[u]) g[u] = ldp<T, V>(qc + (size_t)r2[u] * s);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (act[u]) {
-                    const T jh = d.jhalf[b0 + u];
-#pragma unroll
-                    for (int v = 0; v < V; ++v) acc[v] += jh * g[u].v[v];
-                }
-        }
-    }
-    diag = dg;
-}
-
-// Quantum Sun shared-memory layout: the grain block with a padded row stride
-// (dg + 1, so the 8 rows of one grain group read different banks), then four
-// 256-entry diagonal tables, one per byte of the outer-spin bits.
-template <typename T>
-struct QSunSmem {
-    static __host__ __device__ int grain_stride(int dg) { return dg + 1; }
-    static __host__ __device__ int bytes(int dg) { return (dg * (dg + 1) + 4 * 256) * (int)sizeof(T); }
-};
-
-template <typename T, int V, bool HASQ>
-__device__ __forceinline__ void qsun_row(const QSunDesc<T> &d, const T *smem_t, uint32_t row,
-                                         int s, int c0, const T *__restrict__ q, T (&acc)[V],
-                                         T &diag) {
-    constexpr int U = Batch<T, V>::U;
-    const int gs = d.dg + 1;
-    const T *dtab = smem_t + d.dg * gs;
-    const uint32_t outer = row >> d.L_grain;
-    T dg = dtab[outer & 0xffu];
-    if (d.L_loc > 8) dg += dtab[256 + ((outer >> 8) & 0xffu)];
-    if (d.L_loc > 16) dg += dtab[512 + ((outer >> 16) & 0xffu)];
-    if (d.L_loc > 24) dg += dtab[768 + ((outer >> 24) & 0xffu)];
-    diag = dg;
-    if constexpr (HASQ) {
-        const T *qc = q + c0;
-        for (int j0 = 0; j0 < d.L_loc; j0 += U) {
-            Pack<T, V> g[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (j0 + u < d.L_loc) g[u] = ldp<T, V>(qc + (size_t)(row ^ d.fmask[j0 + u]) * s);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (j0 + u < d.L_loc) {
-                    const T cf = d.cflip[j0 + u];
-#pragma unroll
-                    for (int v = 0; v < V; ++v) acc[v] += cf * g[u].v[v];
-                }
-        }
-        const uint32_t g = row & ((uint32_t)d.dg - 1u);
-        const uint32_t base = row - g;
-        const T *grow = smem_t + g * gs;
-        for (int h0 = 0; h0 < d.dg; h0 += U) {
-            Pack<T, V> x[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (h0 + u < d.dg) x[u] = ldp<T, V>(qc + (size_t)(base + h0 + u) * s);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (h0 + u < d.dg) {
-                    const T w = grow[h0 + u];
-#pragma unroll
-                    for (int v = 0; v < V; ++v) acc[v] += w * x[u].v[v];
-                }
-        }
-    }
-}
-
-// CSR row (a user matrix): the entries of the row in storage order, gathered
-// in unrolled batches of U like the matrix-free rows; the diagonal is an
-// ordinary entry, so diag = 0.
-template <typename T, int V, bool HASQ>
-__device__ __forceinline__ void csr_row(const CsrDesc<T> &d, uint32_t row, int s, int c0, const T *__restrict__ q,
-                                        T (&acc)[V], T &diag) {
-    diag = T(0);
-    if constexpr (HASQ) {
-        constexpr int U = Batch<T, V>::U;
-        const int64_t b = __ldg(d.indptr + row), e = __ldg(d.indptr + row + 1);
-        const T *qc = q + c0;
-        for (int64_t p0 = b; p0 < e; p0 += U) {
-            int32_t col[U];
-            T val[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (p0 + u < e) {
-                    col[u] = __ldg(d.indices + p0 + u);
-                    val[u] = __ldg(d.values + p0 + u);
-                }
-            Pack<T, V> g[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (p0 + u < e) g[u] = ldp<T, V>(qc + (size_t)col[u] * s);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (p0 + u < e) {
-#pragma unroll
-                    for (int v = 0; v < V; ++v) acc[v] += val[u] * g[u].v[v];
-                }
-        }
-    }
-}
 
 template <typename T>
 struct StepArgs {
@@ -283,8 +93,11 @@ __device__ void finish_reduction(int nvals, const double *blockvals, double *par
     }
 }
 
-template <typename T, int V, class Desc, int FLAGS>
-__global__ void __launch_bounds__(kThreads, MinBlocks<T, V>::value) k_step(const Desc d, const StepArgs<T> a) {
+// UB > 0 / MB > 0: a tuned variant's gather batch and resident-CTA target
+// (register cap); 0 keeps the defaults of Batch / MinBlocks.
+template <typename T, int V, class Desc, int FLAGS, int UB = 0, int MB = 0>
+__global__ void __launch_bounds__(kThreads, MB > 0 ? MB : MinBlocks<T, V>::value)
+    k_step(const Desc d, const StepArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr bool HASQ = (FLAGS & StepFlags::Q) != 0;
     constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
@@ -326,38 +139,29 @@ __global__ void __launch_bounds__(kThreads, MinBlocks<T, V>::value) k_step(const
         const uint32_t row = (G == 1u) ? it : it / G;
         const int c0 = (G == 1u) ? 0 : (int)(it - row * G) * V;
         const size_t off = (size_t)row * a.s + c0;
+        if constexpr (HASX) prefetch_l1(a.x + off);
+        if constexpr (HASQ) prefetch_l1(a.q + off);
+        if constexpr (HASP) prefetch_l1(a.p + off);
         T acc[V];
 #pragma unroll
         for (int v = 0; v < V; ++v) acc[v] = T(0);
         T diag;
         if constexpr (DescTraits<Desc>::kind == OP_CHAIN)
-            chain_row<T, V, HASQ>(d, tab, row, a.s, c0, a.q, acc, diag);
+            chain_row<T, V, HASQ, UB>(d, tab, row, a.s, c0, a.q, acc, diag);
         else if constexpr (DescTraits<Desc>::kind == OP_QSUN)
-            qsun_row<T, V, HASQ>(d, smem_t, row, a.s, c0, a.q, acc, diag);
+            qsun_row<T, V, HASQ, UB>(d, smem_t, row, a.s, c0, a.q, acc, diag);
         else
-            csr_row<T, V, HASQ>(d, row, a.s, c0, a.q, acc, diag);
-        Pack<T, V> res;
+            csr_row<T, V, HASQ, UB>(d, row, a.s, c0, a.q, acc, diag);
+        Pack<T, V> xo, qo, po, res;
 #pragma unroll
-        for (int v = 0; v < V; ++v) res.v[v] = T(0);
-        if constexpr (HASX) {
-            const Pack<T, V> xo = ldp<T, V>(a.x + off);
+        for (int v = 0; v < V; ++v) xo.v[v] = qo.v[v] = po.v[v] = T(0);
+        if constexpr (HASX) xo = ldp<T, V>(a.x + off);
+        if constexpr (HASQ) qo = ldp<T, V>(a.q + off);
+        if constexpr (HASP) po = ldp<T, V>(a.p + off);
 #pragma unroll
-            for (int v = 0; v < V; ++v) res.v[v] = a.cx * xo.v[v];
-        }
-        Pack<T, V> qo;
-        if constexpr (HASQ) {
-            qo = ldp<T, V>(a.q + off);
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                const T hq = (acc[v] + diag * qo.v[v]) * a.inva - a.boa * qo.v[v];
-                res.v[v] = res.v[v] + a.alpha * hq;
-            }
-        }
-        if constexpr (HASP) {
-            const Pack<T, V> po = ldp<T, V>(a.p + off);
-#pragma unroll
-            for (int v = 0; v < V; ++v) res.v[v] = res.v[v] + a.beta * po.v[v];
-        }
+        for (int v = 0; v < V; ++v)
+            res.v[v] = step_combine<T>(HASX, HASQ, HASP, a.cx, xo.v[v], a.alpha, acc[v], diag, qo.v[v], a.inva, a.boa,
+                                       a.beta, po.v[v]);
         stp<T, V>(a.out + off, res);
         if constexpr (DOTS) {
 #pragma unroll
@@ -521,22 +325,218 @@ __global__ void __launch_bounds__(kThreads) k_step_coop(const ChainDesc<T> d, co
                 coop_round<T, S>(d, sbm, tab, st, valid, b0, lr, rb, qc, r, g);
 #pragma unroll
                 for (int j = 0; j < S; ++j)
-                    if (r[j] != 0xffffffffu) acc += d.jhalf[b0 + j] * g[j];
+                    if (r[j] != 0xffffffffu) acc = fma_t(d.jhalf[b0 + j], g[j], acc);
             }
         }
         if (valid) {
-            T res = T(0);
-            if constexpr (HASX) res = a.cx * xo;
-            if constexpr (HASQ) {
-                const T hq = (acc + dgv * qo) * a.inva - a.boa * qo;
-                res = res + a.alpha * hq;
-            }
-            if constexpr (HASP) res = res + a.beta * po;
+            const T res = step_combine<T>(HASX, HASQ, HASP, a.cx, xo, a.alpha, acc, dgv, qo, a.inva, a.boa, a.beta, po);
             a.out[t] = res;
         }
     }
 }
 
+
+// ------------------------------------------------ asynchronous-gather QSun step
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Byte offset of the gather slots in k_step_qsun_async's shared memory.
+template <typename T>
+__host__ __device__ inline int qsun_async_slot_offset() {
+    return (QSunSmem<T>::bytes(PF_MAX_GRAIN) + 15) / 16 * 16;
+}
+
+// Quantum Sun step whose row gathers are asynchronous global->shared copies
+// (cp.async): all L_loc flipped rows and dg grain rows of an item are in
+// flight at once while no register holds them, instead of a few per dependent
+// round.  Each thread then waits for its own copies (no barrier: a thread
+// reads only its own slots, laid out so consecutive threads read consecutive
+// 16-byte words) and accumulates in qsun_row's order -- flips, then the grain
+// row -- with the same rounded operations, so results equal every other
+// variant's.
+template <typename T, int V, int FLAGS>
+__global__ void __launch_bounds__(kThreads) k_step_qsun_async(const QSunDesc<T> d, const StepArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
+    constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
+    constexpr int CH = V * (int)sizeof(T) / 16;   // 16-byte copies per gathered segment
+    static_assert(CH >= 1 && V * (int)sizeof(T) == 16 * CH, "segments must be whole 16-byte words");
+    T *sm = reinterpret_cast<T *>(smem_raw);
+    const int gs = d.dg + 1;
+    for (int i = threadIdx.x; i < d.dg * d.dg; i += blockDim.x) sm[(i / d.dg) * gs + (i % d.dg)] = d.grain[i];
+    T *dtab = sm + d.dg * gs;
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+        const int c = i >> 8, byte = i & 255;
+        T acc = T(0);
+        for (int t = 0; t < 8; ++t) {
+            const int j = 8 * c + t;
+            if (j < d.L_loc) acc += ((byte >> t) & 1) ? d.hhalf[j] : -d.hhalf[j];
+        }
+        dtab[i] = acc;
+    }
+    __syncthreads();
+    uint4 *slots = reinterpret_cast<uint4 *>(smem_raw + qsun_async_slot_offset<T>());
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t G = (uint32_t)a.G;
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < a.items; it += stride) {
+        const uint32_t row = (G == 1u) ? it : it / G;
+        const int c0 = (G == 1u) ? 0 : (int)(it - row * G) * V;
+        const size_t off = (size_t)row * a.s + c0;
+        const T *qc = a.q + c0;
+        for (int k = 0; k < d.L_loc; ++k) {
+            const T *src = qc + (size_t)(row ^ d.fmask[k]) * a.s;
+#pragma unroll
+            for (int c = 0; c < CH; ++c) cp_async16(&slots[(k * CH + c) * kThreads + threadIdx.x], src + c * (16 / sizeof(T)));
+        }
+        const uint32_t g = row & ((uint32_t)d.dg - 1u);
+        const uint32_t base = row - g;
+        for (int h = 0; h < d.dg; ++h) {
+            const T *src = qc + (size_t)(base + h) * a.s;
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                cp_async16(&slots[((d.L_loc + h) * CH + c) * kThreads + threadIdx.x], src + c * (16 / sizeof(T)));
+        }
+        // the row's own operands travel while the copies are in flight
+        Pack<T, V> xo, qo, po, res;
+#pragma unroll
+        for (int v = 0; v < V; ++v) xo.v[v] = po.v[v] = T(0);
+        if constexpr (HASX) xo = ldp<T, V>(a.x + off);
+        qo = ldp<T, V>(a.q + off);
+        if constexpr (HASP) po = ldp<T, V>(a.p + off);
+        const uint32_t outer = row >> d.L_grain;
+        T diag = dtab[outer & 0xffu];
+        if (d.L_loc > 8) diag += dtab[256 + ((outer >> 8) & 0xffu)];
+        if (d.L_loc > 16) diag += dtab[512 + ((outer >> 16) & 0xffu)];
+        if (d.L_loc > 24) diag += dtab[768 + ((outer >> 24) & 0xffu)];
+        cp_async_wait_all();
+        T acc[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = T(0);
+        for (int k = 0; k < d.L_loc; ++k) {
+            Pack<T, V> gv;
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                reinterpret_cast<uint4 *>(&gv)[c] = slots[(k * CH + c) * kThreads + threadIdx.x];
+            const T cf = d.cflip[k];
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = fma_t(cf, gv.v[v], acc[v]);
+        }
+        const T *grow = sm + g * gs;
+        for (int h = 0; h < d.dg; ++h) {
+            Pack<T, V> gv;
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                reinterpret_cast<uint4 *>(&gv)[c] = slots[((d.L_loc + h) * CH + c) * kThreads + threadIdx.x];
+            const T w = grow[h];
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = fma_t(w, gv.v[v], acc[v]);
+        }
+#pragma unroll
+        for (int v = 0; v < V; ++v)
+            res.v[v] = step_combine<T>(HASX, true, HASP, a.cx, xo.v[v], a.alpha, acc[v], diag, qo.v[v], a.inva, a.boa,
+                                       a.beta, po.v[v]);
+        stp<T, V>(a.out + off, res);
+    }
+}
+
+// ------------------------------------------------------- tiled QSun step
+// Rows of a tile of 2^t consecutive states differ only in their low t bits,
+// so a flip of an outer bit below t, and the whole grain block (the low
+// L_grain bits), stay inside the tile.  Each CTA stages its tile's segment of
+// q (V columns) in shared memory with coalesced loads, then serves those
+// gathers from shared memory; only flips of the outer bits at or above t go
+// to L2.  The row sums run in qsun_row's order (flips j = 0..L_loc-1, then the
+// grain row) with the same rounded operations, so results equal every other
+// variant's.
+template <typename T>
+__host__ __device__ inline int qsun_tile_offset() {
+    return (QSunSmem<T>::bytes(PF_MAX_GRAIN) + 63) / 64 * 64;
+}
+
+template <typename T, int V, int FLAGS>
+__global__ void __launch_bounds__(kThreads, 2) k_step_qsun_tile(const QSunDesc<T> d, const StepArgs<T> a, int tbits) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
+    constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
+    constexpr int U = 4;
+    T *sm = reinterpret_cast<T *>(smem_raw);
+    const int gs = d.dg + 1;
+    for (int i = threadIdx.x; i < d.dg * d.dg; i += blockDim.x) sm[(i / d.dg) * gs + (i % d.dg)] = d.grain[i];
+    T *dtab = sm + d.dg * gs;
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
+        const int c = i >> 8, byte = i & 255;
+        T acc = T(0);
+        for (int t = 0; t < 8; ++t) {
+            const int j = 8 * c + t;
+            if (j < d.L_loc) acc += ((byte >> t) & 1) ? d.hhalf[j] : -d.hhalf[j];
+        }
+        dtab[i] = acc;
+    }
+    Pack<T, V> *tile = reinterpret_cast<Pack<T, V> *>(smem_raw + qsun_tile_offset<T>());
+    const uint32_t R = 1u << tbits;
+    const uint32_t G = (uint32_t)a.G;
+    const uint32_t ntiles = (a.D >> tbits) * G;
+    for (uint32_t tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+        const uint32_t r0 = (tl / G) << tbits;
+        const int c0 = (int)(tl % G) * V;
+        __syncthreads();   // the previous tile (and, the first time, the tables) is done / ready
+        for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) tile[i] = ldp<T, V>(a.q + (size_t)(r0 + i) * a.s + c0);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) {
+            const uint32_t row = r0 + i;
+            const size_t off = (size_t)row * a.s + c0;
+            if constexpr (HASX) prefetch_l1(a.x + off);
+            if constexpr (HASP) prefetch_l1(a.p + off);
+            T acc[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = T(0);
+            for (int j0 = 0; j0 < d.L_loc; j0 += U) {
+                Pack<T, V> g[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (j0 + u < d.L_loc) {
+                        const uint32_t nb = row ^ d.fmask[j0 + u];
+                        g[u] = ((nb ^ row) >> tbits) == 0u ? tile[nb - r0] : ldp<T, V>(a.q + (size_t)nb * a.s + c0);
+                    }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    if (j0 + u < d.L_loc) {
+                        const T cf = d.cflip[j0 + u];
+#pragma unroll
+                        for (int v = 0; v < V; ++v) acc[v] = fma_t(cf, g[u].v[v], acc[v]);
+                    }
+            }
+            const uint32_t gr = row & ((uint32_t)d.dg - 1u);
+            const uint32_t base = i - gr;
+            const T *grow = sm + gr * gs;
+            for (int h = 0; h < d.dg; ++h) {
+                const Pack<T, V> xg = tile[base + h];
+                const T w = grow[h];
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[v] = fma_t(w, xg.v[v], acc[v]);
+            }
+            const uint32_t outer = row >> d.L_grain;
+            T diag = dtab[outer & 0xffu];
+            if (d.L_loc > 8) diag += dtab[256 + ((outer >> 8) & 0xffu)];
+            if (d.L_loc > 16) diag += dtab[512 + ((outer >> 16) & 0xffu)];
+            if (d.L_loc > 24) diag += dtab[768 + ((outer >> 24) & 0xffu)];
+            Pack<T, V> xo, po, res;
+            const Pack<T, V> qo = tile[i];
+#pragma unroll
+            for (int v = 0; v < V; ++v) xo.v[v] = po.v[v] = T(0);
+            if constexpr (HASX) xo = ldp<T, V>(a.x + off);
+            if constexpr (HASP) po = ldp<T, V>(a.p + off);
+#pragma unroll
+            for (int v = 0; v < V; ++v)
+                res.v[v] = step_combine<T>(HASX, true, HASP, a.cx, xo.v[v], a.alpha, acc[v], diag, qo.v[v], a.inva,
+                                           a.boa, a.beta, po.v[v]);
+            stp<T, V>(a.out + off, res);
+        }
+    }
+}
 
 static thread_local int64_t t_launches = 0;
 void count_launches(int64_t n) { t_launches += n; }
@@ -576,9 +576,24 @@ static int blocks_per_sm(const void *kern, int smem) {
     return nb;
 }
 
-template <typename T, int V, class Desc, int FLAGS>
+// Set by the autotuner: variants whose registers spill to local memory are
+// refused (PF_ERR_UNSUPPORTED) instead of timed.
+thread_local bool t_refuse_spilling = false;
+
+static bool spills(const void *kern) {
+    thread_local std::map<const void *, bool> cache;
+    auto it = cache.find(kern);
+    if (it != cache.end()) return it->second;
+    cudaFuncAttributes attr;
+    PF_CUDA(cudaFuncGetAttributes(&attr, kern));
+    return cache[kern] = attr.localSizeBytes > 0;
+}
+
+template <typename T, int V, class Desc, int FLAGS, int UB = 0, int MB = 0>
 static void launch_one(pf_op *op, cudaStream_t st, const Desc &d, StepArgs<T> a, int smem) {
-    auto kern = k_step<T, V, Desc, FLAGS>;
+    auto kern = k_step<T, V, Desc, FLAGS, UB, MB>;
+    if (t_refuse_spilling && spills((const void *)kern))
+        throw Error(PF_ERR_UNSUPPORTED, "step-kernel variant spills registers");
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     // one item per thread when the whole block fits on the device at once,
     // otherwise a persistent grid of every resident CTA
@@ -593,10 +608,33 @@ static void launch_one(pf_op *op, cudaStream_t st, const Desc &d, StepArgs<T> a,
     count_launches(1);
 }
 
+// The tuned (gather batch, register cap) profiles apply to the filter's
+// steps (Q|P|X and Q|X); every other launch uses the defaults.
+template <typename T, int V, class Desc, int UB, int MB>
+static bool dispatch_profile(pf_op *op, cudaStream_t st, const Desc &d, const StepArgs<T> &a, int flags, int smem) {
+    using F = StepFlags;
+    if (flags == (F::Q | F::P | F::X)) launch_one<T, V, Desc, F::Q | F::P | F::X, UB, MB>(op, st, d, a, smem);
+    else if (flags == (F::Q | F::X)) launch_one<T, V, Desc, F::Q | F::X, UB, MB>(op, st, d, a, smem);
+    else return false;
+    return true;
+}
+
 template <typename T, int V, class Desc>
 static void dispatch_flags(pf_op *op, cudaStream_t st, const Desc &d, const StepArgs<T> &a,
-                           int flags, int smem) {
+                           int flags, int smem, int profile) {
     using F = StepFlags;
+    if (profile != 0) {
+        // gather batch U = 4 or 8 at 2, 3 or 4 resident CTAs per SM
+        bool done = false;
+        switch (profile) {
+            case 1: done = dispatch_profile<T, V, Desc, 8, 2>(op, st, d, a, flags, smem); break;
+            case 2: done = dispatch_profile<T, V, Desc, 8, 3>(op, st, d, a, flags, smem); break;
+            case 3: done = dispatch_profile<T, V, Desc, 4, 4>(op, st, d, a, flags, smem); break;
+            case 4: done = dispatch_profile<T, V, Desc, 8, 4>(op, st, d, a, flags, smem); break;
+            default: throw Error(PF_ERR_INVALID, "unknown step-kernel profile");
+        }
+        if (done) return;
+    }
     switch (flags) {
         case F::X: launch_one<T, V, Desc, F::X>(op, st, d, a, smem); break;
         case F::Q: launch_one<T, V, Desc, F::Q>(op, st, d, a, smem); break;
@@ -631,8 +669,89 @@ const CsrDesc<double> &csr_of<double>(pf_op *op) { return op->csr64; }
 template <>
 const CsrDesc<float> &csr_of<float>(pf_op *op) { return op->csr32; }
 
+// Shared memory of the asynchronous-gather step: the model tables plus
+// (L_loc + dg) segments of V columns per thread.
+template <typename T>
+static int qsun_async_smem(const QSunDesc<T> &d, int V) {
+    return qsun_async_slot_offset<T>() + (d.L_loc + d.dg) * V * (int)sizeof(T) * kThreads;
+}
+
+bool qsun_async_eligible(const pf_op *op, int s, int V, int elem) {
+    if (op->kind != OP_QSUN || s % V != 0) return false;
+    const int seg = V * elem;
+    if (seg != 16 && seg != 32) return false;
+    const int smem = elem == 8 ? qsun_async_smem(op->qsun64, V) : qsun_async_smem(op->qsun32, V);
+    return smem <= 227 * 1024;
+}
+
+template <typename T, int V, int FLAGS>
+static void launch_qsun_async_one(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a) {
+    auto kern = k_step_qsun_async<T, V, FLAGS>;
+    const int smem = qsun_async_smem(d, V);
+    PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int grid = grid_for(op->h, a.items, kThreads, blocks_per_sm((const void *)kern, smem));
+    kern<<<grid, kThreads, smem, st>>>(d, a);
+    PF_CUDA(cudaGetLastError());
+    count_launches(1);
+}
+
+// The asynchronous-gather variant serves the filter's Q|P|X and Q|X steps of a
+// Quantum Sun operator with 16- or 32-byte column segments; false: not offered
+// (the caller launches the per-thread kernel instead).
 template <typename T, int V>
-static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int flags) {
+static bool launch_qsun_async(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a, int flags) {
+    using F = StepFlags;
+    constexpr int seg = V * (int)sizeof(T);
+    if constexpr (seg == 16 || seg == 32) {
+        if (qsun_async_smem(d, V) > 227 * 1024) return false;
+        if (flags == (F::Q | F::P | F::X)) launch_qsun_async_one<T, V, F::Q | F::P | F::X>(op, st, d, a);
+        else if (flags == (F::Q | F::X)) launch_qsun_async_one<T, V, F::Q | F::X>(op, st, d, a);
+        else return false;
+        return true;
+    } else {
+        (void)op, (void)st, (void)d, (void)a, (void)flags;
+        return false;
+    }
+}
+
+// Tile of the tiled QSun step: 2^t rows with t the largest value for which
+// the tile's segment (2^t x V columns) fits in 32 KB, at most L and at least
+// L_grain; 0 when the operator is too small for a tile of 256 rows.
+static int qsun_tile_bits(int L, int seg_bytes) {
+    int t = 0;
+    while (t < L && ((2 << t) * seg_bytes) <= 32 * 1024) ++t;
+    return t >= 8 ? t : 0;
+}
+
+bool qsun_tile_eligible(const pf_op *op, int s, int V, int elem) {
+    return op->kind == OP_QSUN && s % V == 0 && V * elem <= 64 && qsun_tile_bits(op->L, V * elem) > 0;
+}
+
+template <typename T, int V, int FLAGS>
+static void launch_qsun_tile_one(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a, int tbits) {
+    auto kern = k_step_qsun_tile<T, V, FLAGS>;
+    const int smem = qsun_tile_offset<T>() + (1 << tbits) * V * (int)sizeof(T);
+    if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int64_t ntiles = ((int64_t)a.D >> tbits) * a.G;
+    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)op->h->num_sms * blocks_per_sm((const void *)kern, smem));
+    kern<<<grid, kThreads, smem, st>>>(d, a, tbits);
+    PF_CUDA(cudaGetLastError());
+    count_launches(1);
+}
+
+template <typename T, int V>
+static bool launch_qsun_tile(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a, int flags) {
+    using F = StepFlags;
+    const int tbits = qsun_tile_bits(d.L, V * (int)sizeof(T));
+    if (tbits == 0) return false;
+    if (flags == (F::Q | F::P | F::X)) launch_qsun_tile_one<T, V, F::Q | F::P | F::X>(op, st, d, a, tbits);
+    else if (flags == (F::Q | F::X)) launch_qsun_tile_one<T, V, F::Q | F::X>(op, st, d, a, tbits);
+    else return false;
+    return true;
+}
+
+template <typename T, int V>
+static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int flags, int profile) {
     int smem = 0;
     const int lanes = a.G < 32 ? a.G : 32;
     const int dots_smem = (kThreads / 32) * lanes * 2 * V * 8 + 2 * a.s * 8;
@@ -640,16 +759,18 @@ static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int fl
         const ChainDesc<T> &d = chain_of<T>(op);
         if ((flags & StepFlags::Q) && !d.full) smem = rank_table_entries(d.nchunks) * 4;
         if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
-        dispatch_flags<T, V>(op, st, d, a, flags, smem);
+        dispatch_flags<T, V>(op, st, d, a, flags, smem, profile >= kProfileAsync ? 0 : profile);
     } else if (op->kind == OP_QSUN) {
         const QSunDesc<T> &d = qsun_of<T>(op);
+        if (profile == kProfileAsync && launch_qsun_async<T, V>(op, st, d, a, flags)) return;
+        if (profile == kProfileTile && launch_qsun_tile<T, V>(op, st, d, a, flags)) return;
         smem = QSunSmem<T>::bytes(d.dg);
         if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
-        dispatch_flags<T, V>(op, st, d, a, flags, smem);
+        dispatch_flags<T, V>(op, st, d, a, flags, smem, profile >= kProfileAsync ? 0 : profile);
     } else {
         const CsrDesc<T> &d = csr_of<T>(op);
         if (flags & StepFlags::DOTS) smem = dots_smem;
-        dispatch_flags<T, V>(op, st, d, a, flags, smem);
+        dispatch_flags<T, V>(op, st, d, a, flags, smem, profile >= kProfileAsync ? 0 : profile);
     }
 }
 
@@ -725,7 +846,9 @@ int default_width(int s, int elem_bytes) {
 template <typename T>
 void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p, const T *x, T *out,
                        double cx, double alpha, double beta, double inva, double shift, int flags, double *dots,
-                       int V) {
+                       int code) {
+    const int V = variant_width(code), profile = variant_profile(code);
+    PF_CHECK(profile >= 0 && profile <= kStepProfiles, PF_ERR_INVALID, "unknown step-kernel profile");
     PF_CHECK(D == op->dim, PF_ERR_INVALID, "block height does not match the operator dimension");
     PF_CHECK(s >= 1, PF_ERR_INVALID, "block must have at least one column");
     const bool coop = (V == kCoopWidth);
@@ -750,12 +873,12 @@ void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q,
     if (flags & StepFlags::DOTS)
         PF_CHECK(kThreads % a.G == 0, PF_ERR_UNSUPPORTED, "fused dots need s/V to divide 256");
     switch (V) {
-        case 1: dispatch_op<T, 1>(op, st, a, flags); break;
-        case 2: dispatch_op<T, 2>(op, st, a, flags); break;
-        case 4: dispatch_op<T, 4>(op, st, a, flags); break;
-        case 8: dispatch_op<T, 8>(op, st, a, flags); break;
+        case 1: dispatch_op<T, 1>(op, st, a, flags, profile); break;
+        case 2: dispatch_op<T, 2>(op, st, a, flags, profile); break;
+        case 4: dispatch_op<T, 4>(op, st, a, flags, profile); break;
+        case 8: dispatch_op<T, 8>(op, st, a, flags, profile); break;
         case 16:
-            if constexpr (sizeof(T) == 4) { dispatch_op<T, 16>(op, st, a, flags); break; }
+            if constexpr (sizeof(T) == 4) { dispatch_op<T, 16>(op, st, a, flags, profile); break; }
             [[fallthrough]];
         default: throw Error(PF_ERR_INVALID, "bad vector width");
     }
@@ -777,6 +900,7 @@ void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const
         while (V > 1 && (V * (int)sizeof(T) > 32 || kThreads % (s / V) != 0)) V /= 2;
     }
     if (V == kCoopWidth && !coop_eligible(op, s, flags)) V = default_width(s, (int)sizeof(T));
+    if (variant_profile(V) != 0 && (flags & StepFlags::DOTS)) V = variant_width(V);
     launch_step_width<T>(op, st, D, s, q, p, x, out, cx, alpha, beta, inva, shift, flags, dots, V);
 }
 

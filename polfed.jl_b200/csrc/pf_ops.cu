@@ -134,6 +134,7 @@ pf_op *create_spin_chain(pf_handle *h, int L, int Lup, int nbonds, const int32_t
         fill_chain(op->chain64, op);
         fill_chain(op->chain32, op);
         build_chain_diag(op);
+        build_multi_tables(op);
         uint32_t *tst = op->d_states, *trk = op->d_rank_tab;
         double *tdg = op->d_diag64;
         float *tdf = op->d_diag32;
@@ -190,6 +191,12 @@ pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double
     op->grain.assign(grain, grain + dg * dg);
     fill_qsun(op->qsun64, op);
     fill_qsun(op->qsun32, op);
+    try {
+        build_multi_tables(op);
+    } catch (...) {
+        delete op;
+        throw;
+    }
     return op;
 }
 
@@ -245,6 +252,12 @@ pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, c
     }
     op->csr64 = {dptr, didx, dv64};
     op->csr32 = {dptr, didx, dv32};
+    try {
+        build_multi_tables(op);
+    } catch (...) {
+        delete op;
+        throw;
+    }
     return op;
 }
 
@@ -274,6 +287,9 @@ pf_op *bind_op(const pf_op *src, pf_handle *h) {
     op->d_diag64 = src->d_diag64;
     op->d_diag32 = src->d_diag32;
     op->tables_owner = src->tables_owner;
+    op->d_desc64 = src->d_desc64;
+    op->d_desc32 = src->d_desc32;
+    op->multi_owner = src->multi_owner;
     op->smem_bytes = src->smem_bytes;
     {
         std::lock_guard<std::mutex> lock(const_cast<pf_op *>(src)->tune_mu);

@@ -75,6 +75,8 @@ struct pf_pool {
     pf::Clock::time_point busy_since, t_created;
     bool stop = false;
     int waiters = 0;                    // threads blocked in fetch / solve_batch (destroy waits for them)
+    pf_engine *engine = nullptr;        // batches the Clenshaw steps of every solve in flight
+    bool batching = false;              // requests hand their filters to the engine
 };
 
 namespace pf {
@@ -169,6 +171,10 @@ static void pool_worker(pf_pool *pool, int w) {
         // small solves on the high-priority stream: their short launches are
         // dispatched ahead of queued launches of larger solves (same results)
         pf_handle *h = req->urgent ? pool->urgent[w] : pool->handles[w];
+        {
+            std::lock_guard<std::mutex> lock(pool->mu);
+            h->engine = pool->batching ? pool->engine : nullptr;
+        }
         int status = PF_OK;
         bool infeasible = false;
         std::string err;
@@ -248,6 +254,7 @@ pf_pool *pool_create(int device, int workers, double budget) {
             budget = std::max(0.0, 0.9 * ((double)fr - reserve));
         }
         pool->budget = budget;
+        pool->engine = engine_create(device);
         for (int w = 0; w < workers; ++w) pool->threads.emplace_back(pool_worker, pool, w);
     } catch (...) {
         {
@@ -258,6 +265,7 @@ pf_pool *pool_create(int device, int workers, double budget) {
         for (auto &t : pool->threads) t.join();
         for (auto h : pool->handles) pf_handle_destroy(h);
         for (auto h : pool->urgent) pf_handle_destroy(h);
+        engine_destroy(pool->engine);
         delete pool;
         throw;
     }
@@ -296,9 +304,16 @@ void pool_destroy(pf_pool *pool) {
         pool->cv_done.notify_all();
         pool->cv_done.wait(lock, [&] { return pool->waiters == 0; });
     }
+    engine_destroy(pool->engine);
     for (auto h : pool->handles) pf_handle_destroy(h);
     for (auto h : pool->urgent) pf_handle_destroy(h);
     delete pool;
+}
+
+void pool_set_batching(pf_pool *pool, int on) {
+    PF_CHECK(pool, PF_ERR_INVALID, "null pool");
+    std::lock_guard<std::mutex> lock(pool->mu);
+    pool->batching = on != 0;
 }
 
 void pool_set_admission(pf_pool *pool, int policy, double max_wait) {
@@ -485,6 +500,9 @@ void pool_stats(pf_pool *pool, pf_pool_stats *st) {
     st->completed = pool->completed;
     st->failed = pool->failed;
     st->rejected = pool->rejected;
+    if (pool->engine)
+        engine_stats(pool->engine, &st->filter_launches, &st->filter_seconds, &st->filter_bytes,
+                     &st->filter_instance_steps);
     st->queued = (int64_t)pool->queue.size();
     st->running = pool->running;
     st->eigenpairs = pool->eigenpairs;

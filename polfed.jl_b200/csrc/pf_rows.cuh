@@ -1,0 +1,300 @@
+// pf_rows.cuh -- per-row Hamiltonian evaluation shared by the step kernels.
+//
+// Each row function returns, for row `row` and columns c0..c0+V-1 of a
+// row-interleaved block q (element (i, c) at i*s + c), the off-diagonal
+// gather sum in acc[] and the row's diagonal element.  The matrix is never
+// stored: the spin-chain and Quantum Sun rows are derived from the operator
+// descriptor (SpinHalfChains.jl:267-315, QuantumSun.jl:1-102), a CSR row from
+// the user's matrix.
+#pragma once
+#include "pf_internal.h"
+
+namespace pf {
+
+template <typename T, int V>
+struct alignas(sizeof(T) * V) Pack {
+    T v[V];
+};
+
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> ldp(const T *p) {
+    return *reinterpret_cast<const Pack<T, V> *>(p);
+}
+template <typename T, int V>
+__device__ __forceinline__ void stp(T *p, const Pack<T, V> &v) {
+    *reinterpret_cast<Pack<T, V> *>(p) = v;
+}
+
+// ------------------------------------------------------------ sector rank
+__device__ __forceinline__ uint32_t sector_rank(uint32_t st, const uint32_t *tab, int nchunks) {
+    uint32_t r = 0;
+    int p = 0;
+    int off = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        if (c < nchunks) {
+            uint32_t byte = (st >> (8 * c)) & 0xffu;
+            r += tab[off + p * 256 + (int)byte];
+            p += __popc(byte);
+            off += (8 * c + 1) * 256;
+        }
+    }
+    return r;
+}
+
+// Explicitly rounded arithmetic.  Every step-kernel variant (any width,
+// gather batch or register cap; per-thread, warp-cooperative or
+// multi-instance) performs exactly these operations in the same order, so all
+// of them give bit-identical results whatever contractions the compiler would
+// otherwise choose per instantiation.
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double mul_t(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_t(float a, float b) { return __fmul_rn(a, b); }
+
+// One output element of a step: cx x + alpha ((acc + diag q) / a - (b/a) q) + beta p,
+// with the terms that are absent (has_x / has_q / has_p false) left out.
+template <typename T>
+__device__ __forceinline__ T step_combine(bool has_x, bool has_q, bool has_p, T cx, T x, T alpha, T acc, T diag,
+                                          T q, T inva, T boa, T beta, T p) {
+    T res = has_x ? mul_t(cx, x) : T(0);
+    if (has_q) {
+        const T hq = fma_t(-boa, q, mul_t(fma_t(diag, q, acc), inva));
+        res = fma_t(alpha, hq, res);
+    }
+    if (has_p) res = fma_t(beta, p, res);
+    return res;
+}
+
+// Pull a row's own operand segment toward L1 before its gathers are issued,
+// so the later load of it does not add a dependent L2 round trip (no register
+// is held meanwhile).
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// ------------------------------------------------------------ row models
+// Each returns (through acc / diag) the off-diagonal gather sum and the
+// diagonal element of row `row` for columns c0..c0+V-1.
+
+// Gathers are issued in unrolled batches of U independent loads so that each
+// thread keeps several L2/HBM requests in flight (the loop bodies have no
+// load-to-load dependence); accumulation follows the reference's term order.
+// U shrinks as the per-thread column count V grows, to bound registers; a
+// tuned variant may set it explicitly (template argument UB > 0).
+template <typename T, int V>
+struct Batch {
+    static constexpr int bytes = V * (int)sizeof(T);
+    static constexpr int U = bytes >= 64 ? 2 : (bytes >= 16 ? 4 : 8);
+};
+
+// Resident CTAs per SM the step kernel is compiled for: caps registers so
+// enough warps stay resident to cover L2 latency with independent gathers
+// (with no cap the 64-byte-per-thread variants took 170 registers, one CTA
+// per SM, 8 warps -- latency-bound).
+template <typename T, int V>
+struct MinBlocks {
+    static constexpr int bytes = V * (int)sizeof(T);
+    static constexpr int value = bytes >= 32 ? 2 : 3;
+};
+
+template <typename T, int V, bool HASQ, int UB = 0>
+__device__ __forceinline__ void chain_row(const ChainDesc<T> &d, const uint32_t *tab, uint32_t row,
+                                          int s, int c0, const T *__restrict__ q, T (&acc)[V],
+                                          T &diag) {
+    constexpr int U = UB > 0 ? UB : Batch<T, V>::U;
+    const uint32_t st = d.full ? row : __ldg(d.states + row);
+    T dg = T(0);
+    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
+    const T *qc = q + c0;
+    for (int b0 = 0; b0 < d.nb; b0 += U) {
+        uint32_t r2[U];
+        bool act[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int b = b0 + u;
+            act[u] = false;
+            r2[u] = 0u;
+            if (b < d.nb) {
+                const uint32_t bm = d.bmask[b];
+                const uint32_t m = st & bm;
+                const bool differ = (m != 0u) && (m != bm);
+                dg += differ ? -d.jdq[b] : d.jdq[b];
+                act[u] = differ;
+                if (HASQ && differ) {
+                    const uint32_t st2 = st ^ bm;
+                    r2[u] = d.full ? st2 : sector_rank(st2, tab, d.nchunks);
+                }
+            }
+        }
+        if constexpr (HASQ) {
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (act[u]) g[u] = ldp<T, V>(qc + (size_t)r2[u] * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (act[u]) {
+                    const T jh = d.jhalf[b0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(jh, g[u].v[v], acc[v]);
+                }
+        }
+    }
+    diag = dg;
+}
+
+// Quantum Sun shared-memory layout: the grain block with a padded row stride
+// (dg + 1, so the 8 rows of one grain group read different banks), then four
+// 256-entry diagonal tables, one per byte of the outer-spin bits.
+template <typename T>
+struct QSunSmem {
+    static __host__ __device__ int grain_stride(int dg) { return dg + 1; }
+    static __host__ __device__ int bytes(int dg) { return (dg * (dg + 1) + 4 * 256) * (int)sizeof(T); }
+};
+
+template <typename T, int V, bool HASQ, int UB = 0>
+__device__ __forceinline__ void qsun_row(const QSunDesc<T> &d, const T *smem_t, uint32_t row,
+                                         int s, int c0, const T *__restrict__ q, T (&acc)[V],
+                                         T &diag) {
+    constexpr int U = UB > 0 ? UB : Batch<T, V>::U;
+    const int gs = d.dg + 1;
+    const T *dtab = smem_t + d.dg * gs;
+    const uint32_t outer = row >> d.L_grain;
+    T dg = dtab[outer & 0xffu];
+    if (d.L_loc > 8) dg += dtab[256 + ((outer >> 8) & 0xffu)];
+    if (d.L_loc > 16) dg += dtab[512 + ((outer >> 16) & 0xffu)];
+    if (d.L_loc > 24) dg += dtab[768 + ((outer >> 24) & 0xffu)];
+    diag = dg;
+    if constexpr (HASQ) {
+        const T *qc = q + c0;
+        for (int j0 = 0; j0 < d.L_loc; j0 += U) {
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j0 + u < d.L_loc) g[u] = ldp<T, V>(qc + (size_t)(row ^ d.fmask[j0 + u]) * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j0 + u < d.L_loc) {
+                    const T cf = d.cflip[j0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(cf, g[u].v[v], acc[v]);
+                }
+        }
+        const uint32_t g = row & ((uint32_t)d.dg - 1u);
+        const uint32_t base = row - g;
+        const T *grow = smem_t + g * gs;
+        for (int h0 = 0; h0 < d.dg; h0 += U) {
+            Pack<T, V> x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (h0 + u < d.dg) x[u] = ldp<T, V>(qc + (size_t)(base + h0 + u) * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (h0 + u < d.dg) {
+                    const T w = grow[h0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(w, x[u].v[v], acc[v]);
+                }
+        }
+    }
+}
+
+// CSR row (a user matrix): the entries of the row in storage order, gathered
+// in unrolled batches of U like the matrix-free rows; the diagonal is an
+// ordinary entry, so diag = 0.
+template <typename T, int V, bool HASQ, int UB = 0>
+__device__ __forceinline__ void csr_row(const CsrDesc<T> &d, uint32_t row, int s, int c0, const T *__restrict__ q,
+                                        T (&acc)[V], T &diag) {
+    diag = T(0);
+    if constexpr (HASQ) {
+        constexpr int U = UB > 0 ? UB : Batch<T, V>::U;
+        const int64_t b = __ldg(d.indptr + row), e = __ldg(d.indptr + row + 1);
+        const T *qc = q + c0;
+        for (int64_t p0 = b; p0 < e; p0 += U) {
+            int32_t col[U];
+            T val[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (p0 + u < e) {
+                    col[u] = __ldg(d.indices + p0 + u);
+                    val[u] = __ldg(d.values + p0 + u);
+                }
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (p0 + u < e) g[u] = ldp<T, V>(qc + (size_t)col[u] * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (p0 + u < e) {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(val[u], g[u].v[v], acc[v]);
+                }
+        }
+    }
+}
+
+
+// Quantum Sun row with the grain block read from the descriptor (global
+// memory, L1-resident) and the diagonal from a per-row array built by
+// k_qsun_diag: the same values and the same order of additions as qsun_row,
+// so both produce identical results.  Used where one launch serves several
+// operators and per-operator shared-memory tables cannot be staged.
+template <typename T, int V, bool HASQ, int UB = 0>
+__device__ __forceinline__ void qsun_row_g(const QSunDesc<T> &d, const T *__restrict__ dvec, uint32_t row, int s,
+                                           int c0, const T *__restrict__ q, T (&acc)[V], T &diag) {
+    constexpr int U = UB > 0 ? UB : Batch<T, V>::U;
+    diag = dvec[row];
+    if constexpr (HASQ) {
+        const T *qc = q + c0;
+        for (int j0 = 0; j0 < d.L_loc; j0 += U) {
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j0 + u < d.L_loc) g[u] = ldp<T, V>(qc + (size_t)(row ^ d.fmask[j0 + u]) * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (j0 + u < d.L_loc) {
+                    const T cf = d.cflip[j0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(cf, g[u].v[v], acc[v]);
+                }
+        }
+        const uint32_t g = row & ((uint32_t)d.dg - 1u);
+        const uint32_t base = row - g;
+        const T *grow = d.grain + g * d.dg;
+        for (int h0 = 0; h0 < d.dg; h0 += U) {
+            Pack<T, V> x[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (h0 + u < d.dg) x[u] = ldp<T, V>(qc + (size_t)(base + h0 + u) * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (h0 + u < d.dg) {
+                    const T w = grow[h0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(w, x[u].v[v], acc[v]);
+                }
+        }
+    }
+}
+
+// Diagonal of a Quantum Sun row, summed exactly as qsun_row sums it: per byte
+// of the outer-spin bits the sum over its 8 spins of +-h_j/2 in spin order,
+// then the byte sums in byte order.
+template <typename T>
+__device__ __forceinline__ T qsun_diag(const QSunDesc<T> &d, uint32_t row) {
+    const uint32_t outer = row >> d.L_grain;
+    T dg = T(0);
+    for (int c = 0; c < 4; ++c) {
+        if (c > 0 && d.L_loc <= 8 * c) break;
+        const uint32_t byte = (outer >> (8 * c)) & 0xffu;
+        T acc = T(0);
+        for (int t = 0; t < 8; ++t) {
+            const int j = 8 * c + t;
+            if (j < d.L_loc) acc += ((byte >> t) & 1u) ? d.hhalf[j] : -d.hhalf[j];
+        }
+        dg = (c == 0) ? acc : dg + acc;
+    }
+    return dg;
+}
+
+}  // namespace pf

@@ -102,11 +102,15 @@ struct Filter {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 
-    Filter(pf_op *op_, int s_, const std::vector<double> &coeffs, double a_, double b_)
+    // io = false: only the two work blocks (the filter engine reads and
+    // writes the caller's blocks directly)
+    Filter(pf_op *op_, int s_, const std::vector<double> &coeffs, double a_, double b_, bool io = true)
         : op(op_), s(s_), K((int)coeffs.size() - 1), c(coeffs), a(a_), b(b_) {
         const size_t n = (size_t)op->dim * s;
-        X.alloc(n);
-        Y.alloc(n);
+        if (io) {
+            X.alloc(n);
+            Y.alloc(n);
+        }
         if (K >= 1) A.alloc(n);
         if (K >= 2) B.alloc(n);
     }
@@ -749,6 +753,16 @@ void op_kpm(pf_op *op, int dtype, double a, double b, int N, int R, const void *
 }
 
 // ------------------------------------------------------------- the solve
+// Columns per thread of the engine's multi-instance step: the operator's tuned
+// per-thread width (the warp-cooperative variant has no multi-instance form).
+static int engine_width(pf_op *op, int s, int elem) {
+    int V = default_width(s, elem);
+    std::lock_guard<std::mutex> lock(op->tune_mu);
+    auto it = op->tuned_width.find(std::make_pair(elem, s));
+    if (it != op->tuned_width.end() && it->second != kCoopWidth) V = variant_width(it->second);
+    return V;
+}
+
 static int64_t expected_krylov_dim(int howmany, int s, double eta) {
     return (int64_t)std::ceil((20.427 * s + 1.696 * howmany) * eta);  // PolfedDefaults.jl:61-62
 }
@@ -911,11 +925,20 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
             std::lock_guard<std::mutex> lock(op->tune_mu);
             have = op->tuned_width.count(std::make_pair(fdtype == PF_F64 ? 8 : 4, s)) > 0;
         }
-        if (!have) autotune_step(op, s, fdtype, nullptr);
+        if (!have && !cached_step_variant(op, s, fdtype)) autotune_step(op, s, fdtype, nullptr);
     }
+    // A handle working for a request pool hands its filters to the pool's
+    // engine, which batches the Clenshaw steps of every solve in flight into
+    // shared launches; otherwise the filter is this solve's own CUDA graph.
+    pf_engine *eng = (h->engine && multi_eligible(op, fdtype)) ? h->engine : nullptr;
+    const int ew = engine_width(op, s, fdtype == PF_F64 ? 8 : 4);
     if (P->precision == PF_PREC_FP64) {
-        Filter<double> filt(op, s, coeffs, a, b);
+        Filter<double> filt(op, s, coeffs, a, b, eng == nullptr);
         BlockMap fmap = [&](const double *X, double *Y) {
+            if (eng) {
+                engine_filter(eng, op, st, 8, s, ew, coeffs, a, b, (void *)X, Y, filt.A.p, filt.B.p);
+                return;
+            }
             PF_CUDA(cudaMemcpyAsync(filt.X.p, X, (size_t)D * s * sizeof(double), cudaMemcpyDeviceToDevice, st));
             filt.run(st);
             PF_CUDA(cudaMemcpyAsync(Y, filt.Y.p, (size_t)D * s * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -925,7 +948,8 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
         Filter<float> filt(op, s, coeffs, a, b);
         BlockMap fmap = [&](const double *X, double *Y) {
             launch_ri_to_cm<double, float>(st, (int64_t)D * s, 1, X, filt.X.p, (int64_t)D * s);
-            filt.run(st);
+            if (eng) engine_filter(eng, op, st, 4, s, ew, coeffs, a, b, filt.X.p, filt.Y.p, filt.A.p, filt.B.p);
+            else filt.run(st);
             launch_ri_to_cm<float, double>(st, (int64_t)D * s, 1, filt.Y.p, Y, (int64_t)D * s);
         };
         lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage);

@@ -36,11 +36,21 @@ void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, d
 
 extern thread_local int t_new_handle_priority;
 
+// filter engine (pf_engine.cu): one step launch for every filter in flight
+void build_multi_tables(pf_op *op);
+bool multi_eligible(const pf_op *op, int dtype);
+pf_engine *engine_create(int device);
+void engine_destroy(pf_engine *eng);
+void engine_stats(pf_engine *eng, double *launches, double *seconds, double *bytes, double *instance_steps);
+void engine_filter(pf_engine *eng, pf_op *op, cudaStream_t st, int elem, int s, int V,
+                   const std::vector<double> &coeffs, double a, double b, void *X, void *Y, void *A, void *B);
+
 // request pool (pf_pool.cpp)
 double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev);
 pf_pool *pool_create(int device, int workers, double budget);
 void pool_destroy(pf_pool *pool);
 void pool_shutdown(pf_pool *pool);
+void pool_set_batching(pf_pool *pool, int on);
 cudaStream_t pool_stream(pf_pool *pool, int worker);
 void pool_set_priority_dim(pf_pool *pool, int64_t dim);
 void pool_set_admission(pf_pool *pool, int policy, double max_wait);

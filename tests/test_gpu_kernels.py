@@ -302,3 +302,40 @@ def test_operator_errors(pkg, cuda):
         pkg.SpinChainOperator(33, -1, [], [], [], [0.0] * 33).op
     with pytest.raises(_lib.PolfedError):
         pkg.QSunOperator(4, 2, 1.0, [1.0] * 4, [0, 1, 2, 0], [1.0] * 4, np.eye(4)).op
+
+
+@pytest.mark.parametrize("dts", ["fp64", "fp32"])
+def test_every_step_variant_gives_identical_results(pkg, orc, cuda, models, dts):
+    """The autotuner picks among columns-per-thread widths and (gather batch,
+    register cap) profiles; all of them compute the same sums in the same
+    order, so a K = 24 filter is bit-identical across variants."""
+    dt = cuda.float64 if dts == "fp64" else cuda.float32
+    elem = 8 if dts == "fp64" else 4
+    s = 8
+    rng = np.random.default_rng(9)
+    plan = orc.build_transform_plan(("rescaled", 0.2), 10, 1.0, 0.0, order=24)
+    coeffs = orc.filter_coefficients(plan)
+    for name, op, H in models:
+        D = H.shape[0]
+        X = _dev(cuda, rng.standard_normal((D, s)), dt)
+        Emax = float(np.abs(H).sum(axis=1).max())
+        ref = None
+        for width in (1, 2, 4, 8):
+            if width * elem > 64:
+                continue
+            profiles = list(range(5))
+            if op.kind == "qsun" and width * elem in (16, 32):
+                profiles.append(5)                # asynchronous gathers
+            if op.kind == "qsun" and op.dim >= 256:
+                profiles.append(6)                # shared-memory row tiles
+            for profile in profiles:
+                pkg.set_step_width(op, s, width, dts, profile=profile)
+                assert pkg.step_variant(op, s, dts)[0] == width
+                Y = pkg.col_major(D, s, dtype=dt)
+                pkg.chebyshev_filter(op, Y, X, coeffs, a=1.01 * Emax, b=0.0)
+                got = _host(Y)
+                if ref is None:
+                    ref = got
+                else:
+                    np.testing.assert_array_equal(got, ref, err_msg=f"{name} width={width} profile={profile}")
+        pkg.set_step_width(op, s, min(8, 64 // elem), dts)

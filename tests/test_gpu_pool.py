@@ -224,3 +224,37 @@ def test_destroy_wakes_waiting_threads(pkg, orc, cuda):
     t.join(timeout=120)
     assert not t.is_alive()
     assert "pool destroyed" in outcome["r"] or "pool is closed" in outcome["r"], outcome
+
+
+def test_batched_filter_matches_unbatched_uneven_dims(pkg, orc, cuda):
+    """The filter engine runs the Clenshaw steps of every solve in flight as
+    one launch per step.  Chain operators of different dimensions (XXZ L = 12,
+    13, 14 and a J1-J2 L = 12 chain) and two Quantum Sun operators, all with
+    s = 4, solved together with batching on, give the eigenpairs each gives
+    alone on its own graph-captured filter, and the launches are shared."""
+    rng = np.random.default_rng(31)
+    probs = []
+    for L in (12, 13, 14):
+        f = 4 * (2 * rng.random(L) - 1)
+        probs.append((pkg.xxz_hamiltonian(L, L // 2, 1.0, 1.0, 0.0, fields=f), orc.xxz_matrix(L, L // 2, 1.0, 1.0, f)))
+    f = 3 * (2 * rng.random(12) - 1)
+    probs.append((pkg.j1j2_hamiltonian(12, 6, 1.0, 0.5, 1.0, 0.8, 0.0, fields=f),
+                  orc.j1j2_matrix(12, 6, 1.0, 0.5, 1.0, 0.8, f)))
+    for Lloc in (7, 8):
+        fq, nq, cq, gq = pkg.qsun_parameters(Lloc, 3, 0.75, rng=rng)
+        probs.append((pkg.QSunOperator(Lloc, 3, 1.0, cq, nq, fq, gq), orc.qsun_matrix(Lloc, 3, 1.0, cq, nq, fq, gq)))
+    x0s = [rng.random((H.shape[0], 4)) for _, H in probs]
+    for op, _ in probs:
+        pkg.autotune(op, 4, "fp64")
+    alone = [pkg.polfed(op, x0, NEV, TARGET, **_kw(pkg, 40)) for (op, _), x0 in zip(probs, x0s)]
+    with pkg.SolverPool(workers=len(probs)) as pool:
+        pool.set_batching(True)
+        res = pool.solve_batch([op for op, _ in probs], x0s, NEV, TARGET, **_kw(pkg, 40))
+        st = pool.stats()
+    for (op, H), (va, _), (vb, Vb) in zip(probs, alone, res):
+        assert len(va) == len(vb) and len(vb) >= 1
+        assert np.max(np.abs(va - vb) / np.maximum(1, np.abs(va))) < 1e-12
+        _residuals_ok(H, vb, Vb)
+    assert st.filter_launches > 0
+    assert st.filter_instance_steps > 1.2 * st.filter_launches   # launches served several solves
+    assert st.filter_bytes > 0 and st.filter_seconds > 0
