@@ -20,8 +20,8 @@ eigenpair counts iff its FP64 residual ||H psi - E psi|| <= 1e-10 (eigentol).
 * ``roofline`` -- the dominant kernel (the Clenshaw recurrence step):
   algorithmic bytes per launch 4*D*s*8 (read b_{k+1}, b_{k+2}, X; write b_k)
   over its average duration inside the timed solves (CUDA events in the library).
-* ``cpu_baseline`` -- the CPU port of the reference algorithm (oracle/) on this
-  host's cores over a bounded sample, scaled to eigenpairs/s.
+* ``cpu_baseline`` -- one complete solve with the CPU port of the reference
+  algorithm (oracle/) on this host's cores, measured.
 
 N > 1 (torchrun): every rank solves its own realisations (replicas, no data
 path collective); ``scaling`` is weak.
@@ -180,84 +180,82 @@ def read_traffic():
 
 
 # ------------------------------------------------------- CPU baseline
-def cpu_sample(seed=4242, kpm_probes=4, verbose=False):
-    """Time the CPU port of the reference algorithm (oracle/) on a bounded
-    sample of one solve of the workload and scale it to eigenpairs/s.
-
-    Sample: the two Emin/Emax Lanczos probes in full, KPM on ``kpm_probes``
-    probes (scaled by R / kpm_probes), one Chebyshev filter application of
-    the resolved order K to an s=8 block and one full reorthogonalisation
-    against a half-full basis (both scaled by the iteration budget)."""
+def _cpu_realisation(seed, L_loc=None):
+    """One seeded realisation of the workload for the CPU port: the FP64 CSR
+    matrix (the operator of the reference's default CPU path, polfed(mat, ...)
+    with optimize_mapping = false: mul!(Y, mat, X), PolfedCore.jl:172), x0 and
+    the KPM probes."""
     import numpy as np
     from oracle import oracle as orc
     import __graft_entry__ as ge
     pkg = ge.load_package()
+    L_loc = WORKLOAD["L_loc"] if L_loc is None else L_loc
     rng = np.random.default_rng(seed)
-    f, n, c, g = pkg.qsun_parameters(WORKLOAD["L_loc"], WORKLOAD["L_grain"], WORKLOAD["alpha"],
-                                     gamma=WORKLOAD["gamma"], w=WORKLOAD["w"], hz=WORKLOAD["hz"],
-                                     zeta=WORKLOAD["zeta"], rng=rng)
-    H = orc.qsun_matrix(WORKLOAD["L_loc"], WORKLOAD["L_grain"], WORKLOAD["g0"], c, n, f, g)
-    op = orc.CSROperator(H)
-    D, s, nev = op.D, WORKLOAD["blocksize"], WORKLOAD["nev"]
-    x0, _ = np.linalg.qr(rng.standard_normal((D, s)))
+    f, n, c, g = pkg.qsun_parameters(L_loc, WORKLOAD["L_grain"], WORKLOAD["alpha"], gamma=WORKLOAD["gamma"],
+                                     w=WORKLOAD["w"], hz=WORKLOAD["hz"], zeta=WORKLOAD["zeta"], rng=rng)
+    H = orc.qsun_matrix(L_loc, WORKLOAD["L_grain"], WORKLOAD["g0"], c, n, f, g)
+    D = H.shape[0]
+    x0, _ = np.linalg.qr(rng.standard_normal((D, WORKLOAD["blocksize"])))
+    probes = orc.normalized_gaussian_probes(D, WORKLOAD["dos_R"], rng)
+    return orc.CSROperator(H), x0, probes
+
+
+def cpu_solve(seed, L_loc=None, nev=None):
+    """One complete POLFED solve of a fresh realisation on the host cores with
+    the CPU port of the reference path (oracle/: C/OpenMP CSR kernels for the
+    operator, Clenshaw filter and threaded KPM, numpy/OpenBLAS for Lanczos and
+    the projected eigenproblem).  Returns (converged pairs at FP64 residual
+    <= 1e-10, seconds)."""
+    from oracle import oracle as orc
+    op, x0, probes = _cpu_realisation(seed, L_loc)
     t0 = time.perf_counter()
-    Emin, Emax = orc.lanczos_extrema(op.apply, x0[:, 0])
-    t_ext = time.perf_counter() - t0
-    a, b = (Emax - Emin) / 2, (Emax + Emin) / 2
-    probes = orc.normalized_gaussian_probes(D, kpm_probes, rng)
-    t0 = time.perf_counter()
-    mu = orc.dos_moments(op, a, b, WORKLOAD["dos_N"], probes)
-    t_kpm = (time.perf_counter() - t0) * WORKLOAD["dos_R"] / kpm_probes
-    rho = orc.make_rho(mu, WORKLOAD["dos_N"])
-    plan = orc.build_transform_plan(("rescaled", 0.5), nev, a, b)
-    orc.getbounds(plan, a, b, rho)
-    orc.getorderofexpansion(plan)
-    coeffs = orc.filter_coefficients(plan)
-    iters = math.ceil(orc.expectedkrylovdim(nev, s, 1.25) / s)
-    X = np.asfortranarray(x0)
-    t0 = time.perf_counter()
-    Y = op.filter(X, a, b, coeffs)
-    t_filter = time.perf_counter() - t0
-    B = np.asfortranarray(rng.standard_normal((D, (iters // 2) * s)))
-    t0 = time.perf_counter()
-    Y = Y - B @ (B.T @ Y)
-    t_reorth = time.perf_counter() - t0
-    T = t_ext + t_kpm + iters * (t_filter + t_reorth)
-    threads = orc.lib().orc_num_threads()
-    if verbose:
-        print(f"cpu sample: extrema {t_ext:.2f}s kpm(est) {t_kpm:.2f}s filter {t_filter:.3f}s x {iters} "
-              f"reorth {t_reorth:.3f}s -> {T:.1f}s per solve, K={plan.order}", file=sys.stderr)
-    return {
-        "value": nev / T, "unit": "eigenpairs/s", "cores": threads, "kind": "port",
-        "sample": (f"CPU port of the reference path (oracle: C/OpenMP CSR kernels + numpy) on one realisation: "
-                   f"2 Emin/Emax Lanczos probes timed in full ({t_ext:.2f}s), KPM on {kpm_probes} of "
-                   f"{WORKLOAD['dos_R']} probes scaled x{WORKLOAD['dos_R'] / kpm_probes:.0f} ({t_kpm:.2f}s), one "
-                   f"K={plan.order} filter on s={s} ({t_filter:.3f}s) and one reorthogonalisation "
-                   f"({t_reorth:.3f}s) scaled x{iters} iterations; {nev} pairs per estimated {T:.1f}s solve"),
-        "seconds_per_solve": T,
-    }
+    res = orc.polfed(op, x0, WORKLOAD["nev"] if nev is None else nev, ("rescaled", 0.5), N=WORKLOAD["dos_N"],
+                     R=WORKLOAD["dos_R"], probes=probes, eigentol=WORKLOAD["eigentol"])
+    return len(res.vals), time.perf_counter() - t0
+
+
+def cpu_baseline_sample(seed=4242):
+    """The cpu_baseline of our arm: one complete CPU solve of the workload,
+    measured (not extrapolated)."""
+    from oracle import oracle as orc
+    n, sec = cpu_solve(seed)
+    return {"value": n / sec, "unit": "eigenpairs/s", "cores": int(orc.lib().orc_num_threads()), "kind": "port",
+            "sample": (f"one complete solve of a fresh realisation of the workload (D=65536, s=8, nev=200) with the "
+                       f"CPU port of the reference's default path (CSR mul!, Clenshaw filter, threaded KPM with "
+                       f"R=300 probes, FP64 block Lanczos): {n} pairs at residual <= 1e-10 in {sec:.1f} s")}
 
 
 def run_reference(args, rank, world):
-    """The reference arm: the CPU implementation of the path on this host."""
+    """The reference arm: complete CPU solves with the CPU port of the
+    reference's path on this host's cores, one fresh realisation per step.
+    Warm-up steps solve a small realisation of the same model (L_loc = 7,
+    nev = 20), which loads the kernels and starts the thread pools without the
+    cost of a full solve."""
     if rank != 0:
         return 0
-    vals, per = [], None
-    for i in range(args.warmup + args.steps):
-        per = cpu_sample(seed=4242 + i)
-        if i >= args.warmup:
-            vals.append(per["value"])
-    v = statistics.median(vals)
-    cb = dict(per)
-    cb["value"] = v
-    cb.pop("seconds_per_solve", None)
+    from oracle import oracle as orc
+    for i in range(args.warmup):
+        cpu_solve(4000 + i, L_loc=7, nev=20)
+    pairs, secs = [], []
+    for k in range(args.steps):
+        n, sec = cpu_solve(4242 + k)
+        pairs.append(n)
+        secs.append(sec)
+    v = sum(pairs) / sum(secs)
+    cores = int(orc.lib().orc_num_threads())
+    cb = {"value": v, "unit": "eigenpairs/s", "cores": cores, "kind": "port",
+          "sample": (f"{args.steps} complete solves of fresh realisations (D=65536, s=8, nev=200) with the CPU "
+                     f"port of the reference's default path (CSR mul!, Clenshaw filter, threaded KPM, FP64 block "
+                     f"Lanczos); {sum(pairs)} pairs at residual <= 1e-10 in {sum(secs):.1f} s")}
     out = {
         "metric": "converged eigenpairs/s at resid<=1e-10", "value": v, "unit": "eigenpairs/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * WORKLOAD["nev"] / v, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded realisations)",
-        "config": dict(WORKLOAD), "impl": "reference", "cpu_baseline": cb,
+        "config": dict(WORKLOAD, step="one complete CPU solve of a fresh realisation"),
+        "impl": "reference", "cpu_baseline": cb,
         "e2e": {"value": v, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "converged_per_solve": sum(pairs) / len(pairs),
     }
     print(json.dumps(out))
     return 0
@@ -378,14 +376,21 @@ def run_ours(args, rank, world, local_rank):
     alg_bytes = 4.0 * D * s * 8
     achieved = alg_bytes / avg_step / 1e9
     peak, peak_kind = read_peaks()
+    # KPM: ceil((N-1)/2) doubling steps per probe column block, 3 D R_b 8 bytes each
+    # (read v_n, read v_{n-1}, write v_{n+1}); all R probes pass through every step
+    kpm_steps = (WORKLOAD["dos_N"] - 1 + 1) // 2
+    kpm_bytes = 3.0 * D * WORKLOAD["dos_R"] * 8 * kpm_steps
+    kpm_sec = statistics.mean(r.benchmark.stage_seconds["dos"] for r in reps)
+    # the measured ceiling of an L2-resident step: random 64-byte row gathers
+    gather_peak = _lib.gather_peak(local_rank, int(round(math.log2(D)))) / 1e9
+    flip_bytes = float(D) * WORKLOAD["L_loc"] * s * 8   # the flipped rows a step gathers
     launches = sum(r.benchmark.kernel_launches for r in breps)
     stages = {k: sum(r.benchmark.stage_seconds[k] for r in reps) / len(reps) for k in reps[0].benchmark.stage_seconds}
     if rank != 0:
         return 0
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample()
-        cpu.pop("seconds_per_solve", None)
+        cpu = cpu_baseline_sample()
     out = {
         "metric": "converged eigenpairs/s at resid<=1e-10", "value": value, "unit": "eigenpairs/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -405,7 +410,17 @@ def run_ours(args, rank, world, local_rank):
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": read_traffic(), "algorithmic_bytes_per_launch": alg_bytes,
                      "avg_launch_us": avg_step * 1e6,
-                     "measured_in": "the single-solve runs (library CUDA-event stage timers)"},
+                     "measured_in": "the single-solve runs (library CUDA-event stage timers)",
+                     "l2_gather": {"peak_gbs": gather_peak, "achieved_gbs": flip_bytes / avg_step / 1e9,
+                                   "frac": flip_bytes / avg_step / 1e9 / gather_peak,
+                                   "note": "the step's blocks stay in L2 (3 x 4 MB); its L_loc flipped-row "
+                                           "gathers (64 B each) against the measured random-row gather "
+                                           "throughput of an L2-resident block (pf_gather_peak)"},
+                     "kpm": {"kernel": "k_step (KPM doubling step, fused dots)",
+                             "algorithmic_bytes_per_solve": kpm_bytes,
+                             "achieved": kpm_bytes / kpm_sec / 1e9, "frac": kpm_bytes / kpm_sec / 1e9 / peak,
+                             "seconds_per_solve": kpm_sec,
+                             "measured_in": "the single-solve runs (library stage timer 'dos')"}},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "e2e_clocks": e_clocks,

@@ -183,6 +183,12 @@ int pf_kpm_moments(pf_op *op, int dtype, double a, double b, int N, int R,
  * that pf_solve consults before timing. */
 #define PF_WIDTH_COOP 0
 int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms);
+/* Roofline probe (no reference counterpart): the measured throughput, in
+ * bytes per second, of random row gathers -- each thread reads 32 bytes of 16
+ * rows chosen by a row-XOR pattern, as spin flips do -- from an L2-resident
+ * block of 2^log2_rows 64-byte rows (10 <= log2_rows <= 24).  The ceiling of
+ * a step kernel whose blocks stay in L2. */
+int pf_gather_peak(pf_handle *h, int log2_rows, double *bytes_per_s);
 /* The step-kernel variant in use for (dtype, s): columns per thread (0: the
  * warp-cooperative step), gathers issued per batch and the resident CTAs per
  * SM it is compiled for (its register cap). */

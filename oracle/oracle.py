@@ -72,6 +72,12 @@ def lib():
     L.orc_clenshaw_filter.argtypes = [i64, vp, vp, vp, f64, f64, i32, vp, i32, vp, vp, vp]
     L.orc_kpm_trace.restype = None
     L.orc_kpm_trace.argtypes = [i64, vp, vp, vp, f64, f64, i32, i32, vp, vp]
+    L.orc_bucket_apply.restype = None
+    L.orc_bucket_apply.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, vp, vp]
+    L.orc_bucket_filter.restype = None
+    L.orc_bucket_filter.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, vp, i32, vp, vp, vp]
+    L.orc_bucket_kpm_trace.restype = None
+    L.orc_bucket_kpm_trace.argtypes = [i64, i32, vp, vp, vp, vp, vp, i32, i32, vp, vp]
     L.orc_num_threads.restype = i32
     L.orc_set_num_threads.argtypes = [i32]
     _LIB = L
@@ -229,6 +235,89 @@ class CSROperator:
         mu = np.zeros(N, dtype=np.float64)
         lib().orc_kpm_trace(self.D, _p(self.rowptr), _p(self.colidx), _p(self.vals),
                             a, b, N, R, _p(P), _p(mu))
+        return mu
+
+
+class BucketOperator:
+    """The reference's CPU "optimized mapping" (the CPU baseline's operator):
+    the diagonal and the off-diagonal entries grouped into buckets of equal
+    value, both rounded to 15 digits (get_diags_and_offdiagonals_by_value,
+    optimization.jl:134-182; entries below 1e-13 dropped), buckets in
+    ascending value, each row's columns in ascending order (allocate / pack,
+    optimization.jl:229-265).  Htilde uses the rescaled diagonal (d - b)/a and
+    values v/a (optimize_spectral_transform, optimization.jl:101-104).  Same
+    interface as CSROperator; the C kernels follow cpu/mapping.jl,
+    cpu/clenshaw_recurrence_relation.jl, cpu/clenshaw_final_sum.jl and the
+    threaded KPM of Moments.jl:87-109."""
+
+    def __init__(self, M, tol=1e-13, digits=15):
+        M = sp.csr_matrix(M, dtype=np.float64)
+        M.sort_indices()
+        self.D = M.shape[0]
+        D = self.D
+        self.diag = np.ascontiguousarray(np.round(M.diagonal(), digits))
+        coo = M.tocoo()
+        keep = (coo.row != coo.col) & (np.abs(coo.data) >= tol)
+        rows, cols = coo.row[keep].astype(np.int64), coo.col[keep].astype(np.int64)
+        keys = np.round(coo.data[keep], digits)
+        vals, inv = np.unique(keys, return_inverse=True)
+        self.bval = np.ascontiguousarray(vals)
+        self.nb = len(vals)
+        starts, flats, offs, off = [], [], [], 0
+        for k in range(self.nb):
+            sel = inv == k
+            r, c = rows[sel], cols[sel]
+            order = np.lexsort((c, r))
+            r, c = r[order], c[order]
+            starts.append(np.searchsorted(r, np.arange(D + 1)).astype(np.int64))
+            flats.append(c)
+            offs.append(off)
+            off += len(c)
+        self.bstart = np.ascontiguousarray(np.concatenate(starts) if starts else np.zeros(D + 1, np.int64))
+        self.bflat = np.ascontiguousarray(np.concatenate(flats) if flats else np.zeros(1, np.int64))
+        self.boff = np.ascontiguousarray(np.array(offs if offs else [0], dtype=np.int64))
+        self._scaled = {}
+
+    def _tables(self, a, b):
+        key = (a, b)
+        if key not in self._scaled:
+            self._scaled = {key: (np.ascontiguousarray((self.diag - b) / a), np.ascontiguousarray(self.bval / a))}
+        return self._scaled[key]
+
+    def _cm(self, X):
+        X = np.asarray(X, dtype=np.float64)
+        return np.asfortranarray(X.reshape(self.D, -1))
+
+    def _apply(self, X, a, b):
+        Xc = self._cm(X)
+        dg, bv = self._tables(a, b)
+        Y = np.zeros_like(Xc, order="F")
+        lib().orc_bucket_apply(self.D, self.nb, _p(dg), _p(bv), _p(self.bstart), _p(self.boff), _p(self.bflat),
+                               Xc.shape[1], _p(Xc), _p(Y))
+        return Y.reshape(np.shape(X))
+
+    def apply(self, X):
+        return self._apply(X, 1.0, 0.0)
+
+    def rescaled(self, X, a, b):
+        return self._apply(X, a, b)
+
+    def filter(self, X, a, b, coeffs):
+        Xc = self._cm(X)
+        dg, bv = self._tables(a, b)
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.float64)
+        Y = np.zeros_like(Xc, order="F")
+        work = np.empty(3 * self.D, dtype=np.float64)
+        lib().orc_bucket_filter(self.D, self.nb, _p(dg), _p(bv), _p(self.bstart), _p(self.boff), _p(self.bflat),
+                                len(coeffs) - 1, _p(coeffs), Xc.shape[1], _p(Xc), _p(Y), _p(work))
+        return Y.reshape(np.shape(X))
+
+    def kpm_trace(self, a, b, N, probes):
+        P = np.asfortranarray(probes, dtype=np.float64).reshape(self.D, -1, order="F")
+        dg, bv = self._tables(a, b)
+        mu = np.zeros(N, dtype=np.float64)
+        lib().orc_bucket_kpm_trace(self.D, self.nb, _p(dg), _p(bv), _p(self.bstart), _p(self.boff),
+                                   _p(self.bflat), N, P.shape[1], _p(P), _p(mu))
         return mu
 
 

@@ -18,6 +18,15 @@
  *   orc_clenshaw_filter   Clenshaw/Algorithm/ClenshawAlgorithm.jl:12-29 with
  *                         Clenshaw/Clenshaw.jl:69-117,141-153 (Chebyshev)
  *   orc_kpm_trace         DensetiesOfStates/Moments.jl:87-140 (trace!)
+ *   orc_bucket_*          the reference's CPU "optimized mapping": off-diagonal
+ *                         entries grouped by value (optimization.jl:134-182,
+ *                         allocate/pack :229-265), rescaled once
+ *                         (optimize_spectral_transform, optimization.jl:75-119),
+ *                         applied per bucket (cpu/mapping.jl:27-120,
+ *                         single_row_mappings.jl:9-79), the fused Clenshaw row
+ *                         kernels (cpu/clenshaw_recurrence_relation.jl:25-134,
+ *                         cpu/clenshaw_final_sum.jl:25-137) and the threaded
+ *                         KPM over probes (Moments.jl:87-109)
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -257,6 +266,147 @@ void orc_kpm_trace(int64_t D, const int64_t *rowptr, const int64_t *colidx, cons
                 for (int64_t i = 0; i < D; ++i) {
                     v2[i] = 2.0 * v2[i];
                     v2[i] = v2[i] - v0[i];
+                    d += al[i] * v2[i];
+                }
+                loc[n] += d;
+                double *t = v0; v0 = v1; v1 = v2; v2 = t;
+            }
+        }
+#pragma omp critical
+        for (int n = 0; n < N; ++n) mu[n] += loc[n];
+        free(loc);
+        free(w);
+    }
+}
+
+/* ------------------------------------------------ bucketed ("optimized") mapping */
+
+/* The packed form of optimization.jl:134-265: a diagonal diag[D] and nb
+ * value buckets; bucket k holds value bval[k] and, for every row i, the
+ * column indices bflat[boff[k] + bstart[k*(D+1) + i] ... bstart[k*(D+1)+i+1])
+ * of its entries equal to that value (0-based).  Diagonal and values are
+ * already the rescaled ones when used for Htilde. */
+typedef struct {
+    int64_t D;
+    int nb;
+    const double *diag;
+    const double *bval;
+    const int64_t *bstart;   /* nb x (D+1) */
+    const int64_t *boff;     /* nb offsets into bflat */
+    const int64_t *bflat;
+} orc_buckets;
+
+/* Serial single-vector form used inside the per-probe KPM chains. */
+static void bucket_map_vec_serial(const orc_buckets *B, const double *x, double *y) {
+    const int64_t D = B->D;
+    for (int64_t i = 0; i < D; ++i) y[i] = B->diag[i] * x[i];
+    for (int k = 0; k < B->nb; ++k) {
+        const int64_t *st = B->bstart + (int64_t)k * (D + 1);
+        const int64_t *fl = B->bflat + B->boff[k];
+        const double val = B->bval[k];
+        for (int64_t i = 0; i < D; ++i) {
+            double sum = 0.0;
+            for (int64_t p = st[i]; p < st[i + 1]; ++p) sum += x[fl[p]];
+            y[i] += val * sum;
+        }
+    }
+}
+
+static orc_buckets mkb(int64_t D, int nb, const double *diag, const double *bval, const int64_t *bstart,
+                       const int64_t *boff, const int64_t *bflat) {
+    orc_buckets B = {D, nb, diag, bval, bstart, boff, bflat};
+    return B;
+}
+
+/* mapping! for a vector, multi-bucket method (cpu/mapping.jl:46-64), the
+ * reference's default CPU strategy (MulColsParallel(1) -> column by column,
+ * each pass threaded over rows): y = diag .* x, then for each bucket in value
+ * order y_i += val * sum x[flat]. */
+static void bucket_map_vec(const orc_buckets *B, const double *x, double *y) {
+    const int64_t D = B->D;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < D; ++i) y[i] = B->diag[i] * x[i];
+    for (int k = 0; k < B->nb; ++k) {
+        const int64_t *st = B->bstart + (int64_t)k * (D + 1);
+        const int64_t *fl = B->bflat + B->boff[k];
+        const double val = B->bval[k];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < D; ++i) {
+            double sum = 0.0;
+            for (int64_t p = st[i]; p < st[i + 1]; ++p) sum += x[fl[p]];
+            y[i] += val * sum;
+        }
+    }
+}
+
+/* Y = Htilde X for a column-major D x s block, column by column
+ * (mapping_columnwise!, cpu/mapping.jl:67-95). */
+void orc_bucket_apply(int64_t D, int nb, const double *diag, const double *bval, const int64_t *bstart,
+                      const int64_t *boff, const int64_t *bflat, int s, const double *X, double *Y) {
+    orc_buckets B = mkb(D, nb, diag, bval, bstart, boff, bflat);
+    for (int c = 0; c < s; ++c) bucket_map_vec(&B, X + (int64_t)c * D, Y + (int64_t)c * D);
+}
+
+/* The Chebyshev filter with the fused row kernels, column by column: the
+ * recurrence b1 = c X + 2 Ht b2 - b3 (multi-bucket method: mapping!(b1, b2)
+ * then the elementwise update, clenshaw_recurrence_relation.jl:46-64) for
+ * k = K..1 with the buffer rotation of ClenshawAlgorithm.jl:2,25, then the
+ * final sum Y = c0 X + Ht b1 - b2 (clenshaw_final_sum.jl).  work: 3 D doubles. */
+void orc_bucket_filter(int64_t D, int nb, const double *diag, const double *bval, const int64_t *bstart,
+                       const int64_t *boff, const int64_t *bflat, int K, const double *coeffs, int s,
+                       const double *X, double *Y, double *work) {
+    orc_buckets B = mkb(D, nb, diag, bval, bstart, boff, bflat);
+    for (int c = 0; c < s; ++c) {
+        const double *x = X + (int64_t)c * D;
+        double *y = Y + (int64_t)c * D;
+        double *bb[3] = {work, work + D, work + 2 * D};
+        memset(work, 0, sizeof(double) * (size_t)(3 * D));
+        for (int k = K; k >= 1; --k) {
+            const double ck = coeffs[k];
+            bucket_map_vec(&B, bb[1], bb[0]);
+            double *b1 = bb[0], *b3 = bb[2];
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < D; ++i) b1[i] = ck * x[i] + 2.0 * b1[i] - b3[i];
+            double *t0 = bb[0], *t1 = bb[1], *t2 = bb[2];
+            bb[0] = t2; bb[1] = t0; bb[2] = t1;
+        }
+        bucket_map_vec(&B, bb[1], y);
+        const double c0 = coeffs[0];
+        const double *b2 = bb[2];
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < D; ++i) y[i] = c0 * x[i] + y[i] - b2[i];
+    }
+}
+
+/* KPM moments with the bucketed Htilde (trace!, Moments.jl:87-140): probes
+ * spread over threads, each a serial chain v_n = 2 Ht v_{n-1} - v_{n-2}. */
+void orc_bucket_kpm_trace(int64_t D, int nb, const double *diag, const double *bval, const int64_t *bstart,
+                          const int64_t *boff, const int64_t *bflat, int N, int R, const double *probes,
+                          double *mu) {
+    orc_buckets B = mkb(D, nb, diag, bval, bstart, boff, bflat);
+    for (int n = 0; n < N; ++n) mu[n] = 0.0;
+#pragma omp parallel
+    {
+        double *loc = (double *)calloc((size_t)N, sizeof(double));
+        double *w = (double *)malloc(sizeof(double) * (size_t)(3 * D));
+#pragma omp for schedule(static)
+        for (int r = 0; r < R; ++r) {
+            const double *al = probes + (int64_t)r * D;
+            double *v0 = w, *v1 = w + D, *v2 = w + 2 * D;
+            double d = 0.0;
+            for (int64_t i = 0; i < D; ++i) { v0[i] = al[i]; d += al[i] * v0[i]; }
+            loc[0] += d;
+            if (N > 1) {
+                bucket_map_vec_serial(&B, v0, v1);
+                d = 0.0;
+                for (int64_t i = 0; i < D; ++i) d += al[i] * v1[i];
+                loc[1] += d;
+            }
+            for (int n = 2; n < N; ++n) {
+                bucket_map_vec_serial(&B, v1, v2);
+                d = 0.0;
+                for (int64_t i = 0; i < D; ++i) {
+                    v2[i] = 2.0 * v2[i] - v0[i];
                     d += al[i] * v2[i];
                 }
                 loc[n] += d;

@@ -39,6 +39,7 @@ EXPORTED = [
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
     "pf_pool_set_priority_dim", "pf_pool_set_admission", "pf_pool_request_times",
     "pf_pool_wait", "pf_pool_shutdown", "pf_pool_set_batching", "pf_step_variant", "pf_set_step_variant",
+    "pf_gather_peak",
 ]
 PF_REQ_QUEUED, PF_REQ_RUNNING, PF_REQ_DONE, PF_REQ_FAILED, PF_REQ_REJECTED = 0, 1, 2, 3, 4
 PF_ADMIT_FIFO, PF_ADMIT_SHORTEST = 0, 1
@@ -150,6 +151,7 @@ def load():
         "pf_autotune": (i32, [vp, i32, i32, ctypes.POINTER(i32), vp]),
         "pf_set_step_width": (i32, [vp, i32, i32, i32]),
         "pf_set_step_variant": (i32, [vp, i32, i32, i32, i32]),
+        "pf_gather_peak": (i32, [vp, i32, ctypes.POINTER(f64)]),
         "pf_step_variant": (i32, [vp, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
         "pf_pool_create": (i32, [i32, i32, f64, ctypes.POINTER(vp)]),
         "pf_pool_destroy": (i32, [vp]),
@@ -209,6 +211,14 @@ def stream_of(h: int) -> int:
     s = ctypes.c_void_p()
     check(load().pf_handle_stream(h, ctypes.byref(s)))
     return s.value or 0
+
+
+def gather_peak(device: int = 0, log2_rows: int = 17) -> float:
+    """Measured bytes/s of random row gathers from an L2-resident block
+    (pf_gather_peak): the ceiling of an L2-resident step kernel."""
+    v = ctypes.c_double()
+    check(load().pf_gather_peak(handle(device), int(log2_rows), ctypes.byref(v)))
+    return v.value
 
 
 def synchronize(h: int) -> None:

@@ -256,6 +256,13 @@ int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms) {
     PF_API_END
 }
 
+int pf_gather_peak(pf_handle *h, int log2_rows, double *bytes_per_s) {
+    PF_API_BEGIN
+    PF_CHECK(h && bytes_per_s, PF_ERR_INVALID, "null argument");
+    *bytes_per_s = pf::gather_peak(h, log2_rows);
+    PF_API_END
+}
+
 int pf_step_variant(pf_op *op, int dtype, int s, int *width, int *gather_batch, int *ctas_per_sm) {
     PF_API_BEGIN
     PF_CHECK(op && width && gather_batch && ctas_per_sm, PF_ERR_INVALID, "null argument");

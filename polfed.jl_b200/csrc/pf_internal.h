@@ -226,6 +226,9 @@ void build_chain_diag(pf_op *op);
 // scratch blocks and records the fastest in op->tuned_width.  Returns it.
 int autotune_step(pf_op *op, int s, int dtype, std::vector<std::pair<int, float>> *timings);
 extern thread_local bool t_refuse_spilling;
+// Measured throughput (bytes/s) of random 32-byte-per-thread row gathers from
+// an L2-resident block of 2^log2_rows 64-byte rows.
+double gather_peak(pf_handle *h, int log2_rows);
 // Take the variant for (s, dtype) from the persistent tuning cache, if it holds
 // one for this device, model and size; returns whether it did.
 bool cached_step_variant(pf_op *op, int s, int dtype);

@@ -232,4 +232,73 @@ bool cached_step_variant(pf_op *op, int s, int dtype) {
     return true;
 }
 
+// ------------------------------------------------- gather-throughput probe
+// The roofline of a step whose blocks stay in L2: every thread owns half of a
+// 64-byte row (32 bytes, the FP64 s = 8 step's segment) and reads that half
+// of 16 other rows (row XOR a fixed mask per gather, the access pattern of
+// spin flips) of an L2-resident block of D rows, summing them.  All indices
+// stay below D (a power of two).
+template <int NG>
+__global__ void k_gather_probe(const double4 *__restrict__ q, double4 *__restrict__ out, uint32_t D) {
+    const uint32_t items = 2 * D;
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < items; it += gridDim.x * blockDim.x) {
+        const uint32_t row = it >> 1, half = it & 1u;
+        double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+        for (int k = 0; k < NG; ++k) {
+            const uint32_t mask = (0x9e3779b9u * (uint32_t)(k + 1)) >> 7;
+            const uint32_t nb = (row ^ mask) & (D - 1u);
+            const double4 v = q[(size_t)nb * 2 + half];
+            a.x += v.x;
+            a.y += v.y;
+            a.z += v.z;
+            a.w += v.w;
+        }
+        out[it] = a;
+    }
+}
+
+double gather_peak(pf_handle *h, int log2_rows) {
+    PF_CHECK(log2_rows >= 10 && log2_rows <= 24, PF_ERR_INVALID, "log2_rows must be in [10, 24]");
+    PF_CUDA(cudaSetDevice(h->device));
+    const uint32_t D = 1u << log2_rows;
+    double4 *q = nullptr, *out = nullptr;
+    PF_CUDA(cudaMalloc(&q, (size_t)D * 64));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    double best = 0.0;
+    try {
+        PF_CUDA(cudaMalloc(&out, (size_t)D * 64));
+        PF_CUDA(cudaMemsetAsync(q, 0, (size_t)D * 64, h->stream));
+        PF_CUDA(cudaEventCreate(&e0));
+        PF_CUDA(cudaEventCreate(&e1));
+        constexpr int NG = 16;
+        for (int mult = 2; mult <= 8; mult *= 2) {
+            const int grid = h->num_sms * mult;
+            for (int r = 0; r < 3; ++r) k_gather_probe<NG><<<grid, 256, 0, h->stream>>>(q, out, D);
+            PF_CUDA(cudaGetLastError());
+            PF_CUDA(cudaEventRecord(e0, h->stream));
+            const int reps = 50;
+            for (int r = 0; r < reps; ++r) k_gather_probe<NG><<<grid, 256, 0, h->stream>>>(q, out, D);
+            PF_CUDA(cudaEventRecord(e1, h->stream));
+            PF_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const double sec = ms * 1e-3 / reps;
+            best = std::max(best, (double)D * 2 * NG * 32 / sec);   // bytes gathered per second
+        }
+    } catch (...) {
+        cudaFree(q);
+        cudaFree(out);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        throw;
+    }
+    cudaFree(q);
+    cudaFree(out);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    count_launches(9 * 53);
+    return best;
+}
+
 }  // namespace pf

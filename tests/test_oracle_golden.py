@@ -218,3 +218,26 @@ def test_oracle_solve_matches_dense(orc):
     P = orc.clenshaw_coeffs_scalar(r.coeffs, (ev - r.b) / r.a)
     top = np.sort(ev[np.argsort(-P)[:8]])
     np.testing.assert_allclose(np.sort(r.vals), top, atol=1e-10)
+
+
+def test_bucketed_mapping_matches_csr(orc):
+    """The CPU baseline's bucketed operator (the reference's optimized mapping)
+    applies, filters and traces the same Hamiltonian as the CSR operator; an
+    XXZ chain has one off-diagonal value bucket and a J1-J2 chain two, as the
+    reference's packing gives (optimization.jl:134-265)."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+    f = rng.random(10)
+    Hx = orc.xxz_matrix(10, 5, 1.0, 0.7, f)
+    Hj = orc.j1j2_matrix(10, 5, 1.0, 0.5, 1.0, 1.0, f)
+    assert orc.BucketOperator(Hx).nb == 1 and orc.BucketOperator(Hj).nb == 2
+    for H in (Hx, Hj):
+        B, C = orc.BucketOperator(H), orc.CSROperator(H)
+        D = H.shape[0]
+        X = rng.standard_normal((D, 3))
+        np.testing.assert_allclose(B.apply(X), C.apply(X), rtol=0, atol=1e-13)
+        np.testing.assert_allclose(B.rescaled(X, 2.0, 0.3), C.rescaled(X, 2.0, 0.3), rtol=0, atol=1e-13)
+        co = np.cos(np.arange(21) * 0.4) * 0.1
+        np.testing.assert_allclose(B.filter(X, 6.0, 0.1, co), C.filter(X, 6.0, 0.1, co), rtol=0, atol=1e-11)
+        P = orc.normalized_gaussian_probes(D, 4, rng)
+        np.testing.assert_allclose(B.kpm_trace(6.0, 0.1, 16, P), C.kpm_trace(6.0, 0.1, 16, P), rtol=0, atol=1e-11)
