@@ -79,7 +79,8 @@ extern "C" {
 
 /* solve precision */
 #define PF_PREC_FP64  0  /* FP64 throughout (the reference's arithmetic) */
-#define PF_PREC_MIXED 1  /* FP32 filter and KPM; FP64 Ritz, residual, refinement */
+#define PF_PREC_MIXED 1  /* FP32 filter and KPM; FP64 Lanczos basis, Ritz vectors,
+                             residuals and pf_params.refine FP64 refinement passes */
 
 typedef struct pf_handle pf_handle;
 typedef struct pf_op pf_op;
@@ -229,7 +230,11 @@ typedef struct pf_params {
     int    precision;            /* PF_PREC_FP64 */
     int    reorth_passes;        /* 1 = FullRO of the reference; 2 = CGS2 */
     int    extrema_maxdim;       /* 1000 (Plan.jl:143,160) */
-    int    refine;               /* reserved (read by nothing): no FP64 refinement pass is implemented */
+    int    refine;               /* PF_PREC_MIXED: at most this many FP64 refinement passes (4; 0 = none).
+                                    Each applies the FP64 filter to the FP32 run's 2 nev leading Ritz
+                                    vectors (nev targets + nev guards, at most the Krylov dimension)
+                                    and runs a Rayleigh-Ritz step with the FP64 H on them; passes stop
+                                    once all nev targets meet eigentol. */
     int    autotune;             /* 1: time the step-kernel variants once per (op, s, dtype) */
 } pf_params;
 
@@ -251,7 +256,8 @@ typedef struct pf_report {
     int     converged_tol;
     double  eigentol, eigenresidual;
     int     converged_eigentol;
-    int     refined;                    /* pairs repaired by FP64 refinement */
+    int     refined;                    /* pairs that met eigentol only after the FP64 refinement
+                                           (PF_PREC_MIXED; its time is in stage 5) */
     int     numofchecks;
     int     converged_history[PF_REPORT_MAX_CHECKS];
     int     krylovdim_history[PF_REPORT_MAX_CHECKS];

@@ -57,12 +57,14 @@ class TransformConfig:
 @dataclass
 class FactorizationConfig:
     """FactorizationConfig.jl:49-70 (PolfedDefaults.jl:151-191).
-    ``reorth_passes`` 1 is the reference's FullRO; 2 is CGS2."""
+    ``reorth_passes`` 1 is the reference's FullRO; 2 is CGS2.  ``refine_passes``:
+    FP64 refinement passes of a ``precision="mixed"`` solve (0: none)."""
     which: str = "LR"
     tol: float = 1e-14
     eigentol: float = 1e-9
     overestimate_iters: float = 1.25
     reorth_passes: int = 1
+    refine_passes: int = 4
 
 
 @dataclass
@@ -149,6 +151,7 @@ class FactorizationReport:
     eigentol: float
     eigenresidual: float
     converged_eigentol: int
+    refined: int
     numofchecks: int
     converged_history: list
     krylovbasisdim_history: list
@@ -183,7 +186,7 @@ def _make_report(r: _lib.pf_report, kind: int, value: float) -> Report:
     fac = FactorizationReport("LanczosFactorization" if r.blocksize == 1 else "BlockLanczosFactorization",
                               r.blocksize, r.howmany, r.iters_needed, r.iters_reserved, r.krylovdim, r.tol,
                               r.residual, r.converged_tol, r.eigentol, r.eigenresidual, r.converged_eigentol,
-                              r.numofchecks, list(r.converged_history[:n]), list(r.krylovdim_history[:n]),
+                              r.refined, r.numofchecks, list(r.converged_history[:n]), list(r.krylovdim_history[:n]),
                               list(r.maxresidual_history[:n]))
     bench = BenchmarkReport({k: r.stage_seconds[i] for i, k in enumerate(STAGES)}, r.basis_bytes_reserved,
                             r.basis_bytes_used, int(r.kpm_block_matvecs), int(r.kernel_launches))
@@ -245,6 +248,7 @@ def _params(op: Operator, howmany: int, target, mapping: MappingConfig, transfor
     p.eigentol = fact.eigentol
     p.overestimate_iters = fact.overestimate_iters
     p.reorth_passes = int(fact.reorth_passes)
+    p.refine = int(fact.refine_passes)
     p.dos_N, p.dos_R = int(dos.N), int(dos.R)
     if dos.kernel not in _lib.KERNEL_IDS:
         raise ValueError(f"Unknown kernel: {dos.kernel}. Available: {list(_lib.KERNEL_IDS)}")

@@ -336,7 +336,7 @@ void pf_params_default(pf_params *p) {
     p->precision = PF_PREC_FP64;
     p->reorth_passes = 1;
     p->extrema_maxdim = 1000;       // Plan.jl:143,160
-    p->refine = 0;                  // reserved
+    p->refine = 4;                  // FP64 refinement passes of the mixed-precision solve
     p->autotune = 1;
 }
 

@@ -12,6 +12,10 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <memory>
 #include <numeric>
 
 namespace pf {
@@ -317,6 +321,8 @@ struct LanczosOut {
     int numofchecks = 0;
     std::vector<int> conv_hist, dim_hist;
     std::vector<double> res_hist;
+    std::vector<double> resid;     // FP64 residual norms of the returned Ritz vectors (before the prefix)
+    int refined = 0;               // pairs that met eigentol only after the FP64 refinement
 };
 
 using BlockMap = std::function<void(const double *X, double *Y)>;  // RI D x s, on h->stream
@@ -336,9 +342,37 @@ static double *pinned_scratch(pf_handle *h, size_t n) {
     return static_cast<double *>(h->pinned);
 }
 
+// keep_extra >= 0 (the mixed-precision solve): at the final check the
+// Ritz vectors of the howmany + keep_extra leading Ritz values (in `which`
+// order) are back-transformed, whatever converged, and returned in that order
+// with their FP64 Rayleigh quotients and residuals -- no prefix, no sort -- as
+// the starting subspace of the FP64 refinement.
+// The first nconv of the pairs (vals, RI D x cw vecs), reordered ascending
+// (LanczosMethod.jl:74-82); vals and vecs are replaced by the result.
+static void ascending_prefix(pf_handle *h, int64_t D, int nconv, std::vector<double> &vals, DevArray<double> &vecs) {
+    cudaStream_t st = h->stream;
+    std::vector<int> ord(nconv);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return vals[x] < vals[y]; });
+    std::vector<double> sv(nconv);
+    for (int i = 0; i < nconv; ++i) sv[i] = vals[ord[i]];
+    if (nconv > 0) {
+        const int cw = (int)(vecs.n / (size_t)D);  // columns of the RI vecs block
+        DevArray<double> perm((size_t)D * nconv);
+        for (int i = 0; i < nconv; ++i)
+            PF_CUDA(cudaMemcpy2DAsync(perm.p + i, nconv * sizeof(double), vecs.p + ord[i], cw * sizeof(double),
+                                      sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
+        sync(h);
+        std::swap(vecs.p, perm.p);
+        std::swap(vecs.n, perm.n);
+        std::swap(vecs.st, perm.st);
+    }
+    vals = sv;
+}
+
 static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
                     int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
-                    double *stage_acc) {
+                    double *stage_acc, int keep_extra = -1) {
     pf_handle *h = op->h;
     const int64_t D = op->dim;
     cudaStream_t st = h->stream;
@@ -553,6 +587,7 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
             out.res_hist.push_back(maxres);
             if (conv == howmany || numiter >= maxiter) {
                 // calculate_eigenvectors! (getvecs.jl:10-21): Psi = B Phi[:, idx[1:conv]]
+                if (keep_extra >= 0) conv = std::min(k, howmany + keep_extra);
                 out.vecs.alloc((size_t)D * std::max(conv, 1));
                 if (conv > 0) {
                     DevArray<double> phisel((size_t)k * conv);
@@ -574,8 +609,10 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
                     int ec = 0;
                     bool counting = true;
                     double maxe = 0.0;
+                    out.resid.assign(conv, 0.0);
                     for (int i = 0; i < conv; ++i) {
                         const double rr = std::sqrt(std::max(hr[i], 0.0));
+                        out.resid[i] = rr;
                         if (counting && rr < eigentol) ++ec;
                         else counting = false;
                         maxe = std::max(maxe, rr);
@@ -602,25 +639,140 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     clk.flush();
     out.numiter = numiter;
     out.krylovdim = k;
-    // LanczosMethod.jl:74-82: keep the converged prefix, ascending order
-    const int nconv = std::min(out.converged, out.eigenconverged);
-    std::vector<int> ord(nconv);
-    std::iota(ord.begin(), ord.end(), 0);
-    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return out.vals[x] < out.vals[y]; });
-    std::vector<double> sv(nconv);
-    for (int i = 0; i < nconv; ++i) sv[i] = out.vals[ord[i]];
-    if (nconv > 0) {
-        const int cw = (int)(out.vecs.n / (size_t)D);  // columns of the RI vecs block
-        DevArray<double> perm((size_t)D * nconv);
-        for (int i = 0; i < nconv; ++i)
-            PF_CUDA(cudaMemcpy2DAsync(perm.p + i, nconv * sizeof(double), out.vecs.p + ord[i], cw * sizeof(double),
-                                      sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
-        sync(h);
-        std::swap(out.vecs.p, perm.p);
-        std::swap(out.vecs.n, perm.n);
+    if (keep_extra >= 0) {
+        out.nconv = (int)(out.vecs.n / (size_t)D);
+        if (out.vals.empty()) out.nconv = 0;
+        return;   // the refinement takes the vectors as they are
     }
-    out.vals = sv;
-    out.nconv = nconv;
+    // LanczosMethod.jl:74-82: keep the converged prefix, ascending order
+    ascending_prefix(h, D, std::min(out.converged, out.eigenconverged), out.vals, out.vecs);
+    out.nconv = (int)out.vals.size();
+}
+
+// ------------------------------------------------- FP64 refinement (mixed)
+// Q R = W in place for an RI D x m block (CholQR2, Householder on the host
+// if the Gram matrix is not numerically positive definite).
+static void cholqr2_block(pf_handle *h, double *W, int64_t D, int m) {
+    cudaStream_t st = h->stream;
+    const double one = 1.0, zero = 0.0;
+    DevArray<double> Gd((size_t)m * m), Rd((size_t)m * m);
+    std::vector<double> G((size_t)m * m), R;
+    for (int pass = 0; pass < 2; ++pass) {
+        PF_CUBLAS(cublasDgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, m, (int)D, &one, W, m, W, m, &zero, Gd.p, m));
+        double *pin = pinned_scratch(h, (size_t)m * m);
+        PF_CUDA(cudaMemcpyAsync(pin, Gd.p, (size_t)m * m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync(h);
+        std::memcpy(G.data(), pin, (size_t)m * m * sizeof(double));
+        for (int j = 0; j < m; ++j)
+            for (int i = j + 1; i < m; ++i) G[i + (size_t)j * m] = G[j + (size_t)i * m];
+        if (!host_cholesky(G, m, R)) {
+            std::vector<double> hW((size_t)D * m), Rh;
+            PF_CUDA(cudaMemcpyAsync(hW.data(), W, hW.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+            sync(h);
+            host_householder_qr(hW, D, m, Rh);
+            PF_CUDA(cudaMemcpyAsync(W, hW.data(), hW.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            sync(h);
+            return;
+        }
+        std::memcpy(pin, R.data(), (size_t)m * m * sizeof(double));
+        PF_CUDA(cudaMemcpyAsync(Rd.p, pin, (size_t)m * m * sizeof(double), cudaMemcpyHostToDevice, st));
+        PF_CUBLAS(cublasDtrsm(h->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, m,
+                              (int)D, &one, Rd.p, m, W, m));
+        sync(h);   // the staging area is rewritten by the next pass
+    }
+}
+
+// The mixed-precision solve's FP64 refinement.  An FP32 filter perturbs every
+// Krylov block by ~1e-7 relative, so the Ritz vectors of the FP32 run stop
+// near 1e-5 in FP64 residual: their error is spread over the whole spectrum,
+// mostly far from the target window.  Each pass applies the FP64 filter to the
+// current vectors (damping every component by its filter value), orthonormalises
+// them, and runs a Rayleigh-Ritz step with the FP64 Hamiltonian on that
+// subspace, which also undoes the mixing among the window's own eigenvectors.
+// The subspace keeps m = nev + guard vectors; the nev of largest filter value
+// are the targets (the order of the Lanczos selection, which = LR on the
+// filter), the guards the next in |filter value|.  Each pass damps a target's
+// error along an eigenvector outside the subspace by the ratio of their
+// filter values.  Passes stop once the whole target prefix meets eigentol.
+// Returns the number of passes run.
+static int refine_fp64(pf_op *op, const std::vector<double> &coeffs, double a, double b, int nev, double eigentol,
+                       int max_passes, DevArray<double> &Psi, int m, std::vector<double> &vals,
+                       std::vector<double> &resid) {
+    pf_handle *h = op->h;
+    cudaStream_t st = h->stream;
+    const int64_t D = op->dim;
+    const int K = (int)coeffs.size() - 1;
+    const double one = 1.0, zero = 0.0;
+    auto filter_value = [&](double E) { return cheb_clenshaw(coeffs.data(), K, (E - b) / a); };
+    DevArray<double> W((size_t)D * m), HW((size_t)D * m), Gd((size_t)m * m), Wd(m), HPsi((size_t)D * m), r2(m), ev(m);
+    DevArray<int> dinfo(1);
+    int lwork = 0;
+    PF_CUSOLVER(cusolverDnDsyevd_bufferSize(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m, Gd.p, m,
+                                            Wd.p, &lwork));
+    DevArray<double> dwork((size_t)std::max(lwork, 1));
+    std::map<int, std::unique_ptr<Filter<double>>> filters;   // by column-chunk width
+    const int wmax = 32;
+    int passes = 0;
+    for (int pass = 0; pass < max_passes; ++pass) {
+        int ok = 0;
+        while (ok < nev && ok < (int)resid.size() && resid[ok] < eigentol) ++ok;
+        if (ok >= nev) break;
+        ++passes;
+        // W = P(Htilde) Psi, chunks of up to 32 columns through graph-captured filters
+        for (int c0 = 0; c0 < m; c0 += wmax) {
+            const int wc = std::min(wmax, m - c0);
+            auto &f = filters[wc];
+            if (!f) f.reset(new Filter<double>(op, wc, coeffs, a, b));
+            PF_CUDA(cudaMemcpy2DAsync(f->X.p, (size_t)wc * sizeof(double), Psi.p + c0, (size_t)m * sizeof(double),
+                                      (size_t)wc * sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
+            f->run(st);
+            PF_CUDA(cudaMemcpy2DAsync(W.p + c0, (size_t)m * sizeof(double), f->Y.p, (size_t)wc * sizeof(double),
+                                      (size_t)wc * sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
+        }
+        cholqr2_block(h, W.p, D, m);
+        // Rayleigh-Ritz with the FP64 Hamiltonian: G = W^T H W
+        launch_step<double>(op, st, D, m, W.p, nullptr, nullptr, HW.p, 0, 1.0, 0, 1.0, 0.0, StepFlags::Q, nullptr);
+        PF_CUBLAS(cublasDgemm(h->blas, CUBLAS_OP_N, CUBLAS_OP_T, m, m, (int)D, &one, W.p, m, HW.p, m, &zero, Gd.p, m));
+        PF_CUSOLVER(cusolverDnDsyevd(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, m, Gd.p, m, Wd.p,
+                                     dwork.p, lwork, dinfo.p));
+        double *pin = pinned_scratch(h, (size_t)m + 1);
+        PF_CUDA(cudaMemcpyAsync(pin, Wd.p, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        PF_CUDA(cudaMemcpyAsync(reinterpret_cast<int *>(pin + m), dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        sync(h);
+        std::vector<double> theta(pin, pin + m);
+        PF_CHECK(*reinterpret_cast<int *>(pin + m) == 0, PF_ERR_NUMERIC, "refinement eigenproblem failed to converge");
+        // the nev targets: the Ritz pairs of largest filter value (the Lanczos
+        // selection); the guards after them: the rest in decreasing |filter
+        // value|, so the filter's negative side lobes, which damp as slowly as
+        // the window's edge, are kept in the subspace and resolved by the
+        // Rayleigh-Ritz step instead of polluting the targets
+        std::vector<int> idx(m);
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(),
+                         [&](int x, int y) { return filter_value(theta[x]) > filter_value(theta[y]); });
+        std::stable_sort(idx.begin() + std::min(nev, m), idx.end(), [&](int x, int y) {
+            return std::fabs(filter_value(theta[x])) > std::fabs(filter_value(theta[y]));
+        });
+        DevArray<double> Ysel((size_t)m * m);
+        for (int i = 0; i < m; ++i)
+            PF_CUDA(cudaMemcpyAsync(Ysel.p + (size_t)i * m, Gd.p + (size_t)idx[i] * m, m * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st));
+        // Psi = W Y, H Psi = (H W) Y (RI blocks: cuBLAS sees their column-major transposes)
+        PF_CUBLAS(cublasDgemm(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, m, (int)D, m, &one, Ysel.p, m, W.p, m, &zero, Psi.p, m));
+        PF_CUBLAS(cublasDgemm(h->blas, CUBLAS_OP_T, CUBLAS_OP_N, m, (int)D, m, &one, Ysel.p, m, HW.p, m, &zero, HPsi.p,
+                              m));
+        vals.resize(m);
+        for (int i = 0; i < m; ++i) vals[i] = theta[idx[i]];
+        double *pe = pinned_scratch(h, 2 * (size_t)m);
+        std::memcpy(pe, vals.data(), m * sizeof(double));
+        PF_CUDA(cudaMemcpyAsync(ev.p, pe, m * sizeof(double), cudaMemcpyHostToDevice, st));
+        launch_colresid(h, st, D, m, HPsi.p, Psi.p, ev.p, r2.p);
+        PF_CUDA(cudaMemcpyAsync(pe + m, r2.p, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync(h);
+        resid.resize(m);
+        for (int i = 0; i < m; ++i) resid[i] = std::sqrt(std::max(pe[m + i], 0.0));
+    }
+    return passes;
 }
 
 // ------------------------------------------------------------- extrema
@@ -945,14 +1097,49 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
         };
         lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage);
     } else {
-        Filter<float> filt(op, s, coeffs, a, b);
-        BlockMap fmap = [&](const double *X, double *Y) {
-            launch_ri_to_cm<double, float>(st, (int64_t)D * s, 1, X, filt.X.p, (int64_t)D * s);
-            if (eng) engine_filter(eng, op, st, 4, s, ew, coeffs, a, b, filt.X.p, filt.Y.p, filt.A.p, filt.B.p);
-            else filt.run(st);
-            launch_ri_to_cm<float, double>(st, (int64_t)D * s, 1, filt.Y.p, Y, (int64_t)D * s);
-        };
-        lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage);
+        const bool refine = P->refine > 0;
+        // as many guard vectors as targets: the subspace iteration's rate at the
+        // last target is the filter ratio P(lambda_{2 nev}) / P(lambda_{nev})
+        const int guard = std::max(s, nev);
+        {
+            Filter<float> filt(op, s, coeffs, a, b);
+            BlockMap fmap = [&](const double *X, double *Y) {
+                launch_ri_to_cm<double, float>(st, (int64_t)D * s, 1, X, filt.X.p, (int64_t)D * s);
+                if (eng) engine_filter(eng, op, st, 4, s, ew, coeffs, a, b, filt.X.p, filt.Y.p, filt.A.p, filt.B.p);
+                else filt.run(st);
+                launch_ri_to_cm<float, double>(st, (int64_t)D * s, 1, filt.Y.p, Y, (int64_t)D * s);
+            };
+            lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage,
+                    refine ? guard : -1);
+        }
+        if (refine && out.nconv > 0) {
+            // FP64 passes on the FP32 run's nev + guard leading Ritz vectors (filter order)
+            auto r0 = std::chrono::steady_clock::now();
+            const int m = out.nconv;
+            int before = 0;
+            while (before < nev && before < m && out.resid[before] < P->eigentol) ++before;
+            std::vector<double> vals_f(out.vals), resid(out.resid);
+            refine_fp64(op, coeffs, a, b, nev, P->eigentol, P->refine, out.vecs, m, vals_f, resid);
+            int ec = 0;
+            double maxe = 0.0;
+            bool counting = true;
+            for (int i = 0; i < std::min(nev, m); ++i) {
+                if (counting && resid[i] < P->eigentol) ++ec;
+                else counting = false;
+                maxe = std::max(maxe, resid[i]);
+            }
+            out.eigenconverged = ec;
+            out.eigenresidual = maxe;
+            out.refined = std::max(0, ec - before);
+            vals_f.resize(m);
+            ascending_prefix(h, D, ec, vals_f, out.vecs);
+            out.vals = vals_f;
+            out.nconv = ec;
+            stage[5] += std::chrono::duration<double>(std::chrono::steady_clock::now() - r0).count();
+        } else if (refine) {
+            out.nconv = 0;
+            out.vals.clear();
+        }
     }
 
     // outputs
@@ -994,6 +1181,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
         R.eigentol = P->eigentol;
         R.eigenresidual = out.eigenresidual;
         R.converged_eigentol = out.eigenconverged;
+        R.refined = out.refined;
         R.numofchecks = out.numofchecks;
         for (int i = 0; i < (int)out.conv_hist.size() && i < PF_REPORT_MAX_CHECKS; ++i) {
             R.converged_history[i] = out.conv_hist[i];

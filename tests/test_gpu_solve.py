@@ -206,3 +206,38 @@ def test_config_c1_full_size(pkg, orc, cuda):
     n = min(len(vals), len(ref.vals))
     common = np.intersect1d(np.round(vals, 8), np.round(ref.vals, 8))
     assert len(common) >= n - 1
+
+
+def test_mixed_precision_refinement(pkg, orc, cuda):
+    """PF_PREC_MIXED: the FP32 filter alone leaves every Ritz vector near
+    1e-6..1e-5 in FP64 residual, so with refinement off the solve returns no
+    pair at eigentol = 1e-10.  The FP64 refinement passes (filter, then
+    Rayleigh-Ritz with the FP64 H) bring pairs to 1e-10: every pair returned is
+    an FP64 eigenpair to 1e-10 with the FP64 solve's eigenvalue.  With 8
+    passes this problem returns 26 of the FP64 solve's 32 pairs (the last
+    targets converge at the rate of the filter's side lobes, ~0.8 per pass)."""
+    rng = np.random.default_rng(33)
+    f, n, c, g = pkg.qsun_parameters(8, 3, 0.75, rng=rng)
+    op = pkg.QSunOperator(8, 3, 1.0, c, n, f, g)
+    H = orc.qsun_matrix(8, 3, 1.0, c, n, f, g)
+    D = H.shape[0]
+    x0, _ = np.linalg.qr(rng.standard_normal((D, 4)))
+    probes = orc.normalized_gaussian_probes(D, 32, rng)
+    kw = dict(dos=pkg.DoSConfig(N=128, R=32, probes=probes), produce_report=True)
+    v64, V64, r64 = pkg.polfed(op, x0, 32, ("rescaled", 0.4), fact=pkg.FactorizationConfig(eigentol=1e-10), **kw)
+    assert len(v64) == 32
+    v0, _, r0 = pkg.polfed(op, x0, 32, ("rescaled", 0.4), precision="mixed",
+                           fact=pkg.FactorizationConfig(eigentol=1e-10, refine_passes=0), **kw)
+    assert len(v0) == 0 and r0.factorization.refined == 0
+    res = {}
+    for passes in (4, 8):
+        vm, Vm, rm = pkg.polfed(op, x0, 32, ("rescaled", 0.4), precision="mixed",
+                                fact=pkg.FactorizationConfig(eigentol=1e-10, refine_passes=passes), **kw)
+        assert rm.spectral.order == r64.spectral.order
+        assert rm.factorization.refined == len(vm)
+        _check_pairs(H, vm, Vm, 1e-10)
+        d = np.abs(vm[:, None] - v64[None, :]).min(axis=1) / np.maximum(1, np.abs(vm))
+        assert np.all(d < 1e-10), d.max()
+        res[passes] = (len(vm), rm.factorization.eigenresidual)
+    assert res[8][0] >= 24 and res[8][0] >= res[4][0]
+    assert res[8][1] < res[4][1] < 1e-6
