@@ -202,8 +202,18 @@ int pf_set_step_width(pf_op *op, int dtype, int s, int width);
  * operators only, with 16- or 32-byte column segments: every gather of a row
  * issued at once as an asynchronous global-to-shared copy; 6 = Quantum Sun
  * operators only: each CTA stages a tile of 2^t consecutive rows in shared
- * memory and serves the grain block and the low outer-bit flips from it. */
+ * memory and serves the grain block and the low outer-bit flips from it;
+ * 7 = spin chains on an Sz sector only: the rank of a state reached by a
+ * flip of sites at most two apart is updated from the row's own rank (a few
+ * binomial-table reads) instead of re-ranked. */
 int pf_set_step_variant(pf_op *op, int dtype, int s, int width, int profile);
+
+/* Column slabs of the filter (no reference counterpart).  cols > 0: filter in
+ * slabs of cols columns (a divisor of s), so the block each step gathers from
+ * (D x cols) can stay in L2 while the once-touched streams pass with
+ * evict-first hints; cols <= 0: whole blocks (the default).  Results are
+ * unchanged either way. */
+int pf_set_filter_slab(pf_op *op, int cols);
 
 /* ----------------------------------------------------------- solving */
 typedef struct pf_params {

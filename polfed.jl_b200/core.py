@@ -811,6 +811,12 @@ def autotune(op: Operator, s: int, dtype: str = "fp64"):
     return w.value, {widths[i]: t[i] for i in range(6) if t[i] > 0}
 
 
+def set_filter_slab(op: Operator, cols: int = 0):
+    """Filter column slabs: ``cols`` > 0 filters in slabs of that many columns
+    (a divisor of s); <= 0 whole blocks (the default).  Results are unchanged."""
+    _lib.check(_lib.load().pf_set_filter_slab(op.op, int(cols)))
+
+
 def step_variant(op: Operator, s: int, dtype: str = "fp64"):
     """The step-kernel variant in use for block width ``s``: (columns per
     thread, gathers per batch, resident CTAs per SM); width 0 is the

@@ -282,17 +282,26 @@ int pf_step_variant(pf_op *op, int dtype, int s, int *width, int *gather_batch, 
 int pf_set_step_variant(pf_op *op, int dtype, int s, int width, int profile) {
     PF_API_BEGIN
     PF_CHECK(op, PF_ERR_INVALID, "null operator");
-    PF_CHECK(profile >= 0 && profile <= pf::kStepProfiles, PF_ERR_INVALID, "profile must be in 0..6");
+    PF_CHECK(profile >= 0 && profile <= pf::kStepProfiles, PF_ERR_INVALID, "profile must be in 0..7");
     PF_CHECK(width != PF_WIDTH_COOP || profile == 0, PF_ERR_INVALID, "the warp-cooperative step has no profiles");
     PF_CHECK(profile != pf::kProfileAsync || pf::qsun_async_eligible(op, s, width, dtype == PF_F64 ? 8 : 4),
              PF_ERR_INVALID,
              "asynchronous gathers (profile 5) need a Quantum Sun operator and 16- or 32-byte column segments");
     PF_CHECK(profile != pf::kProfileTile || pf::qsun_tile_eligible(op, s, width, dtype == PF_F64 ? 8 : 4),
              PF_ERR_INVALID, "row tiles (profile 6) need a Quantum Sun operator with at least 2^8 states");
+    PF_CHECK(profile != pf::kProfileLocalRank || (op->kind == pf::OP_CHAIN && op->Lup >= 0), PF_ERR_INVALID,
+             "local flip-rank updates (profile 7) need a spin-chain operator on an Sz sector");
     const int st = pf_set_step_width(op, dtype, s, width);
     if (st != PF_OK) return st;
     std::lock_guard<std::mutex> lock(op->tune_mu);
     op->tuned_width[std::make_pair(dtype == PF_F64 ? 8 : 4, s)] = pf::variant_code(width, profile);
+    PF_API_END
+}
+
+int pf_set_filter_slab(pf_op *op, int cols) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    op->slab_cols = cols;
     PF_API_END
 }
 

@@ -167,6 +167,7 @@ struct pf_op {
     void *d_desc64 = nullptr, *d_desc32 = nullptr;
     std::shared_ptr<void> multi_owner;
     int smem_bytes = 0;               // dynamic shared memory of the step kernels
+    int slab_cols = 0;                // filter column slabs: 0 automatic, > 0 forced width, < 0 never
     // autotuned columns-per-thread of the step kernel, keyed by (element bytes, s)
     std::mutex tune_mu;
     std::map<std::pair<int, int>, int> tuned_width;
@@ -191,29 +192,35 @@ struct StepFlags {
 //   Htilde q = (H q - shift q) * inva
 // flags select which of q / p / X take part; DOTS accumulates per column
 // <out,out> and <out,q> into dots[2*s] (deterministic two-stage reduction).
+// ld > 0: the blocks' row stride when only s of their columns take part (a
+// column slab of a wider RI block); stream != 0: x, p and out move with
+// evict-first cache hints.
 template <typename T>
 void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p,
                  const T *x, T *out, double cx, double alpha, double beta, double inva,
-                 double shift, int flags, double *dots);
+                 double shift, int flags, double *dots, int ld = 0, int stream = 0);
 
 // Same with an explicit columns-per-thread width V (s % V == 0, V*sizeof(T) <= 64),
 // or V == kCoopWidth: the warp-cooperative chain step (coop_eligible).
 template <typename T>
 void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p, const T *x, T *out,
                        double cx, double alpha, double beta, double inva, double shift, int flags, double *dots,
-                       int V);
+                       int V, int ld = 0, int stream = 0);
 int default_width(int s, int elem_bytes);
 constexpr int kCoopWidth = 0;
 // A step-kernel variant code: columns per thread V (bits 0-7) and a profile
 // (bits 8+; 0 = default gather batch and register cap, 1..kStepProfiles =
 // the tuned (batch, resident CTAs) pairs (8,2) (8,3) (4,4) (8,4), 5 =
 // asynchronous gathers and 6 = shared-memory row tiles, both Quantum Sun
-// only), or kCoopWidth for the warp-cooperative chain step.
-constexpr int kStepProfiles = 6;
+// only, 7 = local flip-rank updates, sector-basis chains only), or
+// kCoopWidth for the warp-cooperative chain step.
+constexpr int kStepProfiles = 7;
 // Profile 5: the Quantum Sun step with asynchronous (cp.async) row gathers;
-// profile 6: the Quantum Sun step over shared-memory tiles of 2^t rows.
+// profile 6: the Quantum Sun step over shared-memory tiles of 2^t rows;
+// profile 7: the sector-basis chain step with local flip-rank updates.
 constexpr int kProfileAsync = 5;
 constexpr int kProfileTile = 6;
+constexpr int kProfileLocalRank = 7;
 bool qsun_async_eligible(const pf_op *op, int s, int V, int elem);
 bool qsun_tile_eligible(const pf_op *op, int s, int V, int elem);
 constexpr int variant_code(int V, int profile) { return V | (profile << 8); }

@@ -37,7 +37,9 @@ namespace pf {
 template <typename T>
 struct StepArgs {
     uint32_t D;
-    int s;
+    int s;          // columns processed per row
+    int ld;         // row stride of the blocks (>= s: a column slab of a wider RI block)
+    int stream;     // 1: x, p and out move with evict-first hints (slab passes)
     int G;          // column groups per row = s / V
     uint32_t items; // D * G
     const T *q;
@@ -94,8 +96,10 @@ __device__ void finish_reduction(int nvals, const double *blockvals, double *par
 }
 
 // UB > 0 / MB > 0: a tuned variant's gather batch and resident-CTA target
-// (register cap); 0 keeps the defaults of Batch / MinBlocks.
-template <typename T, int V, class Desc, int FLAGS, int UB = 0, int MB = 0>
+// (register cap); 0 keeps the defaults of Batch / MinBlocks.  RK = 1 (chain
+// operators): flip ranks by the local update of flip_rank_local, with the
+// binomial table staged after the rank tables.
+template <typename T, int V, class Desc, int FLAGS, int UB = 0, int MB = 0, int RK = 0>
 __global__ void __launch_bounds__(kThreads, MB > 0 ? MB : MinBlocks<T, V>::value)
     k_step(const Desc d, const StepArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -105,11 +109,22 @@ __global__ void __launch_bounds__(kThreads, MB > 0 ? MB : MinBlocks<T, V>::value
     constexpr bool DOTS = (FLAGS & StepFlags::DOTS) != 0;
     const uint32_t *tab = reinterpret_cast<const uint32_t *>(smem_raw);
     const T *smem_t = reinterpret_cast<const T *>(smem_raw);
+    const uint32_t *ctab = nullptr;
     if constexpr (DescTraits<Desc>::kind == OP_CHAIN) {
         if (HASQ && !d.full) {
             const int n = rank_table_entries(d.nchunks);
             uint32_t *t = reinterpret_cast<uint32_t *>(smem_raw);
             for (int i = threadIdx.x; i < n; i += blockDim.x) t[i] = __ldg(d.rank_tab + i);
+            if constexpr (RK == 1) {
+                uint32_t *c = t + n;   // C(nn, k) for nn, k <= 32
+                for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) {
+                    const int nn = i / 33, k = i % 33;
+                    uint64_t r = k <= nn ? 1u : 0u;
+                    for (int q = 1; q <= k && q <= nn; ++q) r = r * (uint64_t)(nn - k + q) / (uint64_t)q;
+                    c[i] = (uint32_t)r;
+                }
+                ctab = c;
+            }
         }
     } else if constexpr (DescTraits<Desc>::kind == OP_QSUN) {
         T *sm = reinterpret_cast<T *>(smem_raw);
@@ -138,7 +153,7 @@ __global__ void __launch_bounds__(kThreads, MB > 0 ? MB : MinBlocks<T, V>::value
     for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < a.items; it += stride) {
         const uint32_t row = (G == 1u) ? it : it / G;
         const int c0 = (G == 1u) ? 0 : (int)(it - row * G) * V;
-        const size_t off = (size_t)row * a.s + c0;
+        const size_t off = (size_t)row * a.ld + c0;
         if constexpr (HASX) prefetch_l1(a.x + off);
         if constexpr (HASQ) prefetch_l1(a.q + off);
         if constexpr (HASP) prefetch_l1(a.p + off);
@@ -146,23 +161,25 @@ __global__ void __launch_bounds__(kThreads, MB > 0 ? MB : MinBlocks<T, V>::value
 #pragma unroll
         for (int v = 0; v < V; ++v) acc[v] = T(0);
         T diag;
-        if constexpr (DescTraits<Desc>::kind == OP_CHAIN)
-            chain_row<T, V, HASQ, UB>(d, tab, row, a.s, c0, a.q, acc, diag);
+        if constexpr (DescTraits<Desc>::kind == OP_CHAIN && RK == 1)
+            chain_row_local<T, V, HASQ, UB>(d, tab, ctab, row, a.ld, c0, a.q, acc, diag);
+        else if constexpr (DescTraits<Desc>::kind == OP_CHAIN)
+            chain_row<T, V, HASQ, UB>(d, tab, row, a.ld, c0, a.q, acc, diag);
         else if constexpr (DescTraits<Desc>::kind == OP_QSUN)
-            qsun_row<T, V, HASQ, UB>(d, smem_t, row, a.s, c0, a.q, acc, diag);
+            qsun_row<T, V, HASQ, UB>(d, smem_t, row, a.ld, c0, a.q, acc, diag);
         else
-            csr_row<T, V, HASQ, UB>(d, row, a.s, c0, a.q, acc, diag);
+            csr_row<T, V, HASQ, UB>(d, row, a.ld, c0, a.q, acc, diag);
         Pack<T, V> xo, qo, po, res;
 #pragma unroll
         for (int v = 0; v < V; ++v) xo.v[v] = qo.v[v] = po.v[v] = T(0);
-        if constexpr (HASX) xo = ldp<T, V>(a.x + off);
+        if constexpr (HASX) xo = ldp_hint<T, V>(a.x + off, a.stream);
         if constexpr (HASQ) qo = ldp<T, V>(a.q + off);
-        if constexpr (HASP) po = ldp<T, V>(a.p + off);
+        if constexpr (HASP) po = ldp_hint<T, V>(a.p + off, a.stream);
 #pragma unroll
         for (int v = 0; v < V; ++v)
             res.v[v] = step_combine<T>(HASX, HASQ, HASP, a.cx, xo.v[v], a.alpha, acc[v], diag, qo.v[v], a.inva, a.boa,
                                        a.beta, po.v[v]);
-        stp<T, V>(a.out + off, res);
+        stp_hint<T, V>(a.out + off, res, a.stream);
         if constexpr (DOTS) {
 #pragma unroll
             for (int v = 0; v < V; ++v) {
@@ -589,9 +606,9 @@ static bool spills(const void *kern) {
     return cache[kern] = attr.localSizeBytes > 0;
 }
 
-template <typename T, int V, class Desc, int FLAGS, int UB = 0, int MB = 0>
+template <typename T, int V, class Desc, int FLAGS, int UB = 0, int MB = 0, int RK = 0>
 static void launch_one(pf_op *op, cudaStream_t st, const Desc &d, StepArgs<T> a, int smem) {
-    auto kern = k_step<T, V, Desc, FLAGS, UB, MB>;
+    auto kern = k_step<T, V, Desc, FLAGS, UB, MB, RK>;
     if (t_refuse_spilling && spills((const void *)kern))
         throw Error(PF_ERR_UNSUPPORTED, "step-kernel variant spills registers");
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -610,11 +627,11 @@ static void launch_one(pf_op *op, cudaStream_t st, const Desc &d, StepArgs<T> a,
 
 // The tuned (gather batch, register cap) profiles apply to the filter's
 // steps (Q|P|X and Q|X); every other launch uses the defaults.
-template <typename T, int V, class Desc, int UB, int MB>
+template <typename T, int V, class Desc, int UB, int MB, int RK = 0>
 static bool dispatch_profile(pf_op *op, cudaStream_t st, const Desc &d, const StepArgs<T> &a, int flags, int smem) {
     using F = StepFlags;
-    if (flags == (F::Q | F::P | F::X)) launch_one<T, V, Desc, F::Q | F::P | F::X, UB, MB>(op, st, d, a, smem);
-    else if (flags == (F::Q | F::X)) launch_one<T, V, Desc, F::Q | F::X, UB, MB>(op, st, d, a, smem);
+    if (flags == (F::Q | F::P | F::X)) launch_one<T, V, Desc, F::Q | F::P | F::X, UB, MB, RK>(op, st, d, a, smem);
+    else if (flags == (F::Q | F::X)) launch_one<T, V, Desc, F::Q | F::X, UB, MB, RK>(op, st, d, a, smem);
     else return false;
     return true;
 }
@@ -759,11 +776,14 @@ static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int fl
         const ChainDesc<T> &d = chain_of<T>(op);
         if ((flags & StepFlags::Q) && !d.full) smem = rank_table_entries(d.nchunks) * 4;
         if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
+        if (profile == kProfileLocalRank && !d.full &&
+            dispatch_profile<T, V, ChainDesc<T>, 0, 0, 1>(op, st, d, a, flags, smem + 33 * 33 * 4))
+            return;
         dispatch_flags<T, V>(op, st, d, a, flags, smem, profile >= kProfileAsync ? 0 : profile);
     } else if (op->kind == OP_QSUN) {
         const QSunDesc<T> &d = qsun_of<T>(op);
-        if (profile == kProfileAsync && launch_qsun_async<T, V>(op, st, d, a, flags)) return;
-        if (profile == kProfileTile && launch_qsun_tile<T, V>(op, st, d, a, flags)) return;
+        if (profile == kProfileAsync && a.ld == a.s && launch_qsun_async<T, V>(op, st, d, a, flags)) return;
+        if (profile == kProfileTile && a.ld == a.s && launch_qsun_tile<T, V>(op, st, d, a, flags)) return;
         smem = QSunSmem<T>::bytes(d.dg);
         if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
         dispatch_flags<T, V>(op, st, d, a, flags, smem, profile >= kProfileAsync ? 0 : profile);
@@ -846,7 +866,7 @@ int default_width(int s, int elem_bytes) {
 template <typename T>
 void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p, const T *x, T *out,
                        double cx, double alpha, double beta, double inva, double shift, int flags, double *dots,
-                       int code) {
+                       int code, int ld, int stream) {
     const int V = variant_width(code), profile = variant_profile(code);
     PF_CHECK(profile >= 0 && profile <= kStepProfiles, PF_ERR_INVALID, "unknown step-kernel profile");
     PF_CHECK(D == op->dim, PF_ERR_INVALID, "block height does not match the operator dimension");
@@ -859,6 +879,10 @@ void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q,
     StepArgs<T> a;
     a.D = (uint32_t)D;
     a.s = s;
+    a.ld = ld > 0 ? ld : s;
+    a.stream = stream ? 1 : 0;
+    PF_CHECK(a.ld >= s, PF_ERR_INVALID, "row stride smaller than the column count");
+    PF_CHECK(!coop || a.ld == s, PF_ERR_INVALID, "the warp-cooperative step needs contiguous rows");
     a.G = coop ? s : s / V;
     PF_CHECK((int64_t)D * a.G < (int64_t)0xffffffffLL, PF_ERR_UNSUPPORTED, "block too large for one launch");
     a.items = (uint32_t)(D * a.G);
@@ -887,7 +911,7 @@ void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q,
 template <typename T>
 void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const T *p,
                  const T *x, T *out, double cx, double alpha, double beta, double inva,
-                 double shift, int flags, double *dots) {
+                 double shift, int flags, double *dots, int ld, int stream) {
     int V = default_width(s, (int)sizeof(T));
     {
         std::lock_guard<std::mutex> lock(op->tune_mu);
@@ -899,23 +923,24 @@ void launch_step(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q, const
         V = default_width(s, (int)sizeof(T));
         while (V > 1 && (V * (int)sizeof(T) > 32 || kThreads % (s / V) != 0)) V /= 2;
     }
-    if (V == kCoopWidth && !coop_eligible(op, s, flags)) V = default_width(s, (int)sizeof(T));
+    const bool slab = ld > 0 && ld != s;
+    if (V == kCoopWidth && (slab || !coop_eligible(op, s, flags))) V = default_width(s, (int)sizeof(T));
     if (variant_profile(V) != 0 && (flags & StepFlags::DOTS)) V = variant_width(V);
-    launch_step_width<T>(op, st, D, s, q, p, x, out, cx, alpha, beta, inva, shift, flags, dots, V);
+    launch_step_width<T>(op, st, D, s, q, p, x, out, cx, alpha, beta, inva, shift, flags, dots, V, ld, stream);
 }
 
 template void launch_step_width<double>(pf_op *, cudaStream_t, int64_t, int, const double *, const double *,
                                         const double *, double *, double, double, double, double, double, int,
-                                        double *, int);
+                                        double *, int, int, int);
 template void launch_step_width<float>(pf_op *, cudaStream_t, int64_t, int, const float *, const float *,
                                        const float *, float *, double, double, double, double, double, int,
-                                       double *, int);
+                                       double *, int, int, int);
 template void launch_step<double>(pf_op *, cudaStream_t, int64_t, int, const double *, const double *,
                                   const double *, double *, double, double, double, double, double,
-                                  int, double *);
+                                  int, double *, int, int);
 template void launch_step<float>(pf_op *, cudaStream_t, int64_t, int, const float *, const float *,
                                  const float *, float *, double, double, double, double, double,
-                                 int, double *);
+                                 int, double *, int, int);
 
 // --------------------------------------------------------- layout changes
 template <typename TS, typename TD>

@@ -291,6 +291,7 @@ pf_op *bind_op(const pf_op *src, pf_handle *h) {
     op->d_desc32 = src->d_desc32;
     op->multi_owner = src->multi_owner;
     op->smem_bytes = src->smem_bytes;
+    op->slab_cols = src->slab_cols;
     {
         std::lock_guard<std::mutex> lock(const_cast<pf_op *>(src)->tune_mu);
         op->tuned_width = src->tuned_width;

@@ -42,6 +42,45 @@ __device__ __forceinline__ uint32_t sector_rank(uint32_t st, const uint32_t *tab
     return r;
 }
 
+// Loads and stores of a row segment with evict-first ("streaming") cache
+// hints when `stream` is set, so data touched once per pass does not push the
+// gathered block out of L2.  Segments are moved as 8- or 16-byte words.
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> ldp_hint(const T *p, int stream) {
+    if (!stream) return ldp<T, V>(p);
+    Pack<T, V> r;
+    constexpr int bytes = V * (int)sizeof(T);
+    if constexpr (bytes % 16 == 0) {
+        const double2 *s = reinterpret_cast<const double2 *>(p);
+        double2 *d = reinterpret_cast<double2 *>(&r);
+#pragma unroll
+        for (int i = 0; i < bytes / 16; ++i) d[i] = __ldcs(s + i);
+    } else if constexpr (bytes == 8) {
+        *reinterpret_cast<double *>(&r) = __ldcs(reinterpret_cast<const double *>(p));
+    } else {
+        *reinterpret_cast<float *>(&r) = __ldcs(reinterpret_cast<const float *>(p));
+    }
+    return r;
+}
+template <typename T, int V>
+__device__ __forceinline__ void stp_hint(T *p, const Pack<T, V> &v, int stream) {
+    if (!stream) {
+        stp<T, V>(p, v);
+        return;
+    }
+    constexpr int bytes = V * (int)sizeof(T);
+    if constexpr (bytes % 16 == 0) {
+        double2 *d = reinterpret_cast<double2 *>(p);
+        const double2 *s = reinterpret_cast<const double2 *>(&v);
+#pragma unroll
+        for (int i = 0; i < bytes / 16; ++i) __stcs(d + i, s[i]);
+    } else if constexpr (bytes == 8) {
+        __stcs(reinterpret_cast<double *>(p), *reinterpret_cast<const double *>(&v));
+    } else {
+        __stcs(reinterpret_cast<float *>(p), *reinterpret_cast<const float *>(&v));
+    }
+}
+
 // Explicitly rounded arithmetic.  Every step-kernel variant (any width,
 // gather batch or register cap; per-thread, warp-cooperative or
 // multi-instance) performs exactly these operations in the same order, so all
@@ -123,6 +162,84 @@ __device__ __forceinline__ void chain_row(const ChainDesc<T> &d, const uint32_t 
                     const uint32_t st2 = st ^ bm;
                     r2[u] = d.full ? st2 : sector_rank(st2, tab, d.nchunks);
                 }
+            }
+        }
+        if constexpr (HASQ) {
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (act[u]) g[u] = ldp<T, V>(qc + (size_t)r2[u] * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (act[u]) {
+                    const T jh = d.jhalf[b0 + u];
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(jh, g[u].v[v], acc[v]);
+                }
+        }
+    }
+    diag = dg;
+}
+
+// Rank of the state reached by the flip of bond b from state st of rank row,
+// by the local update of the combinatorial number system when the bond joins
+// sites at most two apart: moving a particle between sites lo < hi changes
+// only the terms of the particles in [lo, hi].  With k0 particles below lo,
+// a particle moving up from lo to lo + 1 changes C(lo, k0+1) into
+// C(lo+1, k0+1), i.e. by C(lo, k0) (Pascal's rule); moving to lo + 2 past an
+// empty site changes C(lo, k0+1) into C(lo+2, k0+1), and past an occupied one
+// the middle particle also drops one ordinal.  A move down is the reverse
+// move's negative.  Farther bonds (the periodic wrap) use the full table
+// rank.  ctab[n * 33 + k] = C(n, k) for n, k <= 32.  Exact integer work: the
+// result equals sector_rank(st ^ bmask[b]).
+template <typename T>
+__device__ __forceinline__ uint32_t flip_rank_local(const ChainDesc<T> &d, const uint32_t *tab, const uint32_t *ctab,
+                                                    uint32_t st, uint32_t row, int b) {
+    const int i = d.bi[b], j = d.bj[b];
+    const int lo = i < j ? i : j, hi = i < j ? j : i;
+    const int span = hi - lo;
+    if (span > 2) return sector_rank(st ^ d.bmask[b], tab, d.nchunks);
+    const int k0 = __popc(st & ((1u << lo) - 1u));
+    const bool up = (st >> lo) & 1u;   // the particle sits at lo and moves to hi
+    uint32_t delta;
+    if (span == 1) {
+        delta = ctab[lo * 33 + k0];
+    } else {
+        const bool mid = (st >> (lo + 1)) & 1u;
+        if (!mid) delta = ctab[(lo + 2) * 33 + k0 + 1] - ctab[lo * 33 + k0 + 1];
+        else
+            delta = ctab[(lo + 2) * 33 + k0 + 2] + ctab[(lo + 1) * 33 + k0 + 1] - ctab[lo * 33 + k0 + 1] -
+                    ctab[(lo + 1) * 33 + k0 + 2];
+    }
+    return up ? row + delta : row - delta;
+}
+
+// chain_row with flip ranks from flip_rank_local (the rank of the row's own
+// state is the row index); identical sums in identical order.
+template <typename T, int V, bool HASQ, int UB = 0>
+__device__ __forceinline__ void chain_row_local(const ChainDesc<T> &d, const uint32_t *tab, const uint32_t *ctab,
+                                                uint32_t row, int s, int c0, const T *__restrict__ q, T (&acc)[V],
+                                                T &diag) {
+    constexpr int U = UB > 0 ? UB : Batch<T, V>::U;
+    const uint32_t st = d.full ? row : __ldg(d.states + row);
+    T dg = T(0);
+    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
+    const T *qc = q + c0;
+    for (int b0 = 0; b0 < d.nb; b0 += U) {
+        uint32_t r2[U];
+        bool act[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int b = b0 + u;
+            act[u] = false;
+            r2[u] = 0u;
+            if (b < d.nb) {
+                const uint32_t bm = d.bmask[b];
+                const uint32_t m = st & bm;
+                const bool differ = (m != 0u) && (m != bm);
+                dg += differ ? -d.jdq[b] : d.jdq[b];
+                act[u] = differ;
+                if (HASQ && differ) r2[u] = d.full ? (st ^ bm) : flip_rank_local(d, tab, ctab, st, row, b);
             }
         }
         if constexpr (HASQ) {

@@ -122,28 +122,44 @@ struct Filter {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
     }
-    void enqueue(cudaStream_t st) {
+    // Columns per slab (pf_set_filter_slab): the filter can run in column
+    // slabs whose gathered block (D x slab) stays in L2 while the once-touched
+    // streams pass with evict-first hints; every column's arithmetic is
+    // unchanged.  Off unless requested: at D = 2.7 M, s = 16 the step is
+    // bound by the latency of its dependent gathers, not by DRAM traffic, and
+    // slabs of 4 FP64 columns took 2.4 ms per step against 1.4 ms whole.
+    int slab_cols() const {
+        if (op->slab_cols > 0 && s % op->slab_cols == 0) return op->slab_cols;
+        return s;
+    }
+    int launches_per_step() const { return s / slab_cols(); }
+    // one step of the recurrence over every slab
+    void step(cudaStream_t st, const T *q, const T *p, T *out, double ck, double alpha, double beta, int flags) {
+        const int w = slab_cols();
         const int64_t D = op->dim;
-        const double inva = 1.0 / a;
+        for (int c0 = 0; c0 < s; c0 += w)
+            launch_step<T>(op, st, D, w, q ? q + c0 : nullptr, p ? p + c0 : nullptr, X.p + c0, out + c0, ck, alpha, beta,
+                           1.0 / a, b, flags, nullptr, w == s ? 0 : s, w == s ? 0 : 1);
+    }
+    void enqueue(cudaStream_t st) {
         using F = StepFlags;
         if (K == 0) {
-            launch_step<T>(op, st, D, s, nullptr, nullptr, X.p, Y.p, c[0], 0, 0, inva, b, F::X, nullptr);
+            step(st, nullptr, nullptr, Y.p, c[0], 0, 0, F::X);
             return;
         }
-        launch_step<T>(op, st, D, s, nullptr, nullptr, X.p, A.p, c[K], 0, 0, inva, b, F::X, nullptr);
-        if (K >= 2)
-            launch_step<T>(op, st, D, s, A.p, nullptr, X.p, B.p, c[K - 1], 2.0, 0, inva, b, F::Q | F::X, nullptr);
+        step(st, nullptr, nullptr, A.p, c[K], 0, 0, F::X);
+        if (K >= 2) step(st, A.p, nullptr, B.p, c[K - 1], 2.0, 0, F::Q | F::X);
         for (int k = K - 2; k >= 1; --k) {
             T *q = ((K - k - 1) % 2 == 0) ? A.p : B.p;  // b_{k+1}
             T *o = ((K - k) % 2 == 0) ? A.p : B.p;      // b_{k+2}, overwritten by b_k
-            launch_step<T>(op, st, D, s, q, o, X.p, o, c[k], 2.0, -1.0, inva, b, F::Q | F::P | F::X, nullptr);
+            step(st, q, o, o, c[k], 2.0, -1.0, F::Q | F::P | F::X);
         }
         T *b1 = ((K - 1) % 2 == 0) ? A.p : B.p;
         if (K == 1) {
-            launch_step<T>(op, st, D, s, b1, nullptr, X.p, Y.p, c[0], 1.0, 0, inva, b, F::Q | F::X, nullptr);
+            step(st, b1, nullptr, Y.p, c[0], 1.0, 0, F::Q | F::X);
         } else {
             T *b2 = ((K - 2) % 2 == 0) ? A.p : B.p;
-            launch_step<T>(op, st, D, s, b1, b2, X.p, Y.p, c[0], 1.0, -1.0, inva, b, F::Q | F::P | F::X, nullptr);
+            step(st, b1, b2, Y.p, c[0], 1.0, -1.0, F::Q | F::P | F::X);
         }
     }
     // Capture the K+1 launches once; every later application is one graph launch.
@@ -164,7 +180,7 @@ struct Filter {
             PF_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         }
         PF_CUDA(cudaGraphLaunch(exec, st));
-        count_launches(K + 1);
+        count_launches((int64_t)(K + 1) * launches_per_step());
     }
 };
 

@@ -137,7 +137,8 @@ static int tune_typed(pf_op *op, int s, std::vector<std::pair<int, float>> *timi
             if (s % V == 0)
                 for (int prof = 0; prof <= kStepProfiles; ++prof)
                     if ((prof != kProfileAsync || qsun_async_eligible(op, s, V, (int)sizeof(T))) &&
-                        (prof != kProfileTile || qsun_tile_eligible(op, s, V, (int)sizeof(T))))
+                        (prof != kProfileTile || qsun_tile_eligible(op, s, V, (int)sizeof(T))) &&
+                        (prof != kProfileLocalRank || (op->kind == OP_CHAIN && op->Lup >= 0)))
                         codes.push_back(variant_code(V, prof));
         if (coop_eligible(op, s, StepFlags::Q | StepFlags::P | StepFlags::X)) codes.push_back(kCoopWidth);
         struct Refuse {
@@ -201,10 +202,6 @@ int autotune_step(pf_op *op, int s, int dtype, std::vector<std::pair<int, float>
 }
 
 void variant_params(int code, int elem, int *V, int *U, int *MB) {
-    // profile 5 (asynchronous gathers) reports batch 0: all of a row's gathers at once;
-    // profile 6 (row tiles) batches its L2 gathers by 4
-    static const int prof_u[kStepProfiles + 1] = {0, 8, 8, 4, 8, 0, 4};
-    static const int prof_mb[kStepProfiles + 1] = {0, 2, 3, 4, 4, 0, 2};
     if (code == kCoopWidth) {
         *V = 0, *U = 0, *MB = 0;
         return;
@@ -212,8 +209,13 @@ void variant_params(int code, int elem, int *V, int *U, int *MB) {
     *V = variant_width(code);
     const int prof = variant_profile(code);
     const int bytes = *V * elem;
-    *U = prof ? prof_u[prof] : (bytes >= 64 ? 2 : (bytes >= 16 ? 4 : 8));
-    *MB = prof ? prof_mb[prof] : (bytes >= 32 ? 2 : 3);
+    // defaults of the width (profiles 0 and 7 use them)
+    *U = bytes >= 64 ? 2 : (bytes >= 16 ? 4 : 8);
+    *MB = bytes >= 32 ? 2 : 3;
+    static const int prof_u[5] = {0, 8, 8, 4, 8}, prof_mb[5] = {0, 2, 3, 4, 4};
+    if (prof >= 1 && prof <= 4) *U = prof_u[prof], *MB = prof_mb[prof];
+    if (prof == kProfileAsync) *U = 0, *MB = 0;   // every gather of a row at once
+    if (prof == kProfileTile) *U = 4, *MB = 2;
 }
 
 bool cached_step_variant(pf_op *op, int s, int dtype) {

@@ -328,6 +328,8 @@ def test_every_step_variant_gives_identical_results(pkg, orc, cuda, models, dts)
                 profiles.append(5)                # asynchronous gathers
             if op.kind == "qsun" and op.dim >= 256:
                 profiles.append(6)                # shared-memory row tiles
+            if op.kind == "spin_chain" and op.Lup >= 0:
+                profiles.append(7)                # local flip-rank updates
             for profile in profiles:
                 pkg.set_step_width(op, s, width, dts, profile=profile)
                 assert pkg.step_variant(op, s, dts)[0] == width
@@ -339,3 +341,28 @@ def test_every_step_variant_gives_identical_results(pkg, orc, cuda, models, dts)
                 else:
                     np.testing.assert_array_equal(got, ref, err_msg=f"{name} width={width} profile={profile}")
         pkg.set_step_width(op, s, min(8, 64 // elem), dts)
+
+
+@pytest.mark.parametrize("dts", ["fp64", "fp32"])
+def test_column_slabs_give_identical_filters(pkg, orc, cuda, models, dts):
+    """Large blocks are filtered in column slabs (each step gathers from a
+    slab that fits in L2); every column's arithmetic is unchanged, so forced
+    slabs of 2 and 4 columns reproduce the whole-block filter bit for bit."""
+    dt = cuda.float64 if dts == "fp64" else cuda.float32
+    s = 8
+    rng = np.random.default_rng(19)
+    plan = orc.build_transform_plan(("rescaled", 0.1), 10, 1.0, 0.0, order=30)
+    coeffs = orc.filter_coefficients(plan)
+    for name, op, H in models:
+        D = H.shape[0]
+        X = _dev(cuda, rng.standard_normal((D, s)), dt)
+        Emax = float(np.abs(H).sum(axis=1).max())
+        out = {}
+        for cols in (-1, 4, 2):
+            pkg.set_filter_slab(op, cols)
+            Y = pkg.col_major(D, s, dtype=dt)
+            pkg.chebyshev_filter(op, Y, X, coeffs, a=1.01 * Emax, b=0.0)
+            out[cols] = _host(Y)
+        pkg.set_filter_slab(op, 0)
+        np.testing.assert_array_equal(out[4], out[-1], err_msg=name)
+        np.testing.assert_array_equal(out[2], out[-1], err_msg=name)
