@@ -388,6 +388,7 @@ def run_ours(args, rank, world, local_rank):
     stages = {k: sum(r.benchmark.stage_seconds[k] for r in reps) / len(reps) for k in reps[0].benchmark.stage_seconds}
     if rank != 0:
         return 0
+    served = served_sample(pkg, local_rank) if world == 1 else None
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample()
@@ -422,6 +423,7 @@ def run_ours(args, rank, world, local_rank):
                              "seconds_per_solve": kpm_sec,
                              "measured_in": "the single-solve runs (library stage timer 'dos')"}},
         "cpu_baseline": cpu,
+        "served": served,
         "clocks": clocks,
         "e2e_clocks": e_clocks,
         "converged_per_solve": statistics.mean(nconv),
@@ -440,22 +442,69 @@ DISORDER = {"workload": "disorder average: 256 x XXZ L=16 (D=12870) + 32 x XXZ L
             "seed": 31337, "eigentol": 1e-10, "dos_N": 250, "dos_R": 300, "nev": 50}
 
 
-def _serve_request(pkg, rng, device):
-    """One request of the mixed served stream (seeded)."""
+def _serve_request(pkg, rng, device, small=False):
+    """One request of the mixed served stream (seeded).  small: the bounded
+    sample of the main benchmark line (XXZ L 14..16, Quantum Sun L_loc 10..13,
+    nev 50..200), whose solves take well under a second each."""
     import numpy as np
     if rng.random() < 0.5:
-        L = int(rng.integers(14, 21))
+        L = int(rng.integers(14, 17 if small else 21))
         op = pkg.xxz_hamiltonian(L, L // 2, 1.0, 1.0, 5.0, rng=rng, device=device)
         name = f"xxz_L{L}"
     else:
-        L_loc = int(rng.integers(10, 16))
+        L_loc = int(rng.integers(10, 14 if small else 16))
         op = pkg.qsun_hamiltonian(L_loc, 3, 1.0, 0.75, gamma=1.0, w=0.5, hz=1.0, zeta=0.2, rng=rng, device=device)
         name = f"qsun_Lloc{L_loc}"
     eps = float(rng.uniform(0.1, 0.9))
-    nev = int(rng.choice([20, 50, 100, 200]))
+    nev = int(rng.choice([50, 100, 200] if small else [20, 50, 100, 200]))
     s = int(rng.choice([4, 8, 16]))
     x0 = np.asfortranarray(rng.random((op.dim, s)))
     return name, op, x0, eps, nev, s
+
+
+def served_sample(pkg, local_rank, requests=12, rate=2.0, workers=4):
+    """A bounded served stream for the main benchmark line: seeded Poisson
+    arrivals submitted at their arrival times to a request pool; returns the
+    pool's latency percentiles (submit -> done) and throughput."""
+    import numpy as np
+    rng = np.random.default_rng(SERVE["seed"] + 1)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=requests))
+    arrivals -= arrivals[0]
+    pool = pkg.SolverPool(workers=workers, device=local_rank)
+    pool.set_admission("shortest")
+    wrng = np.random.default_rng(1)
+    _, op, x0, eps, nev, s = _serve_request(pkg, wrng, local_rank, small=True)
+    pool.result(pool.submit(op, x0, 20, ("rescaled", eps), dos=pkg.DoSConfig(N=64, R=16, seed=1)))
+    base = pool.stats()
+    ids = []
+    t0 = time.perf_counter()
+    for i in range(requests):
+        delay = t0 + arrivals[i] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        _, op, x0, eps, nev, s = _serve_request(pkg, rng, local_rank, small=True)
+        ids.append(pool.submit(op, x0, nev, ("rescaled", eps), vecs=False,
+                               dos=pkg.DoSConfig(N=SERVE["dos_N"], R=SERVE["dos_R"], seed=SERVE["seed"] + i),
+                               fact=pkg.FactorizationConfig(eigentol=SERVE["eigentol"])))
+    nconv, rejected, failed = 0, 0, 0
+    for rid in ids:
+        try:
+            vals, _ = pool.result(rid)
+            nconv += len(vals)
+        except pkg._lib.PolfedRejected:
+            rejected += 1
+        except pkg._lib.PolfedError:
+            failed += 1
+    wall = time.perf_counter() - t0
+    st = pool.stats()
+    pool.close()
+    return {"requests": requests, "rate_per_s": rate, "workers": workers, "admission": "shortest",
+            "mix": "XXZ L=14..16 (Sz=0 or -1/2) and Quantum Sun L_loc=10..13, eps~U[0.1,0.9], nev in {50,100,200}, "
+                   "s in {4,8,16}, seeded Poisson arrivals",
+            "eigenpairs_per_s": nconv / wall, "converged": nconv, "rejected": rejected, "failed": failed,
+            "latency_s": {"p50": st.p50_latency, "p99": st.p99_latency, "mean": st.mean_latency,
+                          "note": "submit -> done, host clock, queueing included"},
+            "completed": st.completed - base.completed, "wall_seconds": wall}
 
 
 def run_serve(args, local_rank):
@@ -643,6 +692,60 @@ def run_disorder(args, local_rank):
     return 0
 
 
+C3 = {"workload": "j1j2_L24_Sz0_D2704156_s16_nev100_eps0.5_fp64",
+      "model": "J1-J2 Heisenberg chain, PBC, J1=1, J2=0.5, Delta=1, h_i~U[-1,1], Sz=0", "L": 24, "D": 2704156,
+      "blocksize": 16, "nev": 100, "target": "(:rescaled, 0.5)", "dos_N": 512, "dos_R": 64,
+      "probes": "Rademacher +-1/sqrt(D)", "eigentol": 1e-10, "seed": 2424}
+
+
+def run_c3(args, local_rank):
+    """One complete FP64 solve at the J1-J2 L = 24 configuration, with every
+    returned pair's residual checked again against the FP64 CSR matrix of the
+    oracle (a different code path: scipy sparse products on the host) for a
+    sample of the returned vectors."""
+    import numpy as np
+    import torch
+    import __graft_entry__ as ge
+    from oracle import oracle as orc
+    torch.cuda.set_device(local_rank)
+    pkg = ge.load_package()
+    pkg.load_library()
+    rng = np.random.default_rng(C3["seed"])
+    op = pkg.j1j2_hamiltonian(24, 12, 1.0, 0.5, 1.0, 1.0, 1.0, rng=rng, device=local_rank)
+    D, s, nev = op.dim, C3["blocksize"], C3["nev"]
+    x0 = np.asfortranarray(rng.random((D, s)))
+    pkg.autotune(op, s, "fp64")
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    t0 = time.perf_counter()
+    vals, vecs, rep = pkg.polfed(op, x0, nev, ("rescaled", 0.5), produce_report=True,
+                                 dos=pkg.DoSConfig(N=C3["dos_N"], R=C3["dos_R"], probe_kind="rademacher", seed=11),
+                                 fact=pkg.FactorizationConfig(eigentol=C3["eigentol"]))
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    t1 = time.perf_counter()
+    H = orc.j1j2_matrix(24, 12, 1.0, 0.5, 1.0, 1.0, op.fields)
+    sample = list(range(0, len(vals), max(1, len(vals) // 8)))[:8]
+    res = [float(np.linalg.norm(H @ vecs[:, j] - vals[j] * vecs[:, j])) for j in sample]
+    check_s = time.perf_counter() - t1
+    b = rep.benchmark
+    steps = rep.factorization.itersneeded * (rep.spectral.order + 1)
+    out = {"metric": "converged eigenpairs/s at resid<=1e-10 (J1-J2 L=24 solve)",
+           "value": len(vals) / b.stage_seconds["total"], "unit": "eigenpairs/s", "n_gpus": 1, "dtype": "f64",
+           "data": "synthetic (seeded realisation)", "config": C3, "converged": len(vals),
+           "solve_seconds": b.stage_seconds["total"], "wall_seconds": wall, "order": rep.spectral.order,
+           "iters": rep.factorization.itersneeded, "krylovdim": rep.factorization.krylovdim,
+           "eigenresidual_max": rep.factorization.eigenresidual,
+           "step_us": 1e6 * b.stage_seconds["mapping"] / max(steps, 1),
+           "step_frac_of_hbm": (4.0 * D * s * 8) / (b.stage_seconds["mapping"] / max(steps, 1)) / 1e9 /
+                               read_peaks()[0],
+           "csr_check": {"vectors": sample, "residuals": res, "max": max(res) if res else None,
+                         "seconds": check_s},
+           "stage_seconds": b.stage_seconds, "clocks": clocks}
+    print(json.dumps(out))
+    return 0
+
+
 def profile_step():
     """Two order-30 Chebyshev filters on one realisation of the workload's
     operator (s = 8, FP64) with the autotuned step: a small, bounded case for
@@ -761,6 +864,7 @@ def main():
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--admission", choices=["fifo", "shortest"], default="fifo",
                     help="served stream admission order")
+    ap.add_argument("--c3", action="store_true", help="one FP64 solve at the J1-J2 L=24 configuration")
     ap.add_argument("--step-sweep", action="store_true", help="time the Clenshaw step across sizes and precisions")
     ap.add_argument("--large-only", action="store_true", help="with --step-sweep: only the J1-J2 L=24 case")
     ap.add_argument("--profile-step-large", choices=["fp64", "fp32"], default=None,
@@ -780,6 +884,8 @@ def main():
         return step_sweep(args.large_only)
     if args.profile_step_large:
         return profile_step_large(args.profile_step_large)
+    if args.c3:
+        return run_c3(args, local_rank)
     if args.serve:
         return run_serve(args, local_rank)
     if args.disorder:

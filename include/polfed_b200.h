@@ -184,6 +184,16 @@ int pf_kpm_moments(pf_op *op, int dtype, double a, double b, int N, int R,
  * that pf_solve consults before timing. */
 #define PF_WIDTH_COOP 0
 int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms);
+/* G = B^T r on the 5th-generation tensor cores (tcgen05.mma, BF16 inputs,
+ * FP32 accumulation) in split BF16: every FP64 value v = hi + lo with
+ * hi = bf16(v), lo = bf16(v - hi), and G ~= Bhi^T rhi + Bhi^T rlo + Blo^T rhi,
+ * the row chunks' FP32 partial sums added in FP64.  B is row-major D x nB with
+ * row stride ldb (the Krylov basis layout), r row-major D x s (s <= 32), G
+ * column-major nB x s; all device pointers.  Relative error ~1e-5 of |B| |r|:
+ * the first pass of the reorthogonalisation mode reorth_passes = 3 (the
+ * Gram contraction of reorthogonalization.jl:77-84).  Synchronises. */
+int pf_gram_bf16x3(pf_handle *h, int64_t D, int nB, const double *B, int64_t ldb, const double *r, int s,
+                   double *G);
 /* Roofline probe (no reference counterpart): the measured throughput, in
  * bytes per second, of random row gathers -- each thread reads 32 bytes of 16
  * rows chosen by a row-XOR pattern, as spin flips do -- from an L2-resident
@@ -238,7 +248,9 @@ typedef struct pf_params {
     uint64_t seed;               /* probe seed */
     const double *probes;        /* optional host D x R normalised probes (overrides seed) */
     int    precision;            /* PF_PREC_FP64 */
-    int    reorth_passes;        /* 1 = FullRO of the reference; 2 = CGS2 */
+    int    reorth_passes;        /* 1 = FullRO of the reference; 2 = CGS2 in FP64; 3 = CGS2 whose first
+                                    Gram product B^T r runs on the tensor cores in split BF16
+                                    (pf_gram_bf16x3), the updates and the second pass in FP64 (s <= 32) */
     int    extrema_maxdim;       /* 1000 (Plan.jl:143,160) */
     int    refine;               /* PF_PREC_MIXED: at most this many FP64 refinement passes (4; 0 = none).
                                     Each applies the FP64 filter to the FP32 run's 2 nev leading Ritz

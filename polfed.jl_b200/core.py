@@ -57,7 +57,8 @@ class TransformConfig:
 @dataclass
 class FactorizationConfig:
     """FactorizationConfig.jl:49-70 (PolfedDefaults.jl:151-191).
-    ``reorth_passes`` 1 is the reference's FullRO; 2 is CGS2.  ``refine_passes``:
+    ``reorth_passes`` 1 is the reference's FullRO; 2 is CGS2 in FP64; 3 is CGS2
+    with its first Gram product on the tensor cores in split BF16.  ``refine_passes``:
     FP64 refinement passes of a ``precision="mixed"`` solve (0: none)."""
     which: str = "LR"
     tol: float = 1e-14

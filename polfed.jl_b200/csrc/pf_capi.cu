@@ -256,6 +256,13 @@ int pf_autotune(pf_op *op, int dtype, int s, int *width, float *times_ms) {
     PF_API_END
 }
 
+int pf_gram_bf16x3(pf_handle *h, int64_t D, int nB, const double *B, int64_t ldb, const double *r, int s,
+                   double *G) {
+    PF_API_BEGIN
+    pf::op_gram_bf16x3(h, D, nB, B, ldb, r, s, G);
+    PF_API_END
+}
+
 int pf_gather_peak(pf_handle *h, int log2_rows, double *bytes_per_s) {
     PF_API_BEGIN
     PF_CHECK(h && bytes_per_s, PF_ERR_INVALID, "null argument");

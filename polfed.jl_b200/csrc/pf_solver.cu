@@ -406,6 +406,9 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     DevArray<double> bufs((size_t)D * s * 3);
     double *vlast = bufs.p, *vprev = bufs.p + (size_t)D * s, *r = bufs.p + 2 * (size_t)D * s;
     DevArray<double> smallA((size_t)s * s), smallB((size_t)s * s), G((size_t)maxdim * s);
+    DevArray<unsigned char> tc_work(reorth_passes == 3 ? gram_bf16_workspace(D, maxdim, s) : 0);
+    DevArray<int> tc_err(reorth_passes == 3 ? 1 : 0);
+    if (reorth_passes == 3) PF_CUDA(cudaMemsetAsync(tc_err.p, 0, sizeof(int), st));
     std::vector<double> T((size_t)maxdim * maxdim, 0.0);  // column-major
     std::vector<double> hA((size_t)s * s), hR, hR1, hR2, beta_last((size_t)s * s, 0.0);
     const double one = 1.0, zero = 0.0, mone = -1.0;
@@ -541,11 +544,17 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
         cudaEvent_t e4 = clk.mark();
         clk.add(3, e3, e4);
         // 5 reorthogonalization: r -= B (B^T r), B = all but the last two blocks
+        // (reorth_passes 3: CGS2 whose first Gram product runs on the tensor
+        // cores in split BF16, the second in FP64)
         const int nB = k - 2 * s;
         if (nB > 0) {
-            for (int pass = 0; pass < reorth_passes; ++pass) {
-                PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, nB, s, (int)D, &one, basis.p, ldb, r, s, &zero,
-                                      G.p, nB));
+            const int passes = reorth_passes == 3 ? 2 : reorth_passes;
+            for (int pass = 0; pass < passes; ++pass) {
+                if (reorth_passes == 3 && pass == 0)
+                    gram_bf16x3(h, st, D, nB, basis.p, ldb, r, s, G.p, tc_work.p, tc_err.p);
+                else
+                    PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, nB, s, (int)D, &one, basis.p, ldb, r, s,
+                                          &zero, G.p, nB));
                 PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, nB, &mone, G.p, nB, basis.p, ldb, &one,
                                       r, s));
             }
@@ -653,6 +662,11 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     }
     sync(h);
     clk.flush();
+    if (reorth_passes == 3) {
+        int e = 0;
+        PF_CUDA(cudaMemcpy(&e, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        PF_CHECK(e == 0, PF_ERR_CUDA, "the tensor-core Gram product gave up waiting for its MMAs");
+    }
     out.numiter = numiter;
     out.krylovdim = k;
     if (keep_extra >= 0) {
@@ -879,6 +893,22 @@ void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, d
     extrema_from_device(op, v0.p, maxdim, tol, eigentol, Emin, Emax, nullptr);
 }
 
+// ------------------------------------------- op-level tensor-core Gram product
+void op_gram_bf16x3(pf_handle *h, int64_t D, int nB, const double *B, int64_t ldb, const double *r, int s, double *G) {
+    PF_CHECK(h && B && r && G, PF_ERR_INVALID, "null argument");
+    PF_CHECK(D >= 1 && nB >= 1 && ldb >= nB && ldb < (1ll << 31), PF_ERR_INVALID, "invalid Gram product shape");
+    PF_CUDA(cudaSetDevice(h->device));
+    AllocStream alloc_guard(h->stream);
+    DevArray<unsigned char> work(gram_bf16_workspace(D, nB, s));
+    DevArray<int> err(1);
+    PF_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), h->stream));
+    gram_bf16x3(h, h->stream, D, nB, B, (int)ldb, r, s, G, work.p, err.p);
+    int e = 0;
+    PF_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    sync(h);
+    PF_CHECK(e == 0, PF_ERR_CUDA, "the tensor-core Gram product gave up waiting for its MMAs");
+}
+
 // ------------------------------------------------------- op-level filter
 void op_filter(pf_op *op, int dtype, double a, double b, int K, const double *coeffs, int s, const void *X,
                int64_t ldx, void *Y, int64_t ldy) {
@@ -980,7 +1010,9 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
     PF_CHECK(op && P && x0 && vals && nconv, PF_ERR_INVALID, "null argument");
     PF_CHECK(s >= 1 && nev >= 1, PF_ERR_INVALID, "s and nev must be positive");
     PF_CHECK(P->precision == PF_PREC_FP64 || P->precision == PF_PREC_MIXED, PF_ERR_INVALID, "unknown precision");
-    PF_CHECK(P->reorth_passes >= 1 && P->reorth_passes <= 2, PF_ERR_INVALID, "reorth_passes must be 1 or 2");
+    PF_CHECK(P->reorth_passes >= 1 && P->reorth_passes <= 3, PF_ERR_INVALID, "reorth_passes must be 1, 2 or 3");
+    PF_CHECK(P->reorth_passes != 3 || s <= 32, PF_ERR_UNSUPPORTED,
+             "the tensor-core reorthogonalisation (reorth_passes 3) needs s <= 32");
     pf_handle *h = op->h;
     PF_CUDA(cudaSetDevice(h->device));
     AllocStream alloc_guard(h->stream);

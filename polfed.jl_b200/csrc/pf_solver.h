@@ -36,6 +36,12 @@ void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, d
 
 extern thread_local int t_new_handle_priority;
 
+// split-BF16 Gram product on the tensor cores (pf_tc.cu)
+size_t gram_bf16_workspace(int64_t D, int nB, int s);
+void gram_bf16x3(pf_handle *h, cudaStream_t st, int64_t D, int nB, const double *B, int ldb, const double *r, int s,
+                 double *G, void *work, int *err);
+void op_gram_bf16x3(pf_handle *h, int64_t D, int nB, const double *B, int64_t ldb, const double *r, int s, double *G);
+
 // filter engine (pf_engine.cu): one step launch for every filter in flight
 void build_multi_tables(pf_op *op);
 bool multi_eligible(const pf_op *op, int dtype);

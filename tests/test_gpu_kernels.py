@@ -366,3 +366,29 @@ def test_column_slabs_give_identical_filters(pkg, orc, cuda, models, dts):
         pkg.set_filter_slab(op, 0)
         np.testing.assert_array_equal(out[4], out[-1], err_msg=name)
         np.testing.assert_array_equal(out[2], out[-1], err_msg=name)
+
+
+@pytest.mark.parametrize("D,nB,s", [(4099, 37, 5), (5000, 300, 8), (70000, 632, 16), (2048, 129, 32)])
+def test_tensor_core_gram_split_bf16(pkg, cuda, D, nB, s):
+    """pf_gram_bf16x3: G = B^T r on the tcgen05 tensor cores in split BF16
+    (three BF16 products, FP32 accumulation, chunk sums in FP64) against the
+    FP64 product; every entry within 1e-4 of |B[:, i]| |r[:, c]| (the split
+    keeps ~16 mantissa bits of each factor), far better than one BF16 product."""
+    from polfed_b200 import _lib
+    rng = np.random.default_rng(D + nB + s)
+    ldb = nB + 3                                     # a basis with spare columns, as in the solver
+    Bh = rng.standard_normal((D, ldb)) / np.sqrt(D)
+    rh = rng.standard_normal((D, s)) / np.sqrt(D)
+    B = cuda.tensor(Bh, dtype=cuda.float64, device="cuda:0")        # row-major D x ldb
+    r = cuda.tensor(rh, dtype=cuda.float64, device="cuda:0")        # row-major D x s
+    G = cuda.zeros((s, nB), dtype=cuda.float64, device="cuda:0")    # column-major nB x s
+    _lib.check(_lib.load().pf_gram_bf16x3(_lib.handle(0), D, nB, B.data_ptr(), ldb, r.data_ptr(), s, G.data_ptr()))
+    got = G.cpu().numpy().T
+    ref = Bh[:, :nB].T @ rh
+    scale = np.outer(np.linalg.norm(Bh[:, :nB], axis=0), np.linalg.norm(rh, axis=0))
+    err = np.abs(got - ref) / scale
+    assert err.max() < 1e-4, err.max()
+    # one rounding of each factor to BF16 alone is much worse
+    bf = lambda x: cuda.tensor(x).to(cuda.bfloat16).to(cuda.float64).numpy()
+    single = np.abs(bf(Bh[:, :nB]).T @ bf(rh) - ref) / scale
+    assert err.max() < 0.2 * single.max()

@@ -241,3 +241,23 @@ def test_mixed_precision_refinement(pkg, orc, cuda):
         res[passes] = (len(vm), rm.factorization.eigenresidual)
     assert res[8][0] >= 24 and res[8][0] >= res[4][0]
     assert res[8][1] < res[4][1] < 1e-6
+
+
+def test_cgs2_with_tensor_core_first_pass(pkg, orc, cuda):
+    """reorth_passes = 3: CGS2 whose first Gram product runs on the tensor
+    cores in split BF16 gives the eigenpairs of the FP64 reorthogonalisation."""
+    rng = np.random.default_rng(21)
+    f, n, c, g = pkg.qsun_parameters(8, 3, 0.75, rng=rng)
+    op = pkg.QSunOperator(8, 3, 1.0, c, n, f, g)
+    H = orc.qsun_matrix(8, 3, 1.0, c, n, f, g)
+    D = H.shape[0]
+    x0, _ = np.linalg.qr(rng.standard_normal((D, 8)))
+    probes = orc.normalized_gaussian_probes(D, 32, rng)
+    dos = pkg.DoSConfig(N=128, R=32, probes=probes)
+    v1, _ = pkg.polfed(op, x0, 40, ("rescaled", 0.3), dos=dos, vecs=False,
+                       fact=pkg.FactorizationConfig(eigentol=1e-10, overestimate_iters=2.0))
+    v3, w3 = pkg.polfed(op, x0, 40, ("rescaled", 0.3), dos=dos,
+                        fact=pkg.FactorizationConfig(eigentol=1e-10, overestimate_iters=2.0, reorth_passes=3))
+    assert len(v3) == len(v1) >= 38
+    np.testing.assert_allclose(v3, v1, rtol=1e-11, atol=1e-11)
+    _check_pairs(H, v3, w3, 1e-10)

@@ -36,6 +36,7 @@ def test_params_defaults_match_reference(pkg):
     assert p.which == _lib.PF_WHICH_LR and p.dos_N == 250 and p.dos_R == 300
     assert p.dos_kernel == _lib.KERNEL_IDS["Jackson"] and p.extrema_maxdim == 1000
     assert p.precision == _lib.PF_PREC_FP64 and p.reorth_passes == 1
+    assert p.refine == 4          # FP64 refinement passes of a mixed-precision solve
 
 
 def test_target_spec(pkg):
