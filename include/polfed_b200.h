@@ -30,6 +30,7 @@
 #ifndef POLFED_B200_H
 #define POLFED_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -87,6 +88,10 @@ typedef struct pf_op pf_op;
 
 /* ------------------------------------------------------------ library */
 int         pf_abi_version(void);
+/* sizeof(pf_params), sizeof(pf_report) and sizeof(pf_pool_stats) as this
+ * library was compiled, for bindings that mirror the structs (any pointer
+ * may be NULL). */
+void        pf_abi_sizes(size_t *params, size_t *report, size_t *pool_stats);
 const char *pf_last_error(void);
 
 int pf_handle_create(int device, pf_handle **out);
@@ -173,7 +178,8 @@ int pf_kpm_moments(pf_op *op, int dtype, double a, double b, int N, int R,
  * Times every variant of the Clenshaw step kernel for block width s and dtype
  * on scratch blocks -- 1, 2, 4, 8 or 16 columns per thread, each with five
  * (gather batch, register cap) profiles (and, for the Quantum Sun, the
- * asynchronous-gather profile of pf_set_step_variant), and for chain operators with s in
+ * asynchronous-gather and row-tile profiles of pf_set_step_variant; for
+ * sector chains the local flip-rank profile), and for chain operators with s in
  * {4, 8, 16, 32} the warp-cooperative step (width PF_WIDTH_COOP: the s lanes
  * of a warp share one row) -- keeps the fastest for this operator and returns
  * its width in *width; times_ms[i] (optional, 6 entries) receives the
@@ -210,9 +216,11 @@ int pf_set_step_width(pf_op *op, int dtype, int s, int width);
 /* Same with a profile: 0 = the width's default gather batch and register cap,
  * 1..4 = (8 gathers, 2 CTAs/SM), (8, 3), (4, 4), (8, 4); 5 = Quantum Sun
  * operators only, with 16- or 32-byte column segments: every gather of a row
- * issued at once as an asynchronous global-to-shared copy; 6 = Quantum Sun
- * operators only: each CTA stages a tile of 2^t consecutive rows in shared
- * memory and serves the grain block and the low outer-bit flips from it;
+ * issued at once as an asynchronous global-to-shared copy; 6, 8, 9 = Quantum
+ * Sun operators only, contiguous rows, s / width a power of two: each CTA
+ * stages a tile of 2^t consecutive rows (every column; 1, 2 or 4 rows per
+ * thread, at most 64 KB) in shared memory and serves the grain block and the
+ * flips of outer bits below t from it, gathering only the other flips;
  * 7 = spin chains on an Sz sector only: the rank of a state reached by a
  * flip of sites at most two apart is updated from the row's own rank (a few
  * binomial-table reads) instead of re-ranked. */
@@ -290,6 +298,10 @@ typedef struct pf_report {
     double  stage_seconds[10];
     double  basis_bytes_reserved, basis_bytes_used;
     int64_t kernel_launches;            /* this library's kernel launches in the solve */
+    int     qr_restarts;                /* Lanczos runs restarted with the host QR: the s x s work of
+                                           an iteration runs on the device, and a CholQR pass whose
+                                           Gram matrix is not positive definite (a rank-deficient
+                                           block) is redone with the host's Householder QR */
 } pf_report;
 
 void pf_params_default(pf_params *p);

@@ -29,7 +29,7 @@ PF_REPORT_MAX_CHECKS = 128
 PF_WIDTH_COOP = 0
 
 EXPORTED = [
-    "pf_abi_version", "pf_last_error", "pf_handle_create", "pf_handle_destroy", "pf_handle_stream",
+    "pf_abi_version", "pf_abi_sizes", "pf_last_error", "pf_handle_create", "pf_handle_destroy", "pf_handle_stream",
     "pf_handle_synchronize", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_destroy",
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
@@ -95,7 +95,7 @@ class pf_report(ctypes.Structure):
         ("maxresidual_history", ctypes.c_double * PF_REPORT_MAX_CHECKS),
         ("stage_seconds", ctypes.c_double * 10),
         ("basis_bytes_reserved", ctypes.c_double), ("basis_bytes_used", ctypes.c_double),
-        ("kernel_launches", ctypes.c_int64),
+        ("kernel_launches", ctypes.c_int64), ("qr_restarts", ctypes.c_int),
     ]
 
 
@@ -125,6 +125,7 @@ def load():
     vp, i32, i64, f64, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_uint64
     sig = {
         "pf_abi_version": (i32, []),
+        "pf_abi_sizes": (None, [ctypes.POINTER(ctypes.c_size_t)] * 3),
         "pf_last_error": (ctypes.c_char_p, []),
         "pf_handle_create": (i32, [i32, ctypes.POINTER(vp)]),
         "pf_handle_destroy": (i32, [vp]),

@@ -166,6 +166,7 @@ class BenchmarkReport:
     basis_bytes_used: float
     kpm_block_matvecs: int
     kernel_launches: int
+    qr_restarts: int = 0
 
 
 @dataclass
@@ -190,7 +191,8 @@ def _make_report(r: _lib.pf_report, kind: int, value: float) -> Report:
                               r.refined, r.numofchecks, list(r.converged_history[:n]), list(r.krylovdim_history[:n]),
                               list(r.maxresidual_history[:n]))
     bench = BenchmarkReport({k: r.stage_seconds[i] for i, k in enumerate(STAGES)}, r.basis_bytes_reserved,
-                            r.basis_bytes_used, int(r.kpm_block_matvecs), int(r.kernel_launches))
+                            r.basis_bytes_used, int(r.kpm_block_matvecs), int(r.kernel_launches),
+                            int(r.qr_restarts))
     return Report(spec, fac, bench)
 
 
@@ -831,8 +833,10 @@ def step_variant(op: Operator, s: int, dtype: str = "fp64"):
 def set_step_width(op: Operator, s: int, width: int, dtype: str = "fp64", profile: int = 0):
     """Pin the step-kernel variant for block width ``s`` (see ``autotune``):
     ``width`` columns per thread (0: the warp-cooperative chain step) and a
-    (gather batch, register cap) ``profile`` 0..4, or 5 (Quantum Sun only: all
-    of a row's gathers as asynchronous global-to-shared copies)."""
+    (gather batch, register cap) ``profile`` 0..4; 5 (Quantum Sun only: all
+    of a row's gathers as asynchronous global-to-shared copies); 6, 8, 9
+    (Quantum Sun only: shared-memory row tiles of 1, 2 or 4 rows per thread);
+    7 (spin chains on an Sz sector: local flip-rank updates)."""
     dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
     _lib.check(_lib.load().pf_set_step_variant(op.op, dt, int(s), int(width), int(profile)))
 

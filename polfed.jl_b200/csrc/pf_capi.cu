@@ -54,6 +54,11 @@ struct DeviceRestore {
 extern "C" {
 
 int pf_abi_version(void) { return PF_ABI_VERSION; }
+void pf_abi_sizes(size_t *params, size_t *report, size_t *pool_stats) {
+    if (params) *params = sizeof(pf_params);
+    if (report) *report = sizeof(pf_report);
+    if (pool_stats) *pool_stats = sizeof(pf_pool_stats);
+}
 
 const char *pf_last_error(void) { return pf::g_last_error.c_str(); }
 
@@ -289,13 +294,15 @@ int pf_step_variant(pf_op *op, int dtype, int s, int *width, int *gather_batch, 
 int pf_set_step_variant(pf_op *op, int dtype, int s, int width, int profile) {
     PF_API_BEGIN
     PF_CHECK(op, PF_ERR_INVALID, "null operator");
-    PF_CHECK(profile >= 0 && profile <= pf::kStepProfiles, PF_ERR_INVALID, "profile must be in 0..7");
+    PF_CHECK(profile >= 0 && profile <= pf::kStepProfiles, PF_ERR_INVALID, "profile must be in 0..9");
     PF_CHECK(width != PF_WIDTH_COOP || profile == 0, PF_ERR_INVALID, "the warp-cooperative step has no profiles");
     PF_CHECK(profile != pf::kProfileAsync || pf::qsun_async_eligible(op, s, width, dtype == PF_F64 ? 8 : 4),
              PF_ERR_INVALID,
              "asynchronous gathers (profile 5) need a Quantum Sun operator and 16- or 32-byte column segments");
-    PF_CHECK(profile != pf::kProfileTile || pf::qsun_tile_eligible(op, s, width, dtype == PF_F64 ? 8 : 4),
-             PF_ERR_INVALID, "row tiles (profile 6) need a Quantum Sun operator with at least 2^8 states");
+    PF_CHECK(pf::qsun_tile_ipt(profile) == 0 || pf::qsun_tile_eligible(op, s, width, dtype == PF_F64 ? 8 : 4, profile),
+             PF_ERR_INVALID,
+             "row tiles (profiles 6, 8, 9) need a Quantum Sun operator with at least one tile of states, a power-of-two "
+             "number of column groups and at most 64 KB per tile");
     PF_CHECK(profile != pf::kProfileLocalRank || (op->kind == pf::OP_CHAIN && op->Lup >= 0), PF_ERR_INVALID,
              "local flip-rank updates (profile 7) need a spin-chain operator on an Sz sector");
     const int st = pf_set_step_width(op, dtype, s, width);

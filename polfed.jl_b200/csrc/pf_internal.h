@@ -166,6 +166,9 @@ struct pf_op {
     // of the filter engine; shared with views
     void *d_desc64 = nullptr, *d_desc32 = nullptr;
     std::shared_ptr<void> multi_owner;
+    // Quantum Sun: the tiled step's shared-memory tables, ready-made (owned
+    // by tables_owner)
+    void *d_qtab64 = nullptr, *d_qtab32 = nullptr;
     int smem_bytes = 0;               // dynamic shared memory of the step kernels
     int slab_cols = 0;                // filter column slabs: 0 automatic, > 0 forced width, < 0 never
     // autotuned columns-per-thread of the step kernel, keyed by (element bytes, s)
@@ -209,20 +212,28 @@ void launch_step_width(pf_op *op, cudaStream_t st, int64_t D, int s, const T *q,
 int default_width(int s, int elem_bytes);
 constexpr int kCoopWidth = 0;
 // A step-kernel variant code: columns per thread V (bits 0-7) and a profile
-// (bits 8+; 0 = default gather batch and register cap, 1..kStepProfiles =
-// the tuned (batch, resident CTAs) pairs (8,2) (8,3) (4,4) (8,4), 5 =
-// asynchronous gathers and 6 = shared-memory row tiles, both Quantum Sun
-// only, 7 = local flip-rank updates, sector-basis chains only), or
-// kCoopWidth for the warp-cooperative chain step.
-constexpr int kStepProfiles = 7;
+// (bits 8+; 0 = default gather batch and register cap, 1..4 = the tuned
+// (batch, resident CTAs) pairs (8,2) (8,3) (4,4) (8,4), 5 = asynchronous
+// gathers, 6 / 8 / 9 = shared-memory row tiles of 1 / 2 / 4 rows per thread,
+// all three Quantum Sun only, 7 = local flip-rank updates, sector-basis
+// chains only), or kCoopWidth for the warp-cooperative chain step.
+constexpr int kStepProfiles = 9;
 // Profile 5: the Quantum Sun step with asynchronous (cp.async) row gathers;
-// profile 6: the Quantum Sun step over shared-memory tiles of 2^t rows;
-// profile 7: the sector-basis chain step with local flip-rank updates.
+// profiles 6, 8, 9: the Quantum Sun step over shared-memory tiles of
+// 2^t rows (one, two or four rows per thread); profile 7: the sector-basis
+// chain step with local flip-rank updates.
 constexpr int kProfileAsync = 5;
 constexpr int kProfileTile = 6;
 constexpr int kProfileLocalRank = 7;
+constexpr int kProfileTile2 = 8;
+constexpr int kProfileTile4 = 9;
 bool qsun_async_eligible(const pf_op *op, int s, int V, int elem);
-bool qsun_tile_eligible(const pf_op *op, int s, int V, int elem);
+// rows per thread of a tiled profile (0: not a tiled profile)
+int qsun_tile_ipt(int profile);
+bool qsun_tile_eligible(const pf_op *op, int s, int V, int elem, int profile);
+// Builds the tiled step's model tables (padded grain block and per-byte
+// diagonal sums) in device memory for both precisions.
+void build_qsun_tables(pf_op *op);
 constexpr int variant_code(int V, int profile) { return V | (profile << 8); }
 constexpr int variant_width(int code) { return code & 0xff; }
 constexpr int variant_profile(int code) { return code >> 8; }

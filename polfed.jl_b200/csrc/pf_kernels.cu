@@ -460,29 +460,32 @@ __global__ void __launch_bounds__(kThreads) k_step_qsun_async(const QSunDesc<T> 
 }
 
 // ------------------------------------------------------- tiled QSun step
-// Rows of a tile of 2^t consecutive states differ only in their low t bits,
-// so a flip of an outer bit below t, and the whole grain block (the low
-// L_grain bits), stay inside the tile.  Each CTA stages its tile's segment of
-// q (V columns) in shared memory with coalesced loads, then serves those
-// gathers from shared memory; only flips of the outer bits at or above t go
-// to L2.  The row sums run in qsun_row's order (flips j = 0..L_loc-1, then the
-// grain row) with the same rounded operations, so results equal every other
-// variant's.
+// A flip of outer spin j changes state bits L_grain + j and nbr[j] < L_grain,
+// so in an aligned tile of 2^t consecutive states the flips j < t - L_grain
+// and the whole grain block (the low L_grain bits) stay inside the tile.  A
+// CTA of kThreads threads owns one tile of R = IPT * kThreads / G rows (every
+// column: one contiguous run of the row-interleaved block), stages it in
+// shared memory from its threads' own-row loads, and serves the in-tile flips
+// and the grain block from there; only the L_loc - (t - L_grain) out-of-tile
+// flips gather from L2, the first batch of them in flight while the in-tile
+// flips are summed.  The model tables come ready-made from the operator
+// (k_qsun_tables), so a CTA's set-up is one coalesced copy and a grid of one
+// CTA per tile balances itself.  Each row is summed in qsun_row's order (flips
+// j = 0..L_loc-1, then the grain row) with the same rounded operations, so
+// results equal every other variant's.
 template <typename T>
 __host__ __device__ inline int qsun_tile_offset() {
     return (QSunSmem<T>::bytes(PF_MAX_GRAIN) + 63) / 64 * 64;
 }
 
-template <typename T, int V, int FLAGS>
-__global__ void __launch_bounds__(kThreads, 2) k_step_qsun_tile(const QSunDesc<T> d, const StepArgs<T> a, int tbits) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
-    constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
-    constexpr int U = 4;
-    T *sm = reinterpret_cast<T *>(smem_raw);
+template <typename T>
+__global__ void k_qsun_tables(const QSunDesc<T> d, T *__restrict__ out) {
     const int gs = d.dg + 1;
-    for (int i = threadIdx.x; i < d.dg * d.dg; i += blockDim.x) sm[(i / d.dg) * gs + (i % d.dg)] = d.grain[i];
-    T *dtab = sm + d.dg * gs;
+    for (int i = threadIdx.x; i < d.dg * gs; i += blockDim.x) {
+        const int g = i / gs, h = i - g * gs;
+        out[i] = h < d.dg ? d.grain[g * d.dg + h] : T(0);
+    }
+    T *dtab = out + d.dg * gs;
     for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) {
         const int c = i >> 8, byte = i & 255;
         T acc = T(0);
@@ -492,32 +495,62 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_qsun_tile(const QSunDesc<T
         }
         dtab[i] = acc;
     }
+}
+
+template <typename T, int V, int FLAGS, int IPT>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_step_qsun_tile(const QSunDesc<T> d, const StepArgs<T> a, const T *__restrict__ tabs, int tbits) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
+    constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
+    constexpr int U = 4;
+    T *sm = reinterpret_cast<T *>(smem_raw);
+    const int gs = d.dg + 1;
+    const int ntab = d.dg * gs + 4 * 256;
+    for (int i = threadIdx.x; i < ntab; i += blockDim.x) sm[i] = __ldg(tabs + i);
+    const T *dtab = sm + d.dg * gs;
     Pack<T, V> *tile = reinterpret_cast<Pack<T, V> *>(smem_raw + qsun_tile_offset<T>());
-    const uint32_t R = 1u << tbits;
-    const uint32_t G = (uint32_t)a.G;
-    const uint32_t ntiles = (a.D >> tbits) * G;
+    const uint32_t G = (uint32_t)a.G;   // a power of two dividing kThreads
+    const uint32_t gi = threadIdx.x & (G - 1u);
+    const int c0 = (int)gi * V;
+    const uint32_t rl0 = threadIdx.x / G, rstep = kThreads / G;
+    const int n_in = min(d.L_loc, max(0, tbits - d.L_grain));
+    const uint32_t ntiles = a.D >> tbits;
+    const T *qc = a.q + c0;
     for (uint32_t tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
-        const uint32_t r0 = (tl / G) << tbits;
-        const int c0 = (int)(tl % G) * V;
-        __syncthreads();   // the previous tile (and, the first time, the tables) is done / ready
-        for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) tile[i] = ldp<T, V>(a.q + (size_t)(r0 + i) * a.s + c0);
+        const uint32_t r0 = tl << tbits;
+        __syncthreads();   // the tables are staged / the previous tile is consumed
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const uint32_t rl = rl0 + (uint32_t)k * rstep;
+            tile[rl * G + gi] = ldp<T, V>(qc + (size_t)(r0 + rl) * a.s);
+        }
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < R; i += blockDim.x) {
-            const uint32_t row = r0 + i;
+#pragma unroll 1
+        for (int k = 0; k < IPT; ++k) {
+            const uint32_t rl = rl0 + (uint32_t)k * rstep, row = r0 + rl;
             const size_t off = (size_t)row * a.s + c0;
             if constexpr (HASX) prefetch_l1(a.x + off);
             if constexpr (HASP) prefetch_l1(a.p + off);
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (n_in + u < d.L_loc) g[u] = ldp<T, V>(qc + (size_t)(row ^ d.fmask[n_in + u]) * a.s);
             T acc[V];
 #pragma unroll
             for (int v = 0; v < V; ++v) acc[v] = T(0);
-            for (int j0 = 0; j0 < d.L_loc; j0 += U) {
-                Pack<T, V> g[U];
+            for (int j = 0; j < n_in; ++j) {
+                const Pack<T, V> t = tile[(rl ^ d.fmask[j]) * G + gi];
+                const T cf = d.cflip[j];
 #pragma unroll
-                for (int u = 0; u < U; ++u)
-                    if (j0 + u < d.L_loc) {
-                        const uint32_t nb = row ^ d.fmask[j0 + u];
-                        g[u] = ((nb ^ row) >> tbits) == 0u ? tile[nb - r0] : ldp<T, V>(a.q + (size_t)nb * a.s + c0);
-                    }
+                for (int v = 0; v < V; ++v) acc[v] = fma_t(cf, t.v[v], acc[v]);
+            }
+            for (int j0 = n_in; j0 < d.L_loc; j0 += U) {
+                if (j0 != n_in) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (j0 + u < d.L_loc) g[u] = ldp<T, V>(qc + (size_t)(row ^ d.fmask[j0 + u]) * a.s);
+                }
 #pragma unroll
                 for (int u = 0; u < U; ++u)
                     if (j0 + u < d.L_loc) {
@@ -526,11 +559,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_qsun_tile(const QSunDesc<T
                         for (int v = 0; v < V; ++v) acc[v] = fma_t(cf, g[u].v[v], acc[v]);
                     }
             }
-            const uint32_t gr = row & ((uint32_t)d.dg - 1u);
-            const uint32_t base = i - gr;
+            const uint32_t gr = rl & ((uint32_t)d.dg - 1u);
+            const uint32_t gbase = rl - gr;
             const T *grow = sm + gr * gs;
             for (int h = 0; h < d.dg; ++h) {
-                const Pack<T, V> xg = tile[base + h];
+                const Pack<T, V> xg = tile[(gbase + h) * G + gi];
                 const T w = grow[h];
 #pragma unroll
                 for (int v = 0; v < V; ++v) acc[v] = fma_t(w, xg.v[v], acc[v]);
@@ -541,7 +574,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_step_qsun_tile(const QSunDesc<T
             if (d.L_loc > 16) diag += dtab[512 + ((outer >> 16) & 0xffu)];
             if (d.L_loc > 24) diag += dtab[768 + ((outer >> 24) & 0xffu)];
             Pack<T, V> xo, po, res;
-            const Pack<T, V> qo = tile[i];
+            const Pack<T, V> qo = tile[rl * G + gi];
 #pragma unroll
             for (int v = 0; v < V; ++v) xo.v[v] = po.v[v] = T(0);
             if constexpr (HASX) xo = ldp<T, V>(a.x + off);
@@ -731,40 +764,92 @@ static bool launch_qsun_async(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, 
     }
 }
 
-// Tile of the tiled QSun step: 2^t rows with t the largest value for which
-// the tile's segment (2^t x V columns) fits in 32 KB, at most L and at least
-// L_grain; 0 when the operator is too small for a tile of 256 rows.
-static int qsun_tile_bits(int L, int seg_bytes) {
+// Rows per tile of the tiled QSun step: R = ipt * kThreads / G for G = s / V
+// column groups (a power of two dividing kThreads).  Returns log2(R), or 0
+// when the operator has no such tile: fewer states than R, a tile smaller
+// than the grain block, or more than 64 KB of tile.
+static int qsun_tile_bits(const pf_op *op, int s, int V, int elem, int ipt) {
+    if (op->kind != OP_QSUN || ipt < 1 || V < 1 || s % V != 0 || V * elem > 64) return 0;
+    const int G = s / V;
+    if ((G & (G - 1)) != 0 || G > kThreads) return 0;
+    const int64_t R = (int64_t)ipt * kThreads / G;
     int t = 0;
-    while (t < L && ((2 << t) * seg_bytes) <= 32 * 1024) ++t;
-    return t >= 8 ? t : 0;
+    while (((int64_t)1 << t) < R) ++t;
+    if (t > op->L || t < op->L_grain || R * s * elem > 64 * 1024) return 0;
+    return t;
 }
 
-bool qsun_tile_eligible(const pf_op *op, int s, int V, int elem) {
-    return op->kind == OP_QSUN && s % V == 0 && V * elem <= 64 && qsun_tile_bits(op->L, V * elem) > 0;
+int qsun_tile_ipt(int profile) {
+    return profile == kProfileTile ? 1 : profile == kProfileTile2 ? 2 : profile == kProfileTile4 ? 4 : 0;
 }
 
-template <typename T, int V, int FLAGS>
+bool qsun_tile_eligible(const pf_op *op, int s, int V, int elem, int profile) {
+    const int ipt = qsun_tile_ipt(profile);
+    return ipt > 0 && op->d_qtab64 != nullptr && qsun_tile_bits(op, s, V, elem, ipt) > 0;
+}
+
+void build_qsun_tables(pf_op *op) {
+    if (op->kind != OP_QSUN) return;
+    const int n = op->qsun64.dg * (op->qsun64.dg + 1) + 4 * 256;
+    PF_CUDA(cudaMalloc(&op->d_qtab64, n * sizeof(double)));
+    PF_CUDA(cudaMalloc(&op->d_qtab32, n * sizeof(float)));
+    cudaStream_t st = op->h->stream;
+    k_qsun_tables<double><<<1, 256, 0, st>>>(op->qsun64, static_cast<double *>(op->d_qtab64));
+    k_qsun_tables<float><<<1, 256, 0, st>>>(op->qsun32, static_cast<float *>(op->d_qtab32));
+    PF_CUDA(cudaGetLastError());
+    count_launches(2);
+    PF_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename T>
+static const T *qsun_tabs(const pf_op *op);
+template <>
+const double *qsun_tabs<double>(const pf_op *op) { return static_cast<const double *>(op->d_qtab64); }
+template <>
+const float *qsun_tabs<float>(const pf_op *op) { return static_cast<const float *>(op->d_qtab32); }
+
+template <typename T, int V, int FLAGS, int IPT>
 static void launch_qsun_tile_one(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a, int tbits) {
-    auto kern = k_step_qsun_tile<T, V, FLAGS>;
-    const int smem = qsun_tile_offset<T>() + (1 << tbits) * V * (int)sizeof(T);
+    auto kern = k_step_qsun_tile<T, V, FLAGS, IPT>;
+    if (t_refuse_spilling && spills((const void *)kern))
+        throw Error(PF_ERR_UNSUPPORTED, "step-kernel variant spills registers");
+    const int smem = qsun_tile_offset<T>() + (int)(((int64_t)1 << tbits) * a.s * (int64_t)sizeof(T));
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int64_t ntiles = ((int64_t)a.D >> tbits) * a.G;
-    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)op->h->num_sms * blocks_per_sm((const void *)kern, smem));
-    kern<<<grid, kThreads, smem, st>>>(d, a, tbits);
+    // one CTA per tile (the scheduler balances them) up to 8 waves, then a
+    // persistent loop over the tiles
+    const int64_t ntiles = (int64_t)a.D >> tbits;
+    const int64_t cap = (int64_t)op->h->num_sms * blocks_per_sm((const void *)kern, smem) * 8;
+    const int grid = (int)std::max<int64_t>(1, std::min(ntiles, cap));
+    kern<<<grid, kThreads, smem, st>>>(d, a, qsun_tabs<T>(op), tbits);
     PF_CUDA(cudaGetLastError());
     count_launches(1);
 }
 
-template <typename T, int V>
-static bool launch_qsun_tile(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a, int flags) {
+template <typename T, int V, int IPT>
+static bool launch_qsun_tile_flags(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a, int flags,
+                                   int tbits) {
     using F = StepFlags;
-    const int tbits = qsun_tile_bits(d.L, V * (int)sizeof(T));
-    if (tbits == 0) return false;
-    if (flags == (F::Q | F::P | F::X)) launch_qsun_tile_one<T, V, F::Q | F::P | F::X>(op, st, d, a, tbits);
-    else if (flags == (F::Q | F::X)) launch_qsun_tile_one<T, V, F::Q | F::X>(op, st, d, a, tbits);
+    if (flags == (F::Q | F::P | F::X)) launch_qsun_tile_one<T, V, F::Q | F::P | F::X, IPT>(op, st, d, a, tbits);
+    else if (flags == (F::Q | F::X)) launch_qsun_tile_one<T, V, F::Q | F::X, IPT>(op, st, d, a, tbits);
     else return false;
     return true;
+}
+
+// The tiled variant serves the filter's Q|P|X and Q|X steps of a Quantum Sun
+// operator on contiguous rows; false: not offered (the caller launches the
+// per-thread kernel instead).
+template <typename T, int V>
+static bool launch_qsun_tile(pf_op *op, cudaStream_t st, const QSunDesc<T> &d, const StepArgs<T> &a, int flags,
+                             int profile) {
+    const int ipt = qsun_tile_ipt(profile);
+    const int tbits = qsun_tile_bits(op, a.s, V, (int)sizeof(T), ipt);
+    if (tbits == 0 || qsun_tabs<T>(op) == nullptr) return false;
+    switch (ipt) {
+        case 1: return launch_qsun_tile_flags<T, V, 1>(op, st, d, a, flags, tbits);
+        case 2: return launch_qsun_tile_flags<T, V, 2>(op, st, d, a, flags, tbits);
+        case 4: return launch_qsun_tile_flags<T, V, 4>(op, st, d, a, flags, tbits);
+        default: return false;
+    }
 }
 
 template <typename T, int V>
@@ -783,7 +868,7 @@ static void dispatch_op(pf_op *op, cudaStream_t st, const StepArgs<T> &a, int fl
     } else if (op->kind == OP_QSUN) {
         const QSunDesc<T> &d = qsun_of<T>(op);
         if (profile == kProfileAsync && a.ld == a.s && launch_qsun_async<T, V>(op, st, d, a, flags)) return;
-        if (profile == kProfileTile && a.ld == a.s && launch_qsun_tile<T, V>(op, st, d, a, flags)) return;
+        if (qsun_tile_ipt(profile) > 0 && a.ld == a.s && launch_qsun_tile<T, V>(op, st, d, a, flags, profile)) return;
         smem = QSunSmem<T>::bytes(d.dg);
         if (flags & StepFlags::DOTS) smem = std::max(smem, dots_smem);
         dispatch_flags<T, V>(op, st, d, a, flags, smem, profile >= kProfileAsync ? 0 : profile);

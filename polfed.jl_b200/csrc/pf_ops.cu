@@ -192,8 +192,20 @@ pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double
     fill_qsun(op->qsun64, op);
     fill_qsun(op->qsun32, op);
     try {
+        build_qsun_tables(op);
+        void *t64 = op->d_qtab64, *t32 = op->d_qtab32;
+        const int dev = h->device;
+        op->tables_owner = std::shared_ptr<void>(nullptr, [t64, t32, dev](void *) {
+            cudaSetDevice(dev);
+            cudaFree(t64);
+            cudaFree(t32);
+        });
         build_multi_tables(op);
     } catch (...) {
+        if (!op->tables_owner) {
+            if (op->d_qtab64) cudaFree(op->d_qtab64);
+            if (op->d_qtab32) cudaFree(op->d_qtab32);
+        }
         delete op;
         throw;
     }
@@ -289,6 +301,8 @@ pf_op *bind_op(const pf_op *src, pf_handle *h) {
     op->tables_owner = src->tables_owner;
     op->d_desc64 = src->d_desc64;
     op->d_desc32 = src->d_desc32;
+    op->d_qtab64 = src->d_qtab64;
+    op->d_qtab32 = src->d_qtab32;
     op->multi_owner = src->multi_owner;
     op->smem_bytes = src->smem_bytes;
     op->slab_cols = src->slab_cols;

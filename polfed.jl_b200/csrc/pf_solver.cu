@@ -4,6 +4,7 @@
 #include "pf_internal.h"
 #include "pf_solver.h"
 
+#include <atomic>
 #include <exception>
 #include <thread>
 #include "pf_spectral.h"
@@ -59,6 +60,21 @@ struct DevArray {
     ~DevArray() { free(); }
     DevArray(const DevArray &) = delete;
     DevArray &operator=(const DevArray &) = delete;
+    DevArray(DevArray &&o) noexcept : p(o.p), n(o.n), st(o.st) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DevArray &operator=(DevArray &&o) noexcept {
+        if (this != &o) {
+            free();
+            p = o.p;
+            n = o.n;
+            st = o.st;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
 };
 
 // Accumulates stage times measured with CUDA events on the solve's stream.
@@ -339,6 +355,10 @@ struct LanczosOut {
     std::vector<double> res_hist;
     std::vector<double> resid;     // FP64 residual norms of the returned Ritz vectors (before the prefix)
     int refined = 0;               // pairs that met eigentol only after the FP64 refinement
+    int qr_restarts = 0;           // restarts with the host QR after a device CholQR breakdown
+    LanczosOut() = default;
+    LanczosOut(LanczosOut &&) = default;
+    LanczosOut &operator=(LanczosOut &&) = default;
 };
 
 using BlockMap = std::function<void(const double *X, double *Y)>;  // RI D x s, on h->stream
@@ -386,9 +406,117 @@ static void ascending_prefix(pf_handle *h, int64_t D, int nconv, std::vector<dou
     vals = sv;
 }
 
+// ------------------------------------------ device-side s x s block algebra
+// The small dense work of a Lanczos iteration runs in single-CTA kernels on
+// the solve's stream, so an iteration makes no host round trip: the host
+// reads the device only at convergence checks.
+
+// One CholQR pass: G = R^T R (upper R, column-major s x s) from the upper
+// triangle of G, with host_cholesky's operations in its order, each rounded
+// on its own (no fused multiply-adds), so R equals host_cholesky's bit for
+// bit; and rtot_out = R * rtot_in (rtot_in null: the identity) with the
+// host's product loop.  A pivot host_cholesky rejects sets *flag and gives
+// R = I (the triangular solve then leaves the block as it is).
+__global__ void k_small_chol(const double *__restrict__ G, int s, double *__restrict__ R,
+                             const double *__restrict__ rtot_in, double *__restrict__ rtot_out, int *flag) {
+    extern __shared__ double sh[];
+    double *g = sh, *r = sh + s * s;
+    __shared__ int bad;
+    const int n = s * s;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        g[i] = G[i];
+        r[i] = 0.0;
+    }
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    for (int j = 0; j < s; ++j) {
+        if (threadIdx.x == 0) {
+            const double gjj = g[j + j * s];
+            double d = gjj;
+            for (int k = 0; k < j; ++k) d = __dsub_rn(d, __dmul_rn(r[k + j * s], r[k + j * s]));
+            if (!(d > 1e-28 * fmax(1.0, fabs(gjj))) || !isfinite(d) || d <= 1e-13 * fabs(gjj)) bad = 1;
+            else r[j + j * s] = sqrt(d);
+        }
+        __syncthreads();
+        if (bad) break;
+        const double rjj = r[j + j * s];
+        for (int i = j + 1 + threadIdx.x; i < s; i += blockDim.x) {
+            double v = g[j + i * s];
+            for (int k = 0; k < j; ++k) v = __dsub_rn(v, __dmul_rn(r[k + j * s], r[k + i * s]));
+            r[j + i * s] = __ddiv_rn(v, rjj);
+        }
+        __syncthreads();
+    }
+    if (bad) {
+        for (int i = threadIdx.x; i < n; i += blockDim.x) r[i] = (i % (s + 1) == 0) ? 1.0 : 0.0;
+        if (threadIdx.x == 0) *flag = 1;
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+        R[idx] = r[idx];
+        const int i = idx % s, j = idx / s;
+        double v = 0.0;
+        for (int k = i; k <= j; ++k) {
+            const double t = rtot_in ? rtot_in[k + j * s] : (k == j ? 1.0 : 0.0);
+            v = __dadd_rn(v, __dmul_rn(r[i + k * s], t));
+        }
+        rtot_out[idx] = v;
+    }
+}
+
+// alpha (the overlap V^T W, s x s column-major) made symmetric from its upper
+// triangle in place, and written as the diagonal block of T at (k0, k0).
+__global__ void k_put_alpha(double *__restrict__ A, int s, double *__restrict__ T, int ldT, int k0) {
+    for (int idx = threadIdx.x; idx < s * s; idx += blockDim.x) {
+        const int i = idx % s, j = idx / s;
+        const double v = i <= j ? A[i + j * s] : A[j + i * s];
+        T[(size_t)(k0 + i) + (size_t)(k0 + j) * ldT] = v;
+        if (i > j) A[idx] = v;   // only upper entries are read
+    }
+}
+
+// beta = R (upper, s x s) written as the off-diagonal blocks of T at rows k,
+// columns k - s and their transpose, and kept for the next iteration.
+__global__ void k_put_beta(const double *__restrict__ R, int s, double *__restrict__ T, int ldT, int k,
+                           double *__restrict__ beta) {
+    for (int idx = threadIdx.x; idx < s * s; idx += blockDim.x) {
+        const int i = idx % s, j = idx / s;
+        const double v = R[idx];
+        T[(size_t)(k + i) + (size_t)(k - s + j) * ldT] = v;
+        T[(size_t)(k - s + j) + (size_t)(k + i) * ldT] = v;
+        beta[idx] = v;
+    }
+}
+
+static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
+                         int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
+                         double *stage_acc, int keep_extra, bool host_qr, bool *breakdown);
+
+// Block Lanczos with the s x s work on the device.  A CholQR pass whose
+// Gram matrix is not numerically positive definite (a rank-deficient block)
+// needs the host's Householder QR: the device pass flags it, and at its next
+// convergence check the solve restarts with the host QR, whose every
+// iteration reads the Gram matrix back (the same R bit for bit until the
+// breakdown, then the Householder factors).
 static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
                     int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
                     double *stage_acc, int keep_extra = -1) {
+    bool breakdown = false;
+    // blocks wider than 64 columns (a Gram matrix beyond one CTA's shared
+    // memory) always take the host QR
+    lanczos_pass(op, s, howmany, maxdim_req, tol, eigentol, which, reorth_passes, x0_ri, fmap, out, stage_acc,
+                 keep_extra, s > 64, &breakdown);
+    if (!breakdown) return;
+    LanczosOut again;
+    lanczos_pass(op, s, howmany, maxdim_req, tol, eigentol, which, reorth_passes, x0_ri, fmap, again, stage_acc,
+                 keep_extra, true, nullptr);
+    again.qr_restarts = 1;
+    out = std::move(again);
+}
+
+static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
+                         int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
+                         double *stage_acc, int keep_extra, bool host_qr, bool *breakdown) {
     pf_handle *h = op->h;
     const int64_t D = op->dim;
     cudaStream_t st = h->stream;
@@ -405,59 +533,79 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     DevArray<double> basis((size_t)D * maxdim);
     DevArray<double> bufs((size_t)D * s * 3);
     double *vlast = bufs.p, *vprev = bufs.p + (size_t)D * s, *r = bufs.p + 2 * (size_t)D * s;
-    DevArray<double> smallA((size_t)s * s), smallB((size_t)s * s), G((size_t)maxdim * s);
+    const size_t ss = (size_t)s * s;
+    // small device state: alpha, the pass's R, two running products, beta,
+    // the Gram matrix, the breakdown flag
+    DevArray<double> small(6 * ss), G((size_t)maxdim * s);
+    double *dA = small.p, *dR = dA + ss, *dRt0 = dR + ss, *dRt1 = dRt0 + ss, *dBeta = dRt1 + ss, *dG = dBeta + ss;
+    DevArray<int> dflag(1);
+    PF_CUDA(cudaMemsetAsync(dflag.p, 0, sizeof(int), st));
+    DevArray<double> Tfull((size_t)maxdim * maxdim);   // the projected matrix, column-major
+    PF_CUDA(cudaMemsetAsync(Tfull.p, 0, (size_t)maxdim * maxdim * sizeof(double), st));
+    PF_CUDA(cudaMemsetAsync(dBeta, 0, ss * sizeof(double), st));
     DevArray<unsigned char> tc_work(reorth_passes == 3 ? gram_bf16_workspace(D, maxdim, s) : 0);
     DevArray<int> tc_err(reorth_passes == 3 ? 1 : 0);
     if (reorth_passes == 3) PF_CUDA(cudaMemsetAsync(tc_err.p, 0, sizeof(int), st));
-    std::vector<double> T((size_t)maxdim * maxdim, 0.0);  // column-major
-    std::vector<double> hA((size_t)s * s), hR, hR1, hR2, beta_last((size_t)s * s, 0.0);
+    std::vector<double> hR;
     const double one = 1.0, zero = 0.0, mone = -1.0;
     const int ldb = maxdim;  // row stride of the basis
     StageClock clk(st, stage_acc);
-    // staging regions; each is rewritten only after a sync(h) that follows
-    // the copy which last used it
-    const size_t ss = (size_t)s * s;
-    double *pin = pinned_scratch(h, 5 * ss + (size_t)maxdim * maxdim + (size_t)maxdim * (s + 3) + 8);
-    double *pinA = pin, *pinG = pinA + ss, *pinR = pinG + ss, *pinO1 = pinR + ss, *pinO2 = pinO1 + ss;
-    double *pinT = pinO2 + ss;                          // maxdim x maxdim
-    double *pinLam = pinT + (size_t)maxdim * maxdim;    // maxdim
+    // page-locked staging for the checks (rewritten only after the sync that
+    // follows the copies which last used it)
+    double *pin = pinned_scratch(h, 3 * ss + (size_t)maxdim * (s + 3) + 8);
+    double *pinG = pin, *pinR = pinG + ss, *pinB = pinR + ss;
+    double *pinLam = pinB + ss;                         // maxdim
     double *pinTail = pinLam + maxdim;                  // s x maxdim
     double *pinE = pinTail + (size_t)s * maxdim;        // maxdim
     double *pinRes = pinE + maxdim;                     // maxdim
-    int *pinInfo = reinterpret_cast<int *>(pinRes + maxdim);
+    int *pinInfo = reinterpret_cast<int *>(pinRes + maxdim);   // [info, breakdown flag]
+    const int small_smem = (int)(2 * ss * sizeof(double));
+    if (!host_qr && small_smem > 48 * 1024)
+        PF_CUDA(cudaFuncSetAttribute(k_small_chol, cudaFuncAttributeMaxDynamicSharedMemorySize, small_smem));
 
     auto append = [&](const double *src, int col) {
         PF_CUDA(cudaMemcpy2DAsync(basis.p + col, (size_t)ldb * sizeof(double), src, (size_t)s * sizeof(double),
                                   (size_t)s * sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
     };
-    // alpha = V^T W (s x s, column-major) -> host, upper-triangle symmetrised
-    auto overlap = [&](const double *Vb, const double *Wb) {
-        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, Vb, s, Wb, s, &zero, smallA.p, s));
-        PF_CUDA(cudaMemcpyAsync(pinA, smallA.p, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
-        sync(h);
-        std::memcpy(hA.data(), pinA, ss * sizeof(double));
-        for (int j = 0; j < s; ++j)
-            for (int i = j + 1; i < s; ++i) hA[i + j * s] = hA[j + i * s];  // Hermitian(alpha): upper
+    // alpha = V^T W (s x s), upper triangle symmetrised, into T at (k0, k0)
+    auto overlap = [&](const double *Vb, const double *Wb, int k0) {
+        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, Vb, s, Wb, s, &zero, dA, s));
+        k_put_alpha<<<1, 256, 0, st>>>(dA, s, Tfull.p, maxdim, k0);
+        PF_CUDA(cudaGetLastError());
+        count_launches(1);
     };
-    // Q R = W in place (CholQR2; Householder on the host if it breaks down)
-    auto qr_inplace = [&](double *W, std::vector<double> &Rout) {
+    // Q R = W in place (CholQR2) on the device; R ends in dRt1
+    auto qr_device = [&](double *W) {
+        for (int pass = 0; pass < 2; ++pass) {
+            PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, dG, s));
+            k_small_chol<<<1, 64, small_smem, st>>>(dG, s, dR, pass == 0 ? nullptr : dRt0, pass == 0 ? dRt0 : dRt1,
+                                                   dflag.p);
+            PF_CUDA(cudaGetLastError());
+            count_launches(1);
+            // W^T <- R^{-T} W^T  (i.e. W <- W R^{-1})
+            PF_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, s,
+                                  (int)D, &one, dR, s, W, s));
+        }
+    };
+    // Q R = W in place with the Gram matrices read back (CholQR2; Householder
+    // on the host if it breaks down); R ends in dRt1
+    auto qr_host = [&](double *W) {
         std::vector<double> Rtot((size_t)s * s, 0.0);
         for (int i = 0; i < s; ++i) Rtot[i + i * s] = 1.0;
         bool ok = true;
         for (int pass = 0; pass < 2 && ok; ++pass) {
-            PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, smallA.p, s));
+            PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, dG, s));
             std::vector<double> hG((size_t)s * s), Rp;
-            PF_CUDA(cudaMemcpyAsync(pinG, smallA.p, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(pinG, dG, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
             sync(h);
             std::memcpy(hG.data(), pinG, ss * sizeof(double));
             for (int j = 0; j < s; ++j)
                 for (int i = j + 1; i < s; ++i) hG[i + j * s] = hG[j + i * s];
             if (!host_cholesky(hG, s, Rp)) { ok = false; break; }
             std::memcpy(pinR, Rp.data(), ss * sizeof(double));
-            PF_CUDA(cudaMemcpyAsync(smallB.p, pinR, ss * sizeof(double), cudaMemcpyHostToDevice, st));
-            // W^T <- R^{-T} W^T  (i.e. W <- W R^{-1})
+            PF_CUDA(cudaMemcpyAsync(dR, pinR, ss * sizeof(double), cudaMemcpyHostToDevice, st));
             PF_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, s,
-                                  (int)D, &one, smallB.p, s, W, s));
+                                  (int)D, &one, dR, s, W, s));
             // Rtot <- Rp * Rtot
             std::vector<double> Rn((size_t)s * s, 0.0);
             for (int j = 0; j < s; ++j)
@@ -467,6 +615,7 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
                     Rn[i + j * s] = v;
                 }
             Rtot.swap(Rn);
+            sync(h);   // pinR is rewritten by the next pass
         }
         if (!ok) {
             std::vector<double> hW((size_t)D * s);
@@ -475,7 +624,9 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
             host_householder_qr(hW, D, s, Rtot);
             PF_CUDA(cudaMemcpyAsync(W, hW.data(), hW.size() * sizeof(double), cudaMemcpyHostToDevice, st));
         }
-        Rout.swap(Rtot);
+        std::memcpy(pinR, Rtot.data(), ss * sizeof(double));
+        PF_CUDA(cudaMemcpyAsync(dRt1, pinR, ss * sizeof(double), cudaMemcpyHostToDevice, st));
+        sync(h);
     };
 
     // ---- lanczositer (Factorization.jl:50-67)
@@ -488,13 +639,9 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
         fmap(vlast, r);
         clk.add(1, e0, clk.mark());
     }
-    overlap(vlast, r);
-    for (int j = 0; j < s; ++j)
-        for (int i = 0; i < s; ++i) T[(size_t)i + (size_t)j * maxdim] = hA[i + j * s];
-    std::memcpy(pinO1, hA.data(), ss * sizeof(double));
-    PF_CUDA(cudaMemcpyAsync(smallA.p, pinO1, ss * sizeof(double), cudaMemcpyHostToDevice, st));
+    overlap(vlast, r, 0);
     // r^T -= alpha^T x0^T
-    PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, smallA.p, s, vlast, s, &one, r, s));
+    PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, dA, s, vlast, s, &one, r, s));
     int numiter = 1;
 
     // eigen workspace
@@ -510,14 +657,11 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
     while (true) {
         // 1 tridiagonalization: QR(r) -> beta (BlockLanczosFactorization.jl:115-131)
         cudaEvent_t e0 = clk.mark();
-        qr_inplace(r, hR);
-        clk.flush();
-        for (int j = 0; j < s; ++j)
-            for (int i = 0; i < s; ++i) {
-                T[(size_t)(k + i) + (size_t)(k - s + j) * maxdim] = hR[i + j * s];
-                T[(size_t)(k - s + j) + (size_t)(k + i) * maxdim] = hR[i + j * s];
-            }
-        beta_last = hR;
+        if (host_qr) qr_host(r);
+        else qr_device(r);
+        k_put_beta<<<1, 256, 0, st>>>(dRt1, s, Tfull.p, maxdim, k, dBeta);
+        PF_CUDA(cudaGetLastError());
+        count_launches(1);
         std::swap(vprev, vlast);
         std::swap(vlast, r);  // vlast <- Q ; r <- old vprev storage
         append(vlast, k);
@@ -529,18 +673,12 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
         cudaEvent_t e2 = clk.mark();
         clk.add(1, e1, e2);
         // 3 overlap
-        overlap(vlast, r);
-        for (int j = 0; j < s; ++j)
-            for (int i = 0; i < s; ++i) T[(size_t)(k - s + i) + (size_t)(k - s + j) * maxdim] = hA[i + j * s];
+        overlap(vlast, r, k - s);
         cudaEvent_t e3 = clk.mark();
         clk.add(2, e2, e3);
         // 4 orthogonalization: r -= vlast alpha + vprev beta^T  (orthogonalization.jl:31-33)
-        std::memcpy(pinO1, hA.data(), ss * sizeof(double));
-        std::memcpy(pinO2, beta_last.data(), ss * sizeof(double));
-        PF_CUDA(cudaMemcpyAsync(smallA.p, pinO1, ss * sizeof(double), cudaMemcpyHostToDevice, st));
-        PF_CUDA(cudaMemcpyAsync(smallB.p, pinO2, ss * sizeof(double), cudaMemcpyHostToDevice, st));
-        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, smallA.p, s, vlast, s, &one, r, s));
-        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, s, (int)D, s, &mone, smallB.p, s, vprev, s, &one, r, s));
+        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, dA, s, vlast, s, &one, r, s));
+        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, s, (int)D, s, &mone, dBeta, s, vprev, s, &one, r, s));
         cudaEvent_t e4 = clk.mark();
         clk.add(3, e3, e4);
         // 5 reorthogonalization: r -= B (B^T r), B = all but the last two blocks
@@ -565,22 +703,27 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
         // convergence (ConvergenceInfo.jl:63-130)
         numiter += 1;
         if (nextcheck == numiter || numiter >= maxiter) {
-            // projected matrix, upper triangle is authoritative (Hermitian view)
-            double *Tk = pinT;
-            for (int j = 0; j < k; ++j)
-                for (int i = 0; i < k; ++i) {
-                    const int a = std::min(i, j), b2 = std::max(i, j);
-                    Tk[(size_t)i + (size_t)j * k] = T[(size_t)a + (size_t)b2 * maxdim];
-                }
-            PF_CUDA(cudaMemcpyAsync(dT.p, Tk, (size_t)k * k * sizeof(double), cudaMemcpyHostToDevice, st));
+            // the projected matrix's leading k x k block (upper triangle read)
+            PF_CUDA(cudaMemcpy2DAsync(dT.p, (size_t)k * sizeof(double), Tfull.p, (size_t)maxdim * sizeof(double),
+                                      (size_t)k * sizeof(double), k, cudaMemcpyDeviceToDevice, st));
             PF_CUSOLVER(cusolverDnDsyevd(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, dT.p, k, dW.p,
                                          dwork.p, lwork, dinfo.p));
             PF_CUDA(cudaMemcpyAsync(pinLam, dW.p, k * sizeof(double), cudaMemcpyDeviceToHost, st));
             PF_CUDA(cudaMemcpy2DAsync(pinTail, s * sizeof(double), dT.p + (k - s), (size_t)k * sizeof(double),
                                       s * sizeof(double), k, cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(pinB, dBeta, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
             PF_CUDA(cudaMemcpyAsync(pinInfo, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(pinInfo + 1, dflag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             sync(h);
+            if (pinInfo[1] != 0) {
+                // a device CholQR pass broke down since the last check
+                PF_CHECK(breakdown != nullptr, PF_ERR_NUMERIC, "CholQR breakdown in the host-QR pass");
+                *breakdown = true;
+                clk.flush();
+                return;
+            }
             std::vector<double> lam(pinLam, pinLam + k), tail(pinTail, pinTail + (size_t)s * k);
+            std::vector<double> beta_last(pinB, pinB + ss);
             const int info = *pinInfo;
             PF_CHECK(info == 0, PF_ERR_NUMERIC, "projected eigenproblem failed to converge");
             std::vector<int> idx(k);
@@ -594,13 +737,13 @@ static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, d
             const int nwant = std::min(howmany, k);
             for (int i = 0; i < nwant; ++i) {
                 const int pos = idx[i];
-                double ss = 0.0;
+                double ss2 = 0.0;
                 for (int a = 0; a < s; ++a) {
                     double v = 0.0;
                     for (int b2 = 0; b2 < s; ++b2) v += beta_last[a + b2 * s] * tail[b2 + (size_t)pos * s];
-                    ss += v * v;
+                    ss2 += v * v;
                 }
-                const double res = std::sqrt(ss);
+                const double res = std::sqrt(ss2);
                 if (res > maxres || std::isnan(res)) maxres = std::isnan(res) ? res : std::max(maxres, res);
                 if (maxres < tol) ++conv;
             }
@@ -824,7 +967,7 @@ static pf_handle *aux_handle(pf_handle *h) {
 }
 
 static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, double tol, double eigentol, double *Emin,
-                                double *Emax, double *stage_acc) {
+                                double *Emax, double *stage_acc, int *qr_restarts = nullptr) {
     const int64_t D = op->dim;
     // The :SR probe runs here and the :LR probe at the same time on the
     // auxiliary handle (its own stream, cuBLAS and cuSOLVER): both only read
@@ -835,7 +978,7 @@ static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, dou
     PF_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
     PF_CUDA(cudaEventRecord(ready, op->h->stream));
     PF_CUDA(cudaStreamWaitEvent(ah->stream, ready, 0));
-    auto probe = [&](pf_op *o, int which, double *out) {
+    auto probe = [&](pf_op *o, int which, double *out) -> int {
         BlockMap happly = [&](const double *X, double *Y) {
             launch_step<double>(o, o->h->stream, D, 1, X, nullptr, nullptr, Y, 0, 1.0, 0, 1.0, 0.0, StepFlags::Q,
                                 nullptr);
@@ -845,7 +988,9 @@ static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, dou
         lanczos(o, 1, 1, maxdim, tol, eigentol, which, 1, v0_dev, happly, lo, stage_acc ? dummy : nullptr);
         PF_CHECK(lo.nconv >= 1, PF_ERR_NUMERIC, "Failed to estimate extremal eigenvalue with Lanczos.");
         *out = which == PF_WHICH_SR ? lo.vals.front() : lo.vals.back();
+        return lo.qr_restarts;
     };
+    std::atomic<int> restarts{0};
     std::exception_ptr aux_err;
     int64_t aux_launches = 0;
     double hi = 0.0;
@@ -854,7 +999,7 @@ static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, dou
             PF_CUDA(cudaSetDevice(ah->device));
             AllocStream guard(ah->stream);
             const int64_t before = thread_launches();
-            probe(view.get(), PF_WHICH_LR, &hi);
+            restarts += probe(view.get(), PF_WHICH_LR, &hi);
             aux_launches = thread_launches() - before;
         } catch (...) {
             aux_err = std::current_exception();
@@ -863,7 +1008,7 @@ static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, dou
     std::exception_ptr err;
     double lo = 0.0;
     try {
-        probe(op, PF_WHICH_SR, &lo);
+        restarts += probe(op, PF_WHICH_SR, &lo);
     } catch (...) {
         err = std::current_exception();
     }
@@ -874,6 +1019,7 @@ static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, dou
     if (aux_err) std::rethrow_exception(aux_err);
     *Emin = lo;
     *Emax = hi;
+    if (qr_restarts) *qr_restarts += restarts.load();
 }
 
 void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, double eigentol, double *Emin,
@@ -1050,7 +1196,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
             double lo = 0, hi = 0;
             // v0 = x0[:, 1] (column 0 of the column-major copy)
             extrema_from_device(op, xcm.p, P->extrema_maxdim > 0 ? P->extrema_maxdim : 1000, 1e-14, 1e-8, &lo, &hi,
-                                nullptr);
+                                nullptr, &R.qr_restarts);
             if (!P->has_Emin) Emin = lo;
             if (!P->has_Emax) Emax = hi;
         }
@@ -1241,6 +1387,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
         R.basis_bytes_reserved = (double)D * out.maxiter * s * sizeof(double);
         R.basis_bytes_used = (double)D * out.krylovdim * sizeof(double);
         R.kernel_launches = thread_launches() - launches0;
+        R.qr_restarts += out.qr_restarts;
         *rep = R;
     }
 }

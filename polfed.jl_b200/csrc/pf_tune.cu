@@ -7,7 +7,9 @@
 // warp-cooperative step).  Each width comes in five profiles: the default
 // gather batch and register cap, and the (gather batch U, resident CTAs per
 // SM) pairs (8, 2), (8, 3), (4, 4), (8, 4) -- more independent gathers per
-// thread against more resident warps.  The best choice depends on the model,
+// thread against more resident warps.  Quantum Sun operators add the
+// asynchronous-gather step and the shared-memory row-tile steps (tiles of
+// 1, 2 or 4 rows per thread); sector chains add the local flip-rank step.  The best choice depends on the model,
 // s, dtype and D, so it is measured: every variant runs the recurrence step
 // (the filter's dominant launch) on scratch blocks, timed with CUDA events on
 // the handle's stream, and the fastest is kept on the operator.  Every
@@ -137,7 +139,7 @@ static int tune_typed(pf_op *op, int s, std::vector<std::pair<int, float>> *timi
             if (s % V == 0)
                 for (int prof = 0; prof <= kStepProfiles; ++prof)
                     if ((prof != kProfileAsync || qsun_async_eligible(op, s, V, (int)sizeof(T))) &&
-                        (prof != kProfileTile || qsun_tile_eligible(op, s, V, (int)sizeof(T))) &&
+                        (qsun_tile_ipt(prof) == 0 || qsun_tile_eligible(op, s, V, (int)sizeof(T), prof)) &&
                         (prof != kProfileLocalRank || (op->kind == OP_CHAIN && op->Lup >= 0)))
                         codes.push_back(variant_code(V, prof));
         if (coop_eligible(op, s, StepFlags::Q | StepFlags::P | StepFlags::X)) codes.push_back(kCoopWidth);
@@ -215,7 +217,7 @@ void variant_params(int code, int elem, int *V, int *U, int *MB) {
     static const int prof_u[5] = {0, 8, 8, 4, 8}, prof_mb[5] = {0, 2, 3, 4, 4};
     if (prof >= 1 && prof <= 4) *U = prof_u[prof], *MB = prof_mb[prof];
     if (prof == kProfileAsync) *U = 0, *MB = 0;   // every gather of a row at once
-    if (prof == kProfileTile) *U = 4, *MB = 2;
+    if (qsun_tile_ipt(prof) > 0) *U = 4, *MB = 2;
 }
 
 bool cached_step_variant(pf_op *op, int s, int dtype) {

@@ -304,6 +304,17 @@ def test_operator_errors(pkg, cuda):
         pkg.QSunOperator(4, 2, 1.0, [1.0] * 4, [0, 1, 2, 0], [1.0] * 4, np.eye(4)).op
 
 
+def _tile_ok(op, s, width, elem, ipt):
+    """The tiled Quantum Sun step's rule: s / width column groups (a power of
+    two), tiles of ipt * 256 / groups rows within the operator and at least
+    one grain block, at most 64 KB of tile."""
+    groups = s // width
+    if s % width or groups & (groups - 1):
+        return False
+    rows = ipt * 256 // groups
+    return 2 ** op.L_grain <= rows <= op.dim and rows * s * elem <= 64 * 1024
+
+
 @pytest.mark.parametrize("dts", ["fp64", "fp32"])
 def test_every_step_variant_gives_identical_results(pkg, orc, cuda, models, dts):
     """The autotuner picks among columns-per-thread widths and (gather batch,
@@ -326,8 +337,9 @@ def test_every_step_variant_gives_identical_results(pkg, orc, cuda, models, dts)
             profiles = list(range(5))
             if op.kind == "qsun" and width * elem in (16, 32):
                 profiles.append(5)                # asynchronous gathers
-            if op.kind == "qsun" and op.dim >= 256:
-                profiles.append(6)                # shared-memory row tiles
+            for profile, ipt in ((6, 1), (8, 2), (9, 4)):   # shared-memory row tiles
+                if op.kind == "qsun" and _tile_ok(op, s, width, elem, ipt):
+                    profiles.append(profile)
             if op.kind == "spin_chain" and op.Lup >= 0:
                 profiles.append(7)                # local flip-rank updates
             for profile in profiles:
@@ -341,6 +353,32 @@ def test_every_step_variant_gives_identical_results(pkg, orc, cuda, models, dts)
                 else:
                     np.testing.assert_array_equal(got, ref, err_msg=f"{name} width={width} profile={profile}")
         pkg.set_step_width(op, s, min(8, 64 // elem), dts)
+
+
+@pytest.mark.parametrize("dts", ["fp64", "fp32"])
+def test_tiled_qsun_step_large(pkg, cuda, dts):
+    """At D = 2^19 the tiled Quantum Sun steps have more tiles than CTAs (the
+    persistent loop over tiles) and out-of-tile flips to every high bit; a
+    K = 6 filter equals the default kernel's bit for bit."""
+    dt = cuda.float64 if dts == "fp64" else cuda.float32
+    elem = 8 if dts == "fp64" else 4
+    s = 8
+    rng = np.random.default_rng(19)
+    fq, nq, cq, gq = pkg.qsun_parameters(16, 3, 0.75, rng=rng)
+    op = pkg.QSunOperator(16, 3, 1.0, cq, nq, fq, gq)
+    D = op.dim
+    X = cuda.randn(s, D, dtype=dt, device="cuda:0", generator=cuda.Generator("cuda:0").manual_seed(3)).t()
+    coeffs = np.array([0.3, -0.2, 0.15, 0.1, -0.05, 0.02, 0.01])
+    width = 4 if elem == 8 else 8
+    outs = {}
+    for profile in (0, 6, 8, 9):
+        pkg.set_step_width(op, s, width, dts, profile=profile)
+        Y = pkg.col_major(D, s, dtype=dt)
+        pkg.chebyshev_filter(op, Y, X, coeffs, a=40.0, b=0.0)
+        outs[profile] = Y.cpu()
+    for profile in (6, 8, 9):
+        assert cuda.equal(outs[profile], outs[0]), f"profile {profile}"
+    assert cuda.isfinite(outs[0]).all()
 
 
 @pytest.mark.parametrize("dts", ["fp64", "fp32"])

@@ -261,3 +261,36 @@ def test_cgs2_with_tensor_core_first_pass(pkg, orc, cuda):
     assert len(v3) == len(v1) >= 38
     np.testing.assert_allclose(v3, v1, rtol=1e-11, atol=1e-11)
     _check_pairs(H, v3, w3, 1e-10)
+
+
+@pytest.mark.parametrize("s", [1, 2])
+def test_block_breakdown_restarts_with_the_host_qr(pkg, orc, cuda, s):
+    """The s x s work of an iteration runs on the device; a CholQR pass whose
+    Gram matrix is not positive definite is flagged there and the run restarts
+    with the host QR (Householder, like the reference's qr).  A starting block
+    of eigenvectors spans an invariant subspace, so the first residual block
+    vanishes in the extremal probes and in the filtered Lanczos alike: the
+    solve restarts and still returns the eigenpairs nearest the target.  From
+    a random start nothing restarts."""
+    L = 10
+    rng = np.random.default_rng(5)
+    f = 3 * (2 * rng.random(L) - 1)
+    op = pkg.xxz_hamiltonian(L, L // 2, 1.0, 1.0, 0.0, fields=f)
+    H = orc.xxz_matrix(L, L // 2, 1.0, 1.0, f)
+    ev, U = np.linalg.eigh(H.toarray())
+    nev = 6
+    x0 = U[:, 0].copy() if s == 1 else U[:, :s].copy()
+    dos = pkg.DoSConfig(N=96, R=24, seed=3)
+    vals, vecs, rep = pkg.polfed(op, x0, nev, ("rescaled", 0.5), produce_report=True, dos=dos)
+    assert rep.benchmark.qr_restarts >= 1
+    assert abs(rep.spectral.Emin - ev[0]) < 1e-9 * abs(ev[0])
+    assert abs(rep.spectral.Emax - ev[-1]) < 1e-9 * abs(ev[-1])
+    _check_pairs(H, vals, vecs, 1e-9)
+    target = ev[0] + 0.5 * (ev[-1] - ev[0])
+    nearest = np.sort(ev[np.argsort(np.abs(ev - target))[:nev]])
+    assert len(vals) == nev
+    np.testing.assert_allclose(vals, nearest, rtol=1e-10, atol=1e-10)
+    x1, _ = np.linalg.qr(rng.standard_normal((H.shape[0], s)))
+    vals1, _, rep1 = pkg.polfed(op, x1[:, 0] if s == 1 else x1, nev, ("rescaled", 0.5), produce_report=True, dos=dos)
+    assert rep1.benchmark.qr_restarts == 0
+    np.testing.assert_allclose(vals1, nearest, rtol=1e-10, atol=1e-10)

@@ -26,6 +26,17 @@ def test_library_exports_every_declared_symbol(pkg):
     assert lib.pf_abi_version() == 1
 
 
+def test_struct_mirrors_match_the_library(pkg):
+    """The ctypes mirrors of pf_params, pf_report and pf_pool_stats have the
+    library's own sizes (a field added on one side only shows here)."""
+    from polfed_b200 import _lib
+    sz = [ctypes.c_size_t() for _ in range(3)]
+    _lib.load().pf_abi_sizes(*[ctypes.byref(x) for x in sz])
+    assert sz[0].value == ctypes.sizeof(_lib.pf_params)
+    assert sz[1].value == ctypes.sizeof(_lib.pf_report)
+    assert sz[2].value == ctypes.sizeof(_lib.pf_pool_stats)
+
+
 def test_params_defaults_match_reference(pkg):
     from polfed_b200 import _lib
     p = _lib.pf_params()
