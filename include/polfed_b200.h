@@ -99,6 +99,11 @@ int pf_handle_destroy(pf_handle *h);
 /* The handle's cudaStream_t, for callers that order their own work with it. */
 int pf_handle_stream(pf_handle *h, void **stream);
 int pf_handle_synchronize(pf_handle *h);
+/* on != 0 (the default): the handle's step kernels launch with programmatic
+ * dependent launch -- a step's launch and shared-memory table set-up overlap
+ * the previous step's tail, and it waits for that step's writes before
+ * reading any block; 0: plain stream order.  Results are identical. */
+int pf_handle_set_overlap(pf_handle *h, int on);
 
 /* ---------------------------------------------------------- operators */
 /* Spin-1/2 chain  H = sum_b J_b (S+_i S-_j + h.c.)/2 + J_b Delta_b Sz_i Sz_j
@@ -266,6 +271,10 @@ typedef struct pf_params {
                                     and runs a Rayleigh-Ritz step with the FP64 H on them; passes stop
                                     once all nev targets meet eigentol. */
     int    autotune;             /* 1: time the step-kernel variants once per (op, s, dtype) */
+    int    host_qr;              /* 0: the s x s algebra of a Lanczos iteration stays on the device
+                                    (a CholQR breakdown restarts the run with the host QR); 1: every
+                                    iteration reads its Gram matrices back and factors them on the
+                                    host (the same R bit for bit; Householder QR on a breakdown) */
 } pf_params;
 
 #define PF_REPORT_MAX_CHECKS 128

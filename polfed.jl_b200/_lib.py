@@ -30,7 +30,7 @@ PF_WIDTH_COOP = 0
 
 EXPORTED = [
     "pf_abi_version", "pf_abi_sizes", "pf_last_error", "pf_handle_create", "pf_handle_destroy", "pf_handle_stream",
-    "pf_handle_synchronize", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_destroy",
+    "pf_handle_synchronize", "pf_handle_set_overlap", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_destroy",
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
     "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind", "pf_set_step_width",
@@ -76,6 +76,7 @@ class pf_params(ctypes.Structure):
         ("dos_kernel", ctypes.c_int), ("probe_kind", ctypes.c_int), ("seed", ctypes.c_uint64),
         ("probes", ctypes.c_void_p), ("precision", ctypes.c_int), ("reorth_passes", ctypes.c_int),
         ("extrema_maxdim", ctypes.c_int), ("refine", ctypes.c_int), ("autotune", ctypes.c_int),
+        ("host_qr", ctypes.c_int),
     ]
 
 
@@ -131,6 +132,7 @@ def load():
         "pf_handle_destroy": (i32, [vp]),
         "pf_handle_stream": (i32, [vp, ctypes.POINTER(vp)]),
         "pf_handle_synchronize": (i32, [vp]),
+        "pf_handle_set_overlap": (i32, [vp, i32]),
         "pf_op_spin_chain_create": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_qsun_create": (i32, [vp, i32, i32, f64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_destroy": (i32, [vp]),

@@ -59,13 +59,17 @@ class FactorizationConfig:
     """FactorizationConfig.jl:49-70 (PolfedDefaults.jl:151-191).
     ``reorth_passes`` 1 is the reference's FullRO; 2 is CGS2 in FP64; 3 is CGS2
     with its first Gram product on the tensor cores in split BF16.  ``refine_passes``:
-    FP64 refinement passes of a ``precision="mixed"`` solve (0: none)."""
+    FP64 refinement passes of a ``precision="mixed"`` solve (0: none).
+    ``host_qr``: factor every iteration's Gram matrices on the host instead of
+    the device (the same results; the device form restarts with it when a
+    block breaks down)."""
     which: str = "LR"
     tol: float = 1e-14
     eigentol: float = 1e-9
     overestimate_iters: float = 1.25
     reorth_passes: int = 1
     refine_passes: int = 4
+    host_qr: bool = False
 
 
 @dataclass
@@ -251,6 +255,7 @@ def _params(op: Operator, howmany: int, target, mapping: MappingConfig, transfor
     p.eigentol = fact.eigentol
     p.overestimate_iters = fact.overestimate_iters
     p.reorth_passes = int(fact.reorth_passes)
+    p.host_qr = 1 if fact.host_qr else 0
     p.refine = int(fact.refine_passes)
     p.dos_N, p.dos_R = int(dos.N), int(dos.R)
     if dos.kernel not in _lib.KERNEL_IDS:
@@ -818,6 +823,13 @@ def set_filter_slab(op: Operator, cols: int = 0):
     """Filter column slabs: ``cols`` > 0 filters in slabs of that many columns
     (a divisor of s); <= 0 whole blocks (the default).  Results are unchanged."""
     _lib.check(_lib.load().pf_set_filter_slab(op.op, int(cols)))
+
+
+def set_launch_overlap(on: bool = True, device: int = 0):
+    """Programmatic dependent launch of the step kernels on the device's
+    default handle (on by default): each step's launch and table set-up
+    overlap the previous step's tail.  Results are identical either way."""
+    _lib.check(_lib.load().pf_handle_set_overlap(_lib.handle(device), 1 if on else 0))
 
 
 def step_variant(op: Operator, s: int, dtype: str = "fp64"):

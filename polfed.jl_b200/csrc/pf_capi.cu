@@ -135,6 +135,13 @@ int pf_handle_synchronize(pf_handle *h) {
     PF_API_END
 }
 
+int pf_handle_set_overlap(pf_handle *h, int on) {
+    PF_API_BEGIN
+    PF_CHECK(h, PF_ERR_INVALID, "null handle");
+    h->overlap = on != 0;
+    PF_API_END
+}
+
 int pf_op_spin_chain_create(pf_handle *h, int L, int Lup, int nbonds, const int32_t *bonds, const double *J,
                             const double *Delta, const double *fields, pf_op **out) {
     PF_API_BEGIN
@@ -361,6 +368,7 @@ void pf_params_default(pf_params *p) {
     p->extrema_maxdim = 1000;       // Plan.jl:143,160
     p->refine = 4;                  // FP64 refinement passes of the mixed-precision solve
     p->autotune = 1;
+    p->host_qr = 0;
 }
 
 int pf_solve(pf_op *op, const pf_params *params, int s, int nev, const double *x0, int x0_mem, double *vals,

@@ -142,6 +142,9 @@ struct pf_handle {
     // concurrent solves); grown on demand
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
+    // step kernels launch with programmatic dependent launch (each one's
+    // launch and shared-memory set-up overlap its predecessor's tail)
+    bool overlap = true;
 };
 
 struct pf_op {

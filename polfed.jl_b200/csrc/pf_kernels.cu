@@ -103,6 +103,7 @@ template <typename T, int V, class Desc, int FLAGS, int UB = 0, int MB = 0, int 
 __global__ void __launch_bounds__(kThreads, MB > 0 ? MB : MinBlocks<T, V>::value)
     k_step(const Desc d, const StepArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_trigger();
     constexpr bool HASQ = (FLAGS & StepFlags::Q) != 0;
     constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
     constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(kThreads, MB > 0 ? MB : MinBlocks<T, V>::value
         }
     }
     __syncthreads();
+    pdl_wait();
 
     double dd1[V], dd2[V];
 #pragma unroll
@@ -297,6 +299,7 @@ __device__ __forceinline__ void coop_round(const ChainDesc<T> &d, const uint32_t
 template <typename T, int S, int FLAGS>
 __global__ void __launch_bounds__(kThreads) k_step_coop(const ChainDesc<T> d, const StepArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_trigger();
     constexpr bool HASQ = (FLAGS & StepFlags::Q) != 0;
     constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
     constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
@@ -310,6 +313,7 @@ __global__ void __launch_bounds__(kThreads) k_step_coop(const ChainDesc<T> d, co
         }
         __syncthreads();
     }
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     const int lr = lane & (S - 1);   // this lane's column
     const int rb = lane & ~(S - 1);  // first lane of this lane's row
@@ -377,6 +381,7 @@ __host__ __device__ inline int qsun_async_slot_offset() {
 template <typename T, int V, int FLAGS>
 __global__ void __launch_bounds__(kThreads) k_step_qsun_async(const QSunDesc<T> d, const StepArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_trigger();
     constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
     constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
     constexpr int CH = V * (int)sizeof(T) / 16;   // 16-byte copies per gathered segment
@@ -395,6 +400,7 @@ __global__ void __launch_bounds__(kThreads) k_step_qsun_async(const QSunDesc<T> 
         dtab[i] = acc;
     }
     __syncthreads();
+    pdl_wait();
     uint4 *slots = reinterpret_cast<uint4 *>(smem_raw + qsun_async_slot_offset<T>());
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t G = (uint32_t)a.G;
@@ -501,6 +507,7 @@ template <typename T, int V, int FLAGS, int IPT>
 __global__ void __launch_bounds__(kThreads, 2)
     k_step_qsun_tile(const QSunDesc<T> d, const StepArgs<T> a, const T *__restrict__ tabs, int tbits) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_trigger();
     constexpr bool HASP = (FLAGS & StepFlags::P) != 0;
     constexpr bool HASX = (FLAGS & StepFlags::X) != 0;
     constexpr int U = 4;
@@ -508,6 +515,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int gs = d.dg + 1;
     const int ntab = d.dg * gs + 4 * 256;
     for (int i = threadIdx.x; i < ntab; i += blockDim.x) sm[i] = __ldg(tabs + i);
+    pdl_wait();
     const T *dtab = sm + d.dg * gs;
     Pack<T, V> *tile = reinterpret_cast<Pack<T, V> *>(smem_raw + qsun_tile_offset<T>());
     const uint32_t G = (uint32_t)a.G;   // a power of two dividing kThreads
@@ -588,6 +596,24 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
+// Launches a step kernel on st, with programmatic dependent launch when the
+// handle allows it (the kernels wait for their predecessor themselves).
+template <typename... KArgs, typename... Args>
+static void launch_step_kernel(pf_handle *h, void (*kern)(KArgs...), int grid, int smem, cudaStream_t st,
+                               Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = h->overlap ? 1 : 0;
+    PF_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+}
+
 static thread_local int64_t t_launches = 0;
 void count_launches(int64_t n) { t_launches += n; }
 int64_t thread_launches() { return t_launches; }
@@ -653,7 +679,7 @@ static void launch_one(pf_op *op, cudaStream_t st, const Desc &d, StepArgs<T> a,
         a.partials = op->h->red_partials;
         a.counter = op->h->red_counter;
     }
-    kern<<<grid, kThreads, smem, st>>>(d, a);
+    launch_step_kernel(op->h, kern, grid, smem, st, d, a);
     PF_CUDA(cudaGetLastError());
     count_launches(1);
 }
@@ -740,7 +766,7 @@ static void launch_qsun_async_one(pf_op *op, cudaStream_t st, const QSunDesc<T> 
     const int smem = qsun_async_smem(d, V);
     PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = grid_for(op->h, a.items, kThreads, blocks_per_sm((const void *)kern, smem));
-    kern<<<grid, kThreads, smem, st>>>(d, a);
+    launch_step_kernel(op->h, kern, grid, smem, st, d, a);
     PF_CUDA(cudaGetLastError());
     count_launches(1);
 }
@@ -820,7 +846,7 @@ static void launch_qsun_tile_one(pf_op *op, cudaStream_t st, const QSunDesc<T> &
     const int64_t ntiles = (int64_t)a.D >> tbits;
     const int64_t cap = (int64_t)op->h->num_sms * blocks_per_sm((const void *)kern, smem) * 8;
     const int grid = (int)std::max<int64_t>(1, std::min(ntiles, cap));
-    kern<<<grid, kThreads, smem, st>>>(d, a, qsun_tabs<T>(op), tbits);
+    launch_step_kernel(op->h, kern, grid, smem, st, d, a, qsun_tabs<T>(op), tbits);
     PF_CUDA(cudaGetLastError());
     count_launches(1);
 }
@@ -891,7 +917,7 @@ static void launch_coop_one(pf_op *op, cudaStream_t st, const ChainDesc<T> &d, c
     if ((FLAGS & StepFlags::Q) && !d.full) smem += rank_table_entries(d.nchunks) * 4;
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = grid_for(op->h, (int64_t)a.D * S, kThreads, blocks_per_sm((const void *)kern, smem));
-    kern<<<grid, kThreads, smem, st>>>(d, a);
+    launch_step_kernel(op->h, kern, grid, smem, st, d, a);
     PF_CUDA(cudaGetLastError());
     count_launches(1);
 }

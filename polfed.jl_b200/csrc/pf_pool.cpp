@@ -99,7 +99,7 @@ double solve_footprint(const pf_op *op, const pf_params *p, int s, int nev) {
     bytes += 4.0 * D * s * w + 2.0 * 8.0 * D * s;                     // filter blocks, x0 copies
     bytes += 2.0 * D * 64 * w;                                        // KPM probe blocks
     bytes += 2.0 * 8.0 * D * nev;                                     // Ritz vectors and H psi
-    bytes += 2.0 * 8.0 * maxdim * maxdim + (64 << 20);                // projected problem, slack
+    bytes += 3.0 * 8.0 * maxdim * maxdim + (64 << 20);                // projected matrix, its eigenvectors, slack
     return bytes;
 }
 

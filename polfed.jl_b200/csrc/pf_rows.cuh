@@ -81,6 +81,14 @@ __device__ __forceinline__ void stp_hint(T *p, const Pack<T, V> &v, int stream) 
     }
 }
 
+// Programmatic dependent launch.  A step kernel lets the next kernel of its
+// stream launch as soon as it starts (its CTAs become resident as this grid's
+// retire) and, after staging its own read-only tables, waits until its
+// predecessor has completed and its writes are visible before it reads any
+// block.  Both are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Explicitly rounded arithmetic.  Every step-kernel variant (any width,
 // gather batch or register cap; per-thread, warp-cooperative or
 // multi-instance) performs exactly these operations in the same order, so all
@@ -135,50 +143,69 @@ struct MinBlocks {
     static constexpr int value = bytes >= 32 ? 2 : 3;
 };
 
+// A chain row in two passes: first the diagonal over every bond in bond order
+// (fields, then the Sz Sz terms) and the mask of the bonds whose spins differ;
+// then the flipping bonds only, U of them per round (lowest bond first), each
+// round issuing its U gathers before any is used.  Bonds that do not flip
+// (about half of them) take no slot in a round, so a row needs about half
+// the dependent gather rounds of a walk over every bond; the gathers are
+// still accumulated in bond order.  RANK(b) returns the flipped state's
+// index.
+template <typename T, int V, bool HASQ, int U, class RankF>
+__device__ __forceinline__ void chain_row_walk(const ChainDesc<T> &d, uint32_t st, int s, const T *__restrict__ qc,
+                                               T (&acc)[V], T &diag, RankF rank) {
+    T dg = T(0);
+    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
+    uint64_t act = 0ull;
+    for (int b = 0; b < d.nb; ++b) {
+        const uint32_t bm = d.bmask[b];
+        const uint32_t m = st & bm;
+        const bool differ = (m != 0u) && (m != bm);
+        dg += differ ? -d.jdq[b] : d.jdq[b];
+        if (differ) act |= 1ull << b;
+    }
+    diag = dg;
+    if constexpr (HASQ) {
+        while (act != 0ull) {
+            uint32_t r2[U];
+            T jh[U];
+            bool on[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                on[u] = act != 0ull;
+                r2[u] = 0u;
+                jh[u] = T(0);
+                if (on[u]) {
+                    const int b = __ffsll((long long)act) - 1;
+                    act &= act - 1ull;
+                    r2[u] = rank(b);
+                    jh[u] = d.jhalf[b];
+                }
+            }
+            Pack<T, V> g[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (on[u]) g[u] = ldp<T, V>(qc + (size_t)r2[u] * s);
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (on[u]) {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = fma_t(jh[u], g[u].v[v], acc[v]);
+                }
+        }
+    }
+}
+
 template <typename T, int V, bool HASQ, int UB = 0>
 __device__ __forceinline__ void chain_row(const ChainDesc<T> &d, const uint32_t *tab, uint32_t row,
                                           int s, int c0, const T *__restrict__ q, T (&acc)[V],
                                           T &diag) {
     constexpr int U = UB > 0 ? UB : Batch<T, V>::U;
     const uint32_t st = d.full ? row : __ldg(d.states + row);
-    T dg = T(0);
-    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
-    const T *qc = q + c0;
-    for (int b0 = 0; b0 < d.nb; b0 += U) {
-        uint32_t r2[U];
-        bool act[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int b = b0 + u;
-            act[u] = false;
-            r2[u] = 0u;
-            if (b < d.nb) {
-                const uint32_t bm = d.bmask[b];
-                const uint32_t m = st & bm;
-                const bool differ = (m != 0u) && (m != bm);
-                dg += differ ? -d.jdq[b] : d.jdq[b];
-                act[u] = differ;
-                if (HASQ && differ) {
-                    const uint32_t st2 = st ^ bm;
-                    r2[u] = d.full ? st2 : sector_rank(st2, tab, d.nchunks);
-                }
-            }
-        }
-        if constexpr (HASQ) {
-            Pack<T, V> g[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (act[u]) g[u] = ldp<T, V>(qc + (size_t)r2[u] * s);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (act[u]) {
-                    const T jh = d.jhalf[b0 + u];
-#pragma unroll
-                    for (int v = 0; v < V; ++v) acc[v] = fma_t(jh, g[u].v[v], acc[v]);
-                }
-        }
-    }
-    diag = dg;
+    chain_row_walk<T, V, HASQ, U>(d, st, s, q + c0, acc, diag, [&](int b) -> uint32_t {
+        const uint32_t st2 = st ^ d.bmask[b];
+        return d.full ? st2 : sector_rank(st2, tab, d.nchunks);
+    });
 }
 
 // Rank of the state reached by the flip of bond b from state st of rank row,
@@ -222,41 +249,9 @@ __device__ __forceinline__ void chain_row_local(const ChainDesc<T> &d, const uin
                                                 T &diag) {
     constexpr int U = UB > 0 ? UB : Batch<T, V>::U;
     const uint32_t st = d.full ? row : __ldg(d.states + row);
-    T dg = T(0);
-    for (int i = 0; i < d.L; ++i) dg += ((st >> i) & 1u) ? d.hhalf[i] : -d.hhalf[i];
-    const T *qc = q + c0;
-    for (int b0 = 0; b0 < d.nb; b0 += U) {
-        uint32_t r2[U];
-        bool act[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int b = b0 + u;
-            act[u] = false;
-            r2[u] = 0u;
-            if (b < d.nb) {
-                const uint32_t bm = d.bmask[b];
-                const uint32_t m = st & bm;
-                const bool differ = (m != 0u) && (m != bm);
-                dg += differ ? -d.jdq[b] : d.jdq[b];
-                act[u] = differ;
-                if (HASQ && differ) r2[u] = d.full ? (st ^ bm) : flip_rank_local(d, tab, ctab, st, row, b);
-            }
-        }
-        if constexpr (HASQ) {
-            Pack<T, V> g[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (act[u]) g[u] = ldp<T, V>(qc + (size_t)r2[u] * s);
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                if (act[u]) {
-                    const T jh = d.jhalf[b0 + u];
-#pragma unroll
-                    for (int v = 0; v < V; ++v) acc[v] = fma_t(jh, g[u].v[v], acc[v]);
-                }
-        }
-    }
-    diag = dg;
+    chain_row_walk<T, V, HASQ, U>(d, st, s, q + c0, acc, diag, [&](int b) -> uint32_t {
+        return d.full ? (st ^ d.bmask[b]) : flip_rank_local(d, tab, ctab, st, row, b);
+    });
 }
 
 // Quantum Sun shared-memory layout: the grain block with a padded row stride

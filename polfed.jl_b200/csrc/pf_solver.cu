@@ -500,12 +500,12 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
 // breakdown, then the Householder factors).
 static void lanczos(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
                     int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
-                    double *stage_acc, int keep_extra = -1) {
+                    double *stage_acc, int keep_extra = -1, bool host_qr = false) {
     bool breakdown = false;
     // blocks wider than 64 columns (a Gram matrix beyond one CTA's shared
     // memory) always take the host QR
     lanczos_pass(op, s, howmany, maxdim_req, tol, eigentol, which, reorth_passes, x0_ri, fmap, out, stage_acc,
-                 keep_extra, s > 64, &breakdown);
+                 keep_extra, host_qr || s > 64, &breakdown);
     if (!breakdown) return;
     LanczosOut again;
     lanczos_pass(op, s, howmany, maxdim_req, tol, eigentol, which, reorth_passes, x0_ri, fmap, again, stage_acc,
@@ -967,7 +967,7 @@ static pf_handle *aux_handle(pf_handle *h) {
 }
 
 static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, double tol, double eigentol, double *Emin,
-                                double *Emax, double *stage_acc, int *qr_restarts = nullptr) {
+                                double *Emax, double *stage_acc, int *qr_restarts = nullptr, bool host_qr = false) {
     const int64_t D = op->dim;
     // The :SR probe runs here and the :LR probe at the same time on the
     // auxiliary handle (its own stream, cuBLAS and cuSOLVER): both only read
@@ -985,7 +985,7 @@ static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, dou
         };
         double dummy[10] = {0};
         LanczosOut lo;
-        lanczos(o, 1, 1, maxdim, tol, eigentol, which, 1, v0_dev, happly, lo, stage_acc ? dummy : nullptr);
+        lanczos(o, 1, 1, maxdim, tol, eigentol, which, 1, v0_dev, happly, lo, stage_acc ? dummy : nullptr, -1, host_qr);
         PF_CHECK(lo.nconv >= 1, PF_ERR_NUMERIC, "Failed to estimate extremal eigenvalue with Lanczos.");
         *out = which == PF_WHICH_SR ? lo.vals.front() : lo.vals.back();
         return lo.qr_restarts;
@@ -1196,7 +1196,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
             double lo = 0, hi = 0;
             // v0 = x0[:, 1] (column 0 of the column-major copy)
             extrema_from_device(op, xcm.p, P->extrema_maxdim > 0 ? P->extrema_maxdim : 1000, 1e-14, 1e-8, &lo, &hi,
-                                nullptr, &R.qr_restarts);
+                                nullptr, &R.qr_restarts, P->host_qr != 0);
             if (!P->has_Emin) Emin = lo;
             if (!P->has_Emax) Emax = hi;
         }
@@ -1289,7 +1289,8 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
             filt.run(st);
             PF_CUDA(cudaMemcpyAsync(Y, filt.Y.p, (size_t)D * s * sizeof(double), cudaMemcpyDeviceToDevice, st));
         };
-        lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage);
+        lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage, -1,
+                P->host_qr != 0);
     } else {
         const bool refine = P->refine > 0;
         // as many guard vectors as targets: the subspace iteration's rate at the
@@ -1304,7 +1305,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
                 launch_ri_to_cm<float, double>(st, (int64_t)D * s, 1, filt.Y.p, Y, (int64_t)D * s);
             };
             lanczos(op, s, nev, (int)maxdim, P->tol, P->eigentol, P->which, P->reorth_passes, xri.p, fmap, out, stage,
-                    refine ? guard : -1);
+                    refine ? guard : -1, P->host_qr != 0);
         }
         if (refine && out.nconv > 0) {
             // FP64 passes on the FP32 run's nev + guard leading Ritz vectors (filter order)

@@ -430,3 +430,30 @@ def test_tensor_core_gram_split_bf16(pkg, cuda, D, nB, s):
     bf = lambda x: cuda.tensor(x).to(cuda.bfloat16).to(cuda.float64).numpy()
     single = np.abs(bf(Bh[:, :nB]).T @ bf(rh) - ref) / scale
     assert err.max() < 0.2 * single.max()
+
+
+def test_launch_overlap_leaves_results_unchanged(pkg, orc, cuda, models):
+    """Step kernels launch with programmatic dependent launch (each waits for
+    its predecessor's writes before reading a block); plain stream order
+    gives the same filters and KPM moments bit for bit."""
+    rng = np.random.default_rng(23)
+    plan = orc.build_transform_plan(("rescaled", 0.3), 10, 1.0, 0.0, order=30)
+    coeffs = orc.filter_coefficients(plan)
+    try:
+        for name, op, H in models:
+            D = H.shape[0]
+            Emax = float(np.abs(H).sum(axis=1).max())
+            X = _dev(cuda, rng.standard_normal((D, 4)), cuda.float64)
+            probes = rng.standard_normal((D, 8))
+            probes /= np.linalg.norm(probes, axis=0)
+            out = []
+            for on in (True, False):
+                pkg.set_launch_overlap(on)
+                Y = pkg.col_major(D, 4)
+                pkg.chebyshev_filter(op, Y, X, coeffs, a=1.01 * Emax, b=0.0)
+                mu = pkg.kpm_moments(op, 40, 8, a=1.01 * Emax, b=0.0, probes=_dev(cuda, probes, cuda.float64))
+                out.append((_host(Y), np.asarray(mu)))
+            np.testing.assert_array_equal(out[0][0], out[1][0], err_msg=name)
+            np.testing.assert_array_equal(out[0][1], out[1][1], err_msg=name)
+    finally:
+        pkg.set_launch_overlap(True)
