@@ -122,6 +122,22 @@ int pf_op_spin_chain_create(pf_handle *h, int L, int Lup, int nbonds, const int3
 int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const double *coup,
                       const int32_t *nbr, const double *fields, const double *grain,
                       pf_op **out);
+/* The Quantum Sun for any spin S = two_S / 2 (1/2 .. 15/2; QuantumSun.jl:1-102)
+ * in the full space (u1 = 0) or in the total-S_z sector S_z = two_Sz / 2
+ * (u1 = 1; QuantumSun_U1_conserving.jl:1-212): localized fields, the S^x S^x
+ * (in the sector S^x S^x + S^y S^y) coupling of each localized spin j to grain
+ * site nbr[j] with strength g0 * coup[j], and the grain block.  States are
+ * indexed as the reference indexes them (sorted packed digit codes: the
+ * base-(2S+1) value of the digits, ranked within the sector).  grain is the
+ * final dg x dg block (row-major, dg = (2S+1)^L_grain <= 4096): the full space
+ * takes gamma GOE / sqrt(dg + 1), the sector the GOE masked to equal grain
+ * magnetisation and scaled by gamma / sqrt(tr(R^2) / dim) (R its embedding in
+ * the sector).  The matrix is assembled as CSR on the device and applied by
+ * the CSR step.  A sector outside [-L S, L S] or off the spin lattice fails
+ * with the reference's message. */
+int pf_op_qsun_spin_create(pf_handle *h, int L_loc, int L_grain, int two_S, int u1, int two_Sz, double g0,
+                           const double *coup, const int32_t *nbr, const double *fields, const double *grain,
+                           pf_op **out);
 /* A real symmetric sparse matrix (polfed(mat, ...), PolfedCore.jl:153-184,
  * whose operator is mul!(Y, mat, X)): CSR with 0-based row pointers
  * indptr[D + 1] (indptr[0] = 0, indptr[D] = nnz, non-decreasing), column

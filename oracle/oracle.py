@@ -5,7 +5,9 @@ This module is the checker for the CUDA library.  Only ``tests/``,
 may import it; the product never does.  It restates, in FP64 numpy plus the C
 kernels of ``polfed_oracle.c``, the reference algorithm of Polfed.jl (Julia):
 
-* models -- ``Models/SpinHalfChains.jl:227-315``, ``QSun/QuantumSun.jl:1-102``
+* models -- ``Models/SpinHalfChains.jl:227-315``, ``QSun/QuantumSun.jl:1-102``,
+  ``QSun/QuantumSun_U1_conserving.jl:1-212``, ``QSun/SpinOperators.jl:5-69``,
+  ``QSun/HilbertSpace.jl:9-41``
 * rescaling -- ``Polfed/Plan/Plan.jl:128-191``
 * target spec -- ``Polfed/Structs/TargetSpec.jl:26-58``, ``Plan.jl:203-281``
 * DoS / KPM -- ``DensetiesOfStates/DensitiesOfStates.jl:14-43``,
@@ -183,6 +185,137 @@ def qsun_matrix(L_loc, L_grain, g0, coup, nbr, fields, Hg) -> sp.csr_matrix:
     lib().orc_qsun_coo(L_loc, L_grain, g0, _p(coup), _p(nbr), _p(fields), _p(Hg),
                        _p(rows), _p(cols), _p(vals))
     return _coo_to_csr(rows, cols, vals, 1 << (L_loc + L_grain))
+
+
+# ------------------------------------------------ spin-S Quantum Sun family
+class _SpinBasis:
+    """``SpinBasis`` (SpinOperators.jl:5-21): d = 2S + 1 levels per site,
+    ceil(log2 d) bits per site in a packed state code."""
+
+    def __init__(self, S):
+        self.S = float(S)
+        self.d = int(round(2 * S)) + 1
+        self.bits = int(math.ceil(math.log2(self.d)))
+        self.mask = (1 << self.bits) - 1
+
+    def get_spin(self, state, site):                     # SpinOperators.jl:23-27
+        return float((state >> (site * self.bits)) & self.mask) - self.S
+
+    def set_spin(self, state, site, m_new):              # SpinOperators.jl:29-34
+        shift = site * self.bits
+        state &= ~(self.mask << shift)
+        return state | (int(round(m_new + self.S)) << shift)
+
+    def sigma_z(self, state, site):                      # SpinOperators.jl:38-41
+        return self.get_spin(state, site), state
+
+    def _ladder(self, state, site, cu, cd):
+        m = self.get_spin(state, site)
+        S = self.S
+        has_up, has_down = m < S, m > -S
+        c_up = cu * math.sqrt(S * (S + 1) - m * (m + 1)) if has_up else 0.0
+        c_down = cd * math.sqrt(S * (S + 1) - m * (m - 1)) if has_down else 0.0
+        s_up = self.set_spin(state, site, m + 1) if has_up else 0
+        s_down = self.set_spin(state, site, m - 1) if has_down else 0
+        return has_up, c_up, s_up, has_down, c_down, s_down
+
+    def sigma_x(self, state, site):                      # SpinOperators.jl:43-53
+        return self._ladder(state, site, 0.5, 0.5)
+
+    def sigma_y(self, state, site):                      # SpinOperators.jl:55-69
+        return self._ladder(state, site, 1 / 2j, -(1 / 2j))
+
+
+def _spin_states(L, B):
+    """``build_hilbert`` (HilbertSpace.jl:9-32): every packed code, sorted."""
+    states = [0]
+    for site in range(L):
+        shift = site * B.bits
+        states = [st | (si << shift) for st in states for si in range(B.d)]
+    return sorted(states)
+
+
+def _qsun_spin_terms(states, index, L_loc, L_grain, g0, coup, nbr, fields, B, keep, use_y):
+    """The fields and S^x S^x (and S^y S^y) entries in the reference's push
+    order (QuantumSun.jl:35-95, QuantumSun_U1_conserving.jl:92-207); keep(i)
+    says whether state index i belongs to the basis."""
+    rows, cols, vals = [], [], []
+    for k, state in enumerate(states):
+        if not keep(k):
+            continue
+        for j in range(L_loc):
+            val_z, _ = B.sigma_z(state, L_grain + j)
+            rows.append(k), cols.append(k), vals.append(fields[j] * val_z)
+        for j in range(L_loc):
+            site_loc, site_grain = L_grain + j, int(nbr[j])
+            for op in ((B.sigma_x, B.sigma_y) if use_y else (B.sigma_x,)):
+                has1, c1, s1, has2, c2, s2 = op(state, site_loc)
+                for has, c, s in ((has1, c1, s1), (has2, c2, s2)):
+                    if not has:
+                        continue
+                    hg1, cg1, sg1, hg2, cg2, sg2 = op(s, site_grain)
+                    for hg, cg, sg in ((hg1, cg1, sg1), (hg2, cg2, sg2)):
+                        if not hg:
+                            continue
+                        new = index.get(sg, -1)
+                        if new >= 0 and keep(new):
+                            v = g0 * coup[j] * c * cg
+                            rows.append(new), cols.append(k), vals.append(float(np.real(v)))
+    return rows, cols, vals
+
+
+def qsun_spin_matrix(L_loc, L_grain, g0, coup, nbr, fields, goe, S=0.5, gamma=1.0, use_U1=False,
+                     S_z=0.0) -> sp.csr_matrix:
+    """Sparse H of ``build_hamiltonian`` (QuantumSun.jl:1-102) for spin S, or of
+    ``build_hamiltonian_cons`` (QuantumSun_U1_conserving.jl:1-212) for the
+    total-S_z sector, from the raw GOE draw ``goe`` (the reference scales it
+    per model).  Pure Python: small sizes only."""
+    B = _SpinBasis(S)
+    L = L_loc + L_grain
+    if use_U1:
+        sector_index = S_z + L * S
+        if abs(S_z) > L * S or not float(sector_index).is_integer():
+            raise ValueError(f"Wrong total value of spin to given spin-S particles. You chose S = {S} and S_z = {S_z}.")
+    states = _spin_states(L, B)
+    index = {st: i for i, st in enumerate(states)}
+    dim = len(states)
+    d = B.d
+    dim_loc, dim_grain = d ** L_loc, d ** L_grain
+    goe = np.asarray(goe, dtype=np.float64).reshape(dim_grain, dim_grain)
+    coup = np.asarray(coup, dtype=np.float64)
+    fields = np.asarray(fields, dtype=np.float64)
+    if not use_U1:
+        H_grain = gamma * goe / math.sqrt(dim_grain + 1)
+        rows, cols, vals = _qsun_spin_terms(states, index, L_loc, L_grain, g0, coup, nbr, fields, B,
+                                            lambda k: True, False)
+        H = sp.coo_matrix((vals, (rows, cols)), shape=(dim, dim)).tocsr()
+        return (H + sp.kron(sp.identity(dim_loc), sp.csr_matrix(H_grain))).tocsr()
+    # QuantumSun_U1_conserving.jl:37-90: grain mask, sector rows, restricted and normalised R
+    H_grain = goe.copy()
+    gstates = states[:dim_grain]          # codes of the grain sites alone (the lowest codes)
+    for II in range(dim_grain):
+        for JJ in range(dim_grain):
+            sI = sum(B.get_spin(gstates[II], j) for j in range(L_grain))
+            sJ = sum(B.get_spin(gstates[JJ], j) for j in range(L_grain))
+            if sJ != sI:
+                H_grain[II, JJ] = 0.0
+    mag = np.array([sum(B.sigma_z(st, j)[0] for j in range(L)) for st in states])
+    rows_mag = np.full(dim, -1, dtype=np.int64)
+    counter = 0
+    for k in range(dim):
+        if mag[k] == S_z:
+            rows_mag[k] = counter
+            counter += 1
+    dim_red = counter
+    R = sp.kron(sp.identity(dim_loc), sp.csr_matrix(H_grain)).tocoo()
+    sel = (mag[R.row] == S_z) & (mag[R.col] == S_z)
+    R_cons = sp.coo_matrix((R.data[sel], (rows_mag[R.row[sel]], rows_mag[R.col[sel]])),
+                           shape=(dim_red, dim_red)).tocsr()
+    R_cons = gamma * R_cons / math.sqrt((R_cons @ R_cons).diagonal().sum() / dim_red)
+    rows, cols, vals = _qsun_spin_terms(states, index, L_loc, L_grain, g0, coup, nbr, fields, B,
+                                        lambda k: mag[k] == S_z, True)
+    H = sp.coo_matrix((vals, (rows_mag[rows], rows_mag[cols])), shape=(dim_red, dim_red)).tocsr()
+    return (H + R_cons).tocsr()
 
 
 class CSROperator:

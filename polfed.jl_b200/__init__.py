@@ -13,13 +13,15 @@ from .core import (autotune, set_step_width, step_variant, set_filter_slab, set_
                    chebyshev_filter, clenshaw_finalsum, clenshaw_recurrence, col_major, display_report,
                    expectedkrylovdim, kpm_moments, lanczos_extrema, normalize_target_spec, polfed,
                    polfed_batch, worker_handles, SolverPool, PoolStats, solver_pool)
-from .models import (BoundOperator, QSunOperator, SparseOperator, SpinChainOperator, as_operator, chain_bonds, goe_matrix, j1j2_hamiltonian,
-                     qsun_hamiltonian, qsun_parameters, xxz_hamiltonian)
+from .models import (BoundOperator, QSunOperator, QSunSpinOperator, SparseOperator, SpinChainOperator, as_operator, chain_bonds,
+                     goe_matrix, j1j2_hamiltonian, qsun_hamiltonian, qsun_parameters, qsun_spin_grain,
+                     qsun_spin_parameters, spin_sector_count, xxz_hamiltonian)
 
 __all__ = [
     "polfed", "lanczos_extrema", "MappingConfig", "TransformConfig", "FactorizationConfig", "DoSConfig",
     "Report", "SpectralTransformReport", "FactorizationReport", "BenchmarkReport", "display_report",
-    "xxz_hamiltonian", "j1j2_hamiltonian", "qsun_hamiltonian", "qsun_parameters", "chain_bonds",
+    "xxz_hamiltonian", "j1j2_hamiltonian", "qsun_hamiltonian", "qsun_parameters", "qsun_spin_parameters", "qsun_spin_grain",
+    "spin_sector_count", "QSunSpinOperator", "chain_bonds",
     "goe_matrix", "SpinChainOperator", "QSunOperator", "SparseOperator", "as_operator", "apply", "clenshaw_recurrence",
     "clenshaw_finalsum", "chebyshev_filter", "kpm_moments", "basis_states", "basis_index", "col_major",
     "normalize_target_spec", "expectedkrylovdim", "load_library", "autotune", "set_step_width", "step_variant", "set_filter_slab", "set_launch_overlap", "polfed_batch", "worker_handles", "SolverPool", "PoolStats", "solver_pool", "BoundOperator",

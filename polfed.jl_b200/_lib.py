@@ -30,7 +30,7 @@ PF_WIDTH_COOP = 0
 
 EXPORTED = [
     "pf_abi_version", "pf_abi_sizes", "pf_last_error", "pf_handle_create", "pf_handle_destroy", "pf_handle_stream",
-    "pf_handle_synchronize", "pf_handle_set_overlap", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_destroy",
+    "pf_handle_synchronize", "pf_handle_set_overlap", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_qsun_spin_create", "pf_op_destroy",
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
     "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
     "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind", "pf_set_step_width",
@@ -135,6 +135,7 @@ def load():
         "pf_handle_set_overlap": (i32, [vp, i32]),
         "pf_op_spin_chain_create": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_qsun_create": (i32, [vp, i32, i32, f64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
+        "pf_op_qsun_spin_create": (i32, [vp, i32, i32, i32, i32, i32, f64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_destroy": (i32, [vp]),
         "pf_op_csr_create": (i32, [vp, i64, i64, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_bind": (i32, [vp, vp, ctypes.POINTER(vp)]),

@@ -158,6 +158,15 @@ int pf_op_qsun_create(pf_handle *h, int L_loc, int L_grain, double g0, const dou
     PF_API_END
 }
 
+int pf_op_qsun_spin_create(pf_handle *h, int L_loc, int L_grain, int two_S, int u1, int two_Sz, double g0,
+                           const double *coup, const int32_t *nbr, const double *fields, const double *grain,
+                           pf_op **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    *out = pf::create_qsun_spin(h, L_loc, L_grain, two_S, u1, two_Sz, g0, coup, nbr, fields, grain);
+    PF_API_END
+}
+
 int pf_op_csr_create(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
                      const double *values, pf_op **out) {
     PF_API_BEGIN

@@ -225,11 +225,6 @@ pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, c
         PF_CHECK(std::isfinite(values[p]), PF_ERR_INVALID, "non-finite matrix entry");
     }
     PF_CUDA(cudaSetDevice(h->device));
-    pf_op *op = new pf_op();
-    op->h = h;
-    op->kind = OP_CSR;
-    op->dim = D;
-    op->nnz = nnz;
     int64_t *dptr = nullptr;
     int32_t *didx = nullptr;
     double *dv64 = nullptr;
@@ -246,22 +241,32 @@ pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, c
             PF_CUDA(cudaMemcpy(dv64, values, nnz * sizeof(double), cudaMemcpyHostToDevice));
             PF_CUDA(cudaMemcpy(dv32, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice));
         }
-        const int dev = h->device;
-        op->tables_owner = std::shared_ptr<void>(nullptr, [dptr, didx, dv64, dv32, dev](void *) {
-            cudaSetDevice(dev);
-            cudaFree(dptr);
-            cudaFree(didx);
-            cudaFree(dv64);
-            cudaFree(dv32);
-        });
     } catch (...) {
         if (dptr) cudaFree(dptr);
         if (didx) cudaFree(didx);
         if (dv64) cudaFree(dv64);
         if (dv32) cudaFree(dv32);
-        delete op;
         throw;
     }
+    return adopt_csr(h, D, nnz, dptr, didx, dv64, dv32);
+}
+
+pf_op *adopt_csr(pf_handle *h, int64_t D, int64_t nnz, int64_t *dptr, int32_t *didx, double *dv64, float *dv32) {
+    pf_op *op = nullptr;
+    const int dev = h->device;
+    auto owner = std::shared_ptr<void>(nullptr, [dptr, didx, dv64, dv32, dev](void *) {
+        cudaSetDevice(dev);
+        cudaFree(dptr);
+        cudaFree(didx);
+        cudaFree(dv64);
+        cudaFree(dv32);
+    });
+    op = new pf_op();
+    op->h = h;
+    op->kind = OP_CSR;
+    op->dim = D;
+    op->nnz = nnz;
+    op->tables_owner = owner;
     op->csr64 = {dptr, didx, dv64};
     op->csr32 = {dptr, didx, dv32};
     try {

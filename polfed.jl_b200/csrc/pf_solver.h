@@ -13,6 +13,17 @@ pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double
                    const double *fields, const double *grain);
 pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
                   const double *values);
+// An OP_CSR operator that takes ownership of device arrays (cudaMalloc'd on
+// h's device): row pointers (D + 1), column indices and values in both
+// precisions (nnz each).
+pf_op *adopt_csr(pf_handle *h, int64_t D, int64_t nnz, int64_t *dptr, int32_t *didx, double *dv64, float *dv32);
+// The Quantum Sun for spin S = two_S / 2 (QuantumSun.jl) or its total-S_z
+// sector (u1 != 0, S_z = two_Sz / 2; QuantumSun_U1_conserving.jl), built as a
+// CSR matrix on the device.  grain: the final dg x dg grain block
+// (dg = (two_S + 1)^L_grain, row-major, already normalised and, for the
+// sector, masked to equal grain magnetisation).
+pf_op *create_qsun_spin(pf_handle *h, int L_loc, int L_grain, int two_S, int u1, int two_Sz, double g0,
+                        const double *coup, const int32_t *nbr, const double *fields, const double *grain);
 void destroy_op(pf_op *op);
 pf_op *bind_op(const pf_op *src, pf_handle *h);
 void *handle_scratch(pf_handle *h, size_t bytes);

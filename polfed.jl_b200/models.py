@@ -7,7 +7,9 @@ apply directly.  Arguments, defaults and validation follow the reference:
 * ``xxz_hamiltonian``  -- SpinHalfChains.jl:74-99
 * ``j1j2_hamiltonian`` -- SpinHalfChains.jl:189-220
 * ``qsun_hamiltonian`` -- Models/Models.jl:97-115 -> QSun/QSun.jl:277-324 ->
-  QSun/QuantumSun.jl:1-102 (full space, S = 1/2)
+  QSun/QuantumSun.jl:1-102 (full space, matrix-free for S = 1/2, device-built
+  CSR for S > 1/2) and QSun/QuantumSun_U1_conserving.jl:1-212 (total-S_z
+  sector, any S, device-built CSR)
 
 Random draws use a numpy ``Generator`` (``rng``); Julia's MersenneTwister
 streams are not reproducible outside Julia, so a realisation is identified by
@@ -198,6 +200,90 @@ class QSunOperator(Operator):
         return out.value
 
 
+def spin_sector_count(n_sites: int, d: int, total: int) -> int:
+    """Number of strings of ``n_sites`` digits in 0..d-1 with digit sum
+    ``total`` (the states of a total-S_z sector: digit = m + S)."""
+    if total < 0 or total > n_sites * (d - 1):
+        return 0
+    cnt = [1] + [0] * total
+    for _ in range(n_sites):
+        nxt = [0] * (total + 1)
+        for t in range(total + 1):
+            nxt[t] = sum(cnt[t - c] for c in range(min(d - 1, t) + 1))
+        cnt = nxt
+    return cnt[total]
+
+
+def _spin_sector(L: int, S: float, S_z: float):
+    """(d, digit-sum target) of the sector S_z for L spins S, with the
+    reference's check (QuantumSun_U1_conserving.jl:17-20)."""
+    sector_index = S_z + L * S
+    if abs(S_z) > L * S or not float(sector_index).is_integer():
+        raise ValueError(f"Wrong total value of spin to given spin-S particles. You chose S = {S} and S_z = {S_z}.")
+    return int(round(2 * S)) + 1, int(round(sector_index))
+
+
+def qsun_spin_grain(goe, L_loc: int, L_grain: int, S: float, *, gamma: float = 1.0, use_U1: bool = False,
+                    S_z: float = 0.0) -> np.ndarray:
+    """The grain block as the reference builds it from the GOE draw: the full
+    space takes gamma GOE / sqrt(dg + 1) (QuantumSun.jl:29-30); the sector masks
+    the GOE to equal grain magnetisation and scales it by gamma / sqrt(tr(R^2) /
+    dim) with R = kron(I, masked) restricted to the sector
+    (QuantumSun_U1_conserving.jl:34-90); tr(R^2) = sum over grain states g of
+    (localized completions of g) * sum_g' masked[g, g']^2."""
+    d = int(round(2 * S)) + 1
+    dg = d ** L_grain
+    goe = np.asarray(goe, dtype=np.float64).reshape(dg, dg)
+    if not use_U1:
+        return gamma * goe / math.sqrt(dg + 1)
+    _, T = _spin_sector(L_loc + L_grain, S, S_z)
+    gsum = np.array([sum((g // d ** i) % d for i in range(L_grain)) for g in range(dg)])
+    masked = np.where(gsum[:, None] == gsum[None, :], goe, 0.0)
+    dim = spin_sector_count(L_loc + L_grain, d, T)
+    mult = np.array([spin_sector_count(L_loc, d, T - int(gs)) for gs in gsum], dtype=np.float64)
+    tr = float(np.sum(mult * np.sum(masked * masked, axis=1)))
+    return gamma * masked / math.sqrt(tr / dim)
+
+
+class QSunSpinOperator(Operator):
+    """The Quantum Sun for spin S (QuantumSun.jl:1-102) or in the total-S_z
+    sector (``use_U1``; QuantumSun_U1_conserving.jl:1-212), assembled as a CSR
+    matrix on the device (``pf_op_qsun_spin_create``).  ``grain`` is the final
+    (2S+1)^L_grain block (``qsun_spin_grain``)."""
+
+    kind = "qsun_spin"
+
+    def __init__(self, L_loc: int, L_grain: int, S: float, g0: float, couplings, neighbors, fields, grain,
+                 use_U1: bool = False, S_z: float = 0.0, device: int = 0):
+        super().__init__(device)
+        if not float(2 * S).is_integer() or S <= 0:
+            raise ValueError(f"Wrong value of spin. Only integer spins or half-integer spins are possible. You chose S = {S}")
+        self.L_loc, self.L_grain, self.S = int(L_loc), int(L_grain), float(S)
+        self.g0, self.use_U1, self.S_z = float(g0), bool(use_U1), float(S_z)
+        if self.use_U1:
+            _spin_sector(self.L_loc + self.L_grain, self.S, self.S_z)
+        self.couplings = np.asarray(couplings, dtype=np.float64).reshape(-1)
+        self.neighbors = np.asarray(neighbors, dtype=np.int32).reshape(-1)
+        self.fields = np.asarray(fields, dtype=np.float64).reshape(-1)
+        dg = (int(round(2 * S)) + 1) ** self.L_grain
+        self.grain = np.asarray(grain, dtype=np.float64).reshape(dg, dg)
+        for arr, name in ((self.couplings, "couplings"), (self.neighbors, "neighbors"), (self.fields, "fields")):
+            if len(arr) != self.L_loc:
+                raise ValueError(f"{name} must have length L_loc={self.L_loc}")
+
+    def _create(self) -> int:
+        c = np.ascontiguousarray(self.couplings)
+        n = np.ascontiguousarray(self.neighbors, dtype=np.int32)
+        f = np.ascontiguousarray(self.fields)
+        g = np.ascontiguousarray(self.grain)
+        out = ctypes.c_void_p()
+        _lib.check(_lib.load().pf_op_qsun_spin_create(
+            self.handle, self.L_loc, self.L_grain, int(round(2 * self.S)), 1 if self.use_U1 else 0,
+            int(round(2 * self.S_z)), self.g0, c.ctypes.data, n.ctypes.data, f.ctypes.data, g.ctypes.data,
+            ctypes.byref(out)))
+        return out.value
+
+
 class SparseOperator(Operator):
     """A real symmetric sparse matrix as the operator of ``polfed(mat, ...)``
     (PolfedCore.jl:153-184, whose operator is ``mul!(Y, mat, X)``).  ``mat``
@@ -298,18 +384,45 @@ def qsun_parameters(L_loc: int, L_grain: int, alpha: float, *, gamma: float = 1.
     return fields, neighbors, couplings, grain
 
 
+def qsun_spin_parameters(L_loc: int, L_grain: int, alpha: float, S: float = 0.5, *, w: float = 0.5,
+                         hz: float = 1.0, zeta: float = 0.2, rng=None):
+    """The draws of build_hamiltonian / build_hamiltonian_cons in their order
+    (QuantumSun.jl:21-30, QuantumSun_U1_conserving.jl:28-36): fields, grain
+    neighbours, couplings, then the raw GOE of dimension (2S+1)^L_grain (its
+    scaling depends on the model: ``qsun_spin_grain``)."""
+    rng = np.random.default_rng() if rng is None else rng
+    fields = rng.random(L_loc) * ((hz + w) - (hz - w)) + (hz - w)
+    neighbors = rng.integers(0, L_grain, size=L_loc)
+    couplings = np.zeros(L_loc)
+    if alpha > 0:
+        couplings[0] = 1.0
+        for j in range(2, L_loc + 1):
+            u = j - 1 + rng.random() * 2 * zeta - zeta
+            couplings[j - 1] = alpha ** u
+    dg = (int(round(2 * S)) + 1) ** L_grain
+    return fields, neighbors, couplings, goe_matrix(dg, rng)
+
+
 def qsun_hamiltonian(L_loc: int, L_grain: int, g0: float, alpha: float, *, gamma: float = 1.0, w: float = 0.5,
                      hz: float = 1.0, zeta: float = 0.2, S: float = 0.5, rng=None, use_U1: bool = False,
                      S_z: float = 0.0, couplings=None, neighbors=None, fields=None, grain=None,
                      device: int = 0) -> QSunOperator:
-    """Quantum Sun model (QSun.jl:277-324 / QuantumSun.jl:1-102).  Explicit
-    ``couplings`` / ``neighbors`` / ``fields`` / ``grain`` override the draws."""
+    """Quantum Sun model (QSun.jl:277-324).  The spin-1/2 full space
+    (QuantumSun.jl:1-102) is the matrix-free ``QSunOperator``; spin S > 1/2 and
+    the total-S_z sector (``use_U1``, QuantumSun_U1_conserving.jl:1-212) are a
+    ``QSunSpinOperator`` assembled on the device.  Explicit ``couplings`` /
+    ``neighbors`` / ``fields`` / ``grain`` override the draws (``grain`` is the
+    final block; for S > 1/2 or the sector see ``qsun_spin_grain``)."""
     if not float(2 * S).is_integer():
         raise ValueError(f"Wrong value of spin. Only integer spins or half-integer spins are possible. You chose S = {S}")
-    if S != 0.5:
-        raise NotImplementedError("the B200 path implements the spin-1/2 Quantum Sun only")
-    if use_U1:
-        raise NotImplementedError("the U(1) Quantum Sun sector is not implemented on the B200 path")
+    if S != 0.5 or use_U1:
+        if use_U1:
+            _spin_sector(L_loc + L_grain, S, S_z)
+        f, n, c, goe = qsun_spin_parameters(L_loc, L_grain, alpha, S, w=w, hz=hz, zeta=zeta, rng=rng)
+        g = qsun_spin_grain(goe, L_loc, L_grain, S, gamma=gamma, use_U1=use_U1, S_z=S_z) if grain is None else grain
+        return QSunSpinOperator(L_loc, L_grain, S, g0, c if couplings is None else couplings,
+                                n if neighbors is None else neighbors, f if fields is None else fields, g,
+                                use_U1=use_U1, S_z=S_z, device=device)
     f, n, c, g = qsun_parameters(L_loc, L_grain, alpha, gamma=gamma, w=w, hz=hz, zeta=zeta, rng=rng)
     return QSunOperator(L_loc, L_grain, g0, c if couplings is None else couplings,
                         n if neighbors is None else neighbors, f if fields is None else fields,

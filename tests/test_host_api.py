@@ -111,10 +111,15 @@ def test_qsun_parameters(pkg):
     assert g.shape == (8, 8) and np.allclose(g, g.T)
     op = pkg.qsun_hamiltonian(13, 3, 1.0, 0.75, rng=np.random.default_rng(1))
     assert op.L_loc == 13 and op.grain.shape == (8, 8)
-    with pytest.raises(NotImplementedError):
-        pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, S=1.0)
+    # spin S > 1/2 and the total-S_z sector: device-built CSR operators
+    op1 = pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, S=1.0, rng=np.random.default_rng(2))
+    assert isinstance(op1, pkg.QSunSpinOperator) and op1.grain.shape == (9, 9)
+    op2 = pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, use_U1=True, S_z=1.0, rng=np.random.default_rng(2))
+    assert isinstance(op2, pkg.QSunSpinOperator) and op2.use_U1 and op2.grain.shape == (4, 4)
     with pytest.raises(ValueError):
         pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, S=0.3)
+    with pytest.raises(ValueError, match="Wrong total value of spin"):
+        pkg.qsun_hamiltonian(4, 2, 1.0, 0.5, use_U1=True, S_z=0.5)
 
 
 def test_pool_refuses_without_a_device_and_footprint_guards(pkg):
@@ -152,3 +157,25 @@ def test_sparse_operator_host_validation(pkg):
     np.testing.assert_array_equal(d.indptr, A.indptr)
     np.testing.assert_array_equal(d.indices, A.indices)
     np.testing.assert_array_equal(d.values, A.data)
+
+
+@pytest.mark.parametrize("S,L_loc,L_grain,S_z", [(0.5, 4, 2, 0.0), (1.0, 3, 2, 1.0), (1.5, 2, 2, 1.0)])
+def test_qsun_spin_grain_normalisation(pkg, orc, S, L_loc, L_grain, S_z):
+    """The sector's grain block is the GOE masked to equal grain magnetisation
+    and scaled so that tr(R^2) / dim = gamma^2 for its embedding R in the
+    sector (QuantumSun_U1_conserving.jl:34-90): the oracle's R (fields and
+    couplings zero) has exactly the host-side block's entries."""
+    rng = np.random.default_rng(4)
+    f, n, c, goe = pkg.qsun_spin_parameters(L_loc, L_grain, 0.75, S, rng=rng)
+    g = pkg.qsun_spin_grain(goe, L_loc, L_grain, S, gamma=1.3, use_U1=True, S_z=S_z)
+    R = orc.qsun_spin_matrix(L_loc, L_grain, 0.0, c, n, np.zeros(L_loc), goe, S=S, gamma=1.3, use_U1=True,
+                             S_z=S_z).toarray()
+    assert abs(np.trace(R @ R) / R.shape[0] - 1.3 ** 2) < 1e-12
+    d = int(round(2 * S)) + 1
+    B = orc._SpinBasis(S)
+    states = orc._spin_states(L_loc + L_grain, B)
+    mag = np.array([sum(B.get_spin(st, j) for j in range(L_loc + L_grain)) for st in states])
+    sector = np.nonzero(mag == S_z)[0]
+    K = np.kron(np.eye(d ** L_loc), g)[np.ix_(sector, sector)]
+    np.testing.assert_allclose(R, K, rtol=1e-13, atol=1e-15)
+    assert pkg.spin_sector_count(L_loc + L_grain, d, int(round(S_z + (L_loc + L_grain) * S))) == R.shape[0]

@@ -81,6 +81,41 @@ def test_qsun_structure(orc):
     np.testing.assert_allclose(H[:dg, :dg] - np.diag(np.diag(H[:dg, :dg])), Hg - np.diag(np.diag(Hg)), atol=1e-15)
 
 
+def _qsun_spin_draw(rng, L_loc, L_grain, S, alpha):
+    d = int(round(2 * S)) + 1
+    dg = d ** L_grain
+    X = rng.standard_normal((dg, dg))
+    coup = np.array([1.0] + [alpha ** (j + 0.1) for j in range(1, L_loc)])
+    return rng.random(L_loc) + 0.5, rng.integers(0, L_grain, L_loc), coup, (X + X.T) / math.sqrt(2)
+
+
+def test_qsun_spin_shapes_and_sector_error(orc):
+    """test_qsun.jl:5-76: the full-space and U(1)-sector builders' sizes and
+    Hermiticity (spin 1/2 and 3/2), and the sector check's message."""
+    rng = np.random.default_rng(8)
+    for c in GOLD["qsun_shapes"]["cases"]:
+        f, n, cp, goe = _qsun_spin_draw(rng, c["L_loc"], c["L_grain"], c["S"], c["alpha"])
+        H = orc.qsun_spin_matrix(c["L_loc"], c["L_grain"], c["g0"], cp, n, f, goe, S=c["S"], use_U1=c["use_U1"],
+                                 S_z=c["S_z"])
+        assert H.shape == (c["dim"], c["dim"]), c
+        A = H.toarray()
+        np.testing.assert_allclose(A, A.T, atol=1e-15)
+    e = GOLD["qsun_sector_error"]
+    f, n, cp, goe = _qsun_spin_draw(rng, e["L_loc"], e["L_grain"], e["S"], 0.5)
+    with pytest.raises(ValueError, match=e["message"].replace(".", r"\.")):
+        orc.qsun_spin_matrix(e["L_loc"], e["L_grain"], 1.0, cp, n, f, goe, S=e["S"], use_U1=True, S_z=e["S_z"])
+
+
+def test_qsun_spin_half_matches_the_spin_half_builder(orc):
+    """The general-spin restatement at S = 1/2 equals the spin-1/2 builder
+    (the GOE scaled by 1 / sqrt(dg + 1) as QuantumSun.jl:29-30 does)."""
+    rng = np.random.default_rng(9)
+    f, n, cp, goe = _qsun_spin_draw(rng, 4, 3, 0.5, 0.75)
+    H1 = orc.qsun_spin_matrix(4, 3, 1.0, cp, n, f, goe)
+    H2 = orc.qsun_matrix(4, 3, 1.0, cp, n, f, goe / 3.0)
+    assert abs(H1 - H2).max() == 0.0
+
+
 def test_structured_csr_apply(orc):
     # optimization.jl:236-304: the optimized map equals H * x for vectors and blocks.
     g = GOLD["structured_packing"]
