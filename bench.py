@@ -772,6 +772,43 @@ def profile_step():
     return 0
 
 
+def profile_kpm():
+    """KPM on the workload's operator at its block width: one 64-probe block of
+    normalised Gaussian probes, 40 moments (20 doubling steps with fused
+    dots), FP64 -- a bounded case for ncu captures of the KPM step."""
+    import numpy as np
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+    ops, _ = make_realisations(pkg, 1, 1000)
+    op = ops[0]
+    mu = pkg.kpm_moments(op, 40, 64, a=8.0, b=0.0)
+    print(json.dumps({"profile_kpm": True, "D": op.dim, "R": 64, "N": 40, "mu0": float(np.asarray(mu)[0])}))
+    return 0
+
+
+def profile_gram():
+    """The split-BF16 tensor-core Gram product G = B^T r at the workload's
+    final Krylov size (D = 65536, 624 basis columns, s = 8), twice -- a
+    bounded case for ncu captures of k_gram_bf16x3."""
+    import torch
+    from polfed_b200 import _lib
+    import __graft_entry__ as ge
+    ge.load_package()
+    D, nB, s = 65536, 624, WORKLOAD["blocksize"]
+    g = torch.Generator(device="cuda:0").manual_seed(5)
+    B = torch.randn(D, nB, dtype=torch.float64, device="cuda:0", generator=g)
+    r = torch.randn(D, s, dtype=torch.float64, device="cuda:0", generator=g)
+    G = torch.empty(s, nB, dtype=torch.float64, device="cuda:0")
+    for _ in range(2):
+        _lib.check(_lib.load().pf_gram_bf16x3(_lib.handle(0), D, nB, B.data_ptr(), nB, r.data_ptr(), s,
+                                              G.data_ptr()))
+    torch.cuda.synchronize()
+    ref = (B.t() @ r).t()
+    err = float((G - ref).abs().max() / (B.norm(dim=0).max() * r.norm(dim=0).max()))
+    print(json.dumps({"profile_gram": True, "D": D, "nB": nB, "s": s, "max_err_rel": err}))
+    return 0
+
+
 STEP_CASES = [
     # (name, constructor, s)
     ("qsun_Lloc13_D65536", lambda pkg, rng: pkg.qsun_hamiltonian(13, 3, 1.0, 0.75, rng=rng), 8),
@@ -874,6 +911,10 @@ def main():
                     help="two order-2 filters on J1-J2 L=24 (a bounded large-D case for ncu)")
     ap.add_argument("--profile-step", action="store_true",
                     help="only run two short Chebyshev filters on one realisation (a bounded case for ncu)")
+    ap.add_argument("--profile-kpm", action="store_true",
+                    help="only run 40 KPM moments of one 64-probe block (a bounded case for ncu)")
+    ap.add_argument("--profile-gram", action="store_true",
+                    help="only run the tensor-core Gram product at the final Krylov size (a bounded case for ncu)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = _env_int("WORLD_SIZE", 1)
@@ -883,6 +924,10 @@ def main():
         return run_reference(args, rank, world)
     if args.profile_step:
         return profile_step()
+    if args.profile_kpm:
+        return profile_kpm()
+    if args.profile_gram:
+        return profile_gram()
     if args.step_sweep:
         return step_sweep(args.large_only)
     if args.profile_step_large:

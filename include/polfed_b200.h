@@ -145,6 +145,16 @@ int pf_op_qsun_spin_create(pf_handle *h, int L_loc, int L_grain, int two_S, int 
  * caller's contract, as in the reference.  D < 2^31. */
 int pf_op_csr_create(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
                      const double *values, pf_op **out);
+/* A complex Hermitian sparse matrix H = A + iB (the reference's CPU path
+ * takes complex Hermitian input; its GPU path refuses it, PolfedCore.jl:160-162):
+ * CSR as pf_op_csr_create with values[2 nnz] interleaved (re, im) -- the
+ * layout of C double _Complex, Julia ComplexF64 and numpy complex128 arrays.
+ * Hermiticity is the caller's contract; a diagonal entry with a nonzero
+ * imaginary part is refused.  The operator is H's real embedding
+ * M = [[A, -B], [B, A]] (pf_op_dim = 2 D; pf_apply applies M to [Re X; Im X])
+ * and is solved with pf_solve_hermitian.  D < 2^30. */
+int pf_op_csr_create_hermitian(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr,
+                               const int32_t *indices, const double *values, pf_op **out);
 /* A view of op that runs on handle h (same device).  It shares op's device
  * tables, so several host threads can solve concurrently, each on its own
  * handle / stream.  Destroy views and the original in any order; the tables
@@ -339,6 +349,17 @@ void pf_params_default(pf_params *p);
 int pf_solve(pf_op *op, const pf_params *params, int s, int nev,
              const double *x0, int x0_mem, double *vals, double *vecs, int vecs_mem,
              pf_report *report, int *nconv);
+/* POLFED on a complex Hermitian operator (pf_op_csr_create_hermitian).  x0 is
+ * D x s complex column-major (interleaved re, im), vecs D x nev complex
+ * (interleaved); vals real.  The complex block Lanczos from x0 is run as the
+ * real block Lanczos of the embedding from [v, i v] (2s columns, 2 nev pairs:
+ * every eigenvalue of H appears twice), and each group of equal eigenvalues
+ * is turned back into complex eigenvectors x + iy (one per complex direction,
+ * unit norm, arbitrary phase).  The report describes that real run, with
+ * blocksize s, howmany nev and converged_eigentol the returned count. */
+int pf_solve_hermitian(pf_op *op, const pf_params *params, int s, int nev,
+                       const double *x0, int x0_mem, double *vals, double *vecs, int vecs_mem,
+                       pf_report *report, int *nconv);
 
 /* ------------------------------------------------ batching and serving */
 /* No reference counterpart: the reference solves one problem per call.  A

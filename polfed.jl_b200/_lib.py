@@ -32,9 +32,9 @@ EXPORTED = [
     "pf_abi_version", "pf_abi_sizes", "pf_last_error", "pf_handle_create", "pf_handle_destroy", "pf_handle_stream",
     "pf_handle_synchronize", "pf_handle_set_overlap", "pf_op_spin_chain_create", "pf_op_qsun_create", "pf_op_qsun_spin_create", "pf_op_destroy",
     "pf_op_dim", "pf_basis_unrank", "pf_basis_rank", "pf_apply", "pf_clenshaw_recurrence",
-    "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve",
+    "pf_clenshaw_finalsum", "pf_filter", "pf_kpm_moments", "pf_params_default", "pf_solve", "pf_solve_hermitian",
     "pf_lanczos_extrema", "pf_autotune", "pf_apply_noalloc", "pf_op_bind", "pf_set_step_width",
-    "pf_op_csr_create",
+    "pf_op_csr_create", "pf_op_csr_create_hermitian",
     "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
     "pf_pool_set_priority_dim", "pf_pool_set_admission", "pf_pool_request_times",
@@ -138,6 +138,7 @@ def load():
         "pf_op_qsun_spin_create": (i32, [vp, i32, i32, i32, i32, i32, f64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_destroy": (i32, [vp]),
         "pf_op_csr_create": (i32, [vp, i64, i64, vp, vp, vp, ctypes.POINTER(vp)]),
+        "pf_op_csr_create_hermitian": (i32, [vp, i64, i64, vp, vp, vp, ctypes.POINTER(vp)]),
         "pf_op_bind": (i32, [vp, vp, ctypes.POINTER(vp)]),
         "pf_op_dim": (i64, [vp]),
         "pf_basis_unrank": (i32, [vp, i64, vp, vp]),
@@ -151,6 +152,8 @@ def load():
         "pf_params_default": (None, [ctypes.POINTER(pf_params)]),
         "pf_solve": (i32, [vp, ctypes.POINTER(pf_params), i32, i32, vp, i32, vp, vp, i32,
                            ctypes.POINTER(pf_report), ctypes.POINTER(i32)]),
+        "pf_solve_hermitian": (i32, [vp, ctypes.POINTER(pf_params), i32, i32, vp, i32, vp, vp, i32,
+                                     ctypes.POINTER(pf_report), ctypes.POINTER(i32)]),
         "pf_lanczos_extrema": (i32, [vp, vp, i32, f64, f64, ctypes.POINTER(f64), ctypes.POINTER(f64)]),
         "pf_autotune": (i32, [vp, i32, i32, ctypes.POINTER(i32), vp]),
         "pf_set_step_width": (i32, [vp, i32, i32, i32]),

@@ -279,8 +279,8 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
            precision: str = "fp64", vecs: bool = True):
     """POLFED on the B200 (PolfedCore.jl:194-263).
 
-    ``op`` is a model operator or a real symmetric matrix (scipy.sparse, a
-    CSR triple or dense; PolfedCore.jl:153-184).  ``x0`` is D (scalar
+    ``op`` is a model operator or a real symmetric / complex Hermitian
+    matrix (scipy.sparse, a CSR triple or dense; PolfedCore.jl:153-184).  ``x0`` is D (scalar
     Lanczos) or D x s (block Lanczos): a host array, or a
     column-major float64 CUDA tensor (then the eigenvectors are returned as a
     column-major CUDA tensor and never leave HBM).  A non-normalised /
@@ -294,6 +294,9 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
     if howmany < 1:
         raise ValueError("howmany must be positive")
     op = as_operator(op)   # polfed(mat, ...): a sparse or dense matrix runs as a CSR operator
+    if getattr(op, "is_complex", False):
+        return _polfed_hermitian(op, x0, howmany, target, produce_report, mapping, transform, fact, dos,
+                                 precision, vecs)
     D = op.dim
     on_device = _is_cuda_tensor(x0)
     if on_device:
@@ -344,6 +347,53 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
     if produce_report:
         return out_vals, out_vecs, _make_report(rep, kind, val)
     return out_vals, out_vecs
+
+
+def _polfed_hermitian(op, x0, howmany, target, produce_report, mapping, transform, fact, dos, precision, vecs):
+    """polfed on a complex Hermitian matrix (``pf_solve_hermitian``): x0 is
+    D or D x s complex (host, or a column-major complex128 CUDA tensor); the
+    eigenvectors come back complex, unit norm, arbitrary phase.  KPM probes, if
+    given (D x R, real or complex), act on the real embedding as [Re; Im]."""
+    D = op.complex_dim
+    on_device = _is_cuda_tensor(x0)
+    if on_device:
+        import torch
+        if x0.dtype != torch.complex128:
+            raise ValueError("x0 must be complex128")
+        s = 1 if x0.dim() == 1 else x0.shape[1]
+        if x0.shape[0] != D or x0.stride(0) != 1 or (x0.dim() == 2 and x0.stride(1) != D):
+            raise ValueError(f"x0 must be a column-major {D} x s complex CUDA tensor")
+        keep_x = x0
+        x_ptr, x_mem = x0.data_ptr(), _lib.PF_MEM_DEVICE
+        V = torch.empty((howmany, D), dtype=torch.complex128, device=x0.device).t() if vecs else None
+        v_ptr, v_mem = (V.data_ptr() if vecs else None), _lib.PF_MEM_DEVICE
+    else:
+        x = np.asarray(x0, dtype=np.complex128)
+        if x.ndim not in (1, 2) or x.shape[0] != D or x.size == 0:
+            raise ValueError(f"x0 must be a non-empty vector or matrix with {D} rows")
+        s = 1 if x.ndim == 1 else x.shape[1]
+        keep_x = np.asfortranarray(x.reshape(D, s))
+        x_ptr, x_mem = keep_x.ctypes.data, _lib.PF_MEM_HOST
+        V = np.zeros((D, howmany), dtype=np.complex128, order="F") if vecs else None
+        v_ptr, v_mem = (V.ctypes.data if vecs else None), _lib.PF_MEM_HOST
+    if dos.probes is not None:
+        pr = np.asarray(dos.probes)
+        if pr.shape != (D, dos.R):
+            raise ValueError(f"probes must be D x R = {D} x {dos.R}")
+        dos = DoSConfig(N=dos.N, R=dos.R, kernel=dos.kernel, probe_kind=dos.probe_kind, seed=dos.seed,
+                        probes=np.vstack([pr.real, pr.imag]) if np.iscomplexobj(pr) else np.vstack([pr, 0 * pr]))
+    p, keep, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
+    vals = np.zeros(howmany)
+    rep = _lib.pf_report()
+    n = ctypes.c_int(0)
+    _lib.check(_lib.load().pf_solve_hermitian(op.op, ctypes.byref(p), s, howmany, x_ptr, x_mem, vals.ctypes.data,
+                                              v_ptr, v_mem, ctypes.byref(rep), ctypes.byref(n)))
+    del keep, keep_x
+    k = n.value
+    out_vecs = (V[:, :k] if on_device else V[:, :k].copy()) if vecs else None
+    if produce_report:
+        return vals[:k].copy(), out_vecs, _make_report(rep, kind, val)
+    return vals[:k].copy(), out_vecs
 
 
 _WORKERS: dict = {}

@@ -167,6 +167,14 @@ int pf_op_qsun_spin_create(pf_handle *h, int L_loc, int L_grain, int two_S, int 
     PF_API_END
 }
 
+int pf_op_csr_create_hermitian(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr,
+                               const int32_t *indices, const double *values, pf_op **out) {
+    PF_API_BEGIN
+    PF_CHECK(out != nullptr, PF_ERR_INVALID, "null output pointer");
+    *out = pf::create_csr_hermitian(h, D, nnz, indptr, indices, values);
+    PF_API_END
+}
+
 int pf_op_csr_create(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
                      const double *values, pf_op **out) {
     PF_API_BEGIN
@@ -384,7 +392,16 @@ int pf_solve(pf_op *op, const pf_params *params, int s, int nev, const double *x
              double *vecs, int vecs_mem, pf_report *report, int *nconv) {
     PF_API_BEGIN
     PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    PF_CHECK(op->complex_dim == 0, PF_ERR_INVALID, "a Hermitian operator is solved with pf_solve_hermitian");
     pf::solve(op, params, s, nev, x0, x0_mem, vals, vecs, vecs_mem, report, nconv);
+    PF_API_END
+}
+
+int pf_solve_hermitian(pf_op *op, const pf_params *params, int s, int nev, const double *x0, int x0_mem,
+                       double *vals, double *vecs, int vecs_mem, pf_report *report, int *nconv) {
+    PF_API_BEGIN
+    PF_CHECK(op, PF_ERR_INVALID, "null operator");
+    pf::solve_hermitian(op, params, s, nev, x0, x0_mem, vals, vecs, vecs_mem, report, nconv);
     PF_API_END
 }
 

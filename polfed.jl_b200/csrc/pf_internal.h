@@ -159,6 +159,9 @@ struct pf_op {
     pf::CsrDesc<double> csr64{};
     pf::CsrDesc<float> csr32{};
     int64_t nnz = 0;
+    // > 0: the real embedding [[A, -B], [B, A]] of a complex Hermitian H = A + iB
+    // of this dimension (dim = 2 complex_dim); solved by solve_hermitian
+    int64_t complex_dim = 0;
     uint32_t *d_states = nullptr;
     uint32_t *d_rank_tab = nullptr;
     double *d_diag64 = nullptr;       // chain diagonal in each precision (warp-cooperative step)

@@ -251,6 +251,51 @@ pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, c
     return adopt_csr(h, D, nnz, dptr, didx, dv64, dv32);
 }
 
+// H = A + iB Hermitian (CSR, values interleaved re, im) as the real symmetric
+// M = [[A, -B], [B, A]] of twice the dimension: M [x; y] = [Re H(x+iy); Im H(x+iy)].
+pf_op *create_csr_hermitian(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                            const double *values) {
+    PF_CHECK(h != nullptr, PF_ERR_INVALID, "null handle");
+    PF_CHECK(D >= 1 && D < ((int64_t)1 << 30), PF_ERR_UNSUPPORTED, "Hermitian matrix dimension must be in [1, 2^30)");
+    PF_CHECK(nnz >= 0 && indptr && (nnz == 0 || (indices && values)), PF_ERR_INVALID, "null CSR array");
+    PF_CHECK(indptr[0] == 0 && indptr[D] == nnz, PF_ERR_INVALID, "indptr must start at 0 and end at nnz");
+    for (int64_t i = 0; i < D; ++i)
+        PF_CHECK(indptr[i + 1] >= indptr[i], PF_ERR_INVALID, "indptr must be non-decreasing");
+    for (int64_t p = 0; p < nnz; ++p) {
+        PF_CHECK(indices[p] >= 0 && (int64_t)indices[p] < D, PF_ERR_INVALID, "column index out of range");
+        PF_CHECK(std::isfinite(values[2 * p]) && std::isfinite(values[2 * p + 1]), PF_ERR_INVALID,
+                 "non-finite matrix entry");
+    }
+    for (int64_t i = 0; i < D; ++i)
+        for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p)
+            PF_CHECK(indices[p] != i || values[2 * p + 1] == 0.0, PF_ERR_INVALID,
+                     "a Hermitian matrix has a real diagonal");
+    // rows 0..D-1: [A, -B]; rows D..2D-1: [B, A] (entries whose part is zero are left out)
+    std::vector<int64_t> ptr((size_t)2 * D + 1, 0);
+    std::vector<int32_t> idx;
+    std::vector<double> val;
+    idx.reserve((size_t)4 * nnz);
+    val.reserve((size_t)4 * nnz);
+    for (int half = 0; half < 2; ++half)
+        for (int64_t i = 0; i < D; ++i) {
+            for (int64_t p = indptr[i]; p < indptr[i + 1]; ++p) {
+                const double re = values[2 * p], im = values[2 * p + 1];
+                const int32_t c = indices[p];
+                if (half == 0) {
+                    if (re != 0.0) idx.push_back(c), val.push_back(re);
+                    if (im != 0.0) idx.push_back((int32_t)(D + c)), val.push_back(-im);
+                } else {
+                    if (im != 0.0) idx.push_back(c), val.push_back(im);
+                    if (re != 0.0) idx.push_back((int32_t)(D + c)), val.push_back(re);
+                }
+            }
+            ptr[(size_t)half * D + i + 1] = (int64_t)idx.size();
+        }
+    pf_op *op = create_csr(h, 2 * D, (int64_t)idx.size(), ptr.data(), idx.data(), val.data());
+    op->complex_dim = D;
+    return op;
+}
+
 pf_op *adopt_csr(pf_handle *h, int64_t D, int64_t nnz, int64_t *dptr, int32_t *didx, double *dv64, float *dv32) {
     pf_op *op = nullptr;
     const int dev = h->device;
@@ -299,6 +344,7 @@ pf_op *bind_op(const pf_op *src, pf_handle *h) {
     op->csr64 = src->csr64;
     op->csr32 = src->csr32;
     op->nnz = src->nnz;
+    op->complex_dim = src->complex_dim;
     op->d_states = src->d_states;
     op->d_rank_tab = src->d_rank_tab;
     op->d_diag64 = src->d_diag64;

@@ -5,6 +5,7 @@
 #include "pf_solver.h"
 
 #include <atomic>
+#include <complex>
 #include <exception>
 #include <thread>
 #include "pf_spectral.h"
@@ -1389,6 +1390,147 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
         R.basis_bytes_used = (double)D * out.krylovdim * sizeof(double);
         R.kernel_launches = thread_launches() - launches0;
         R.qr_restarts += out.qr_restarts;
+        *rep = R;
+    }
+}
+
+// ------------------------------------------------ complex Hermitian input
+// polfed on H = A + iB (the reference's CPU path takes complex Hermitian
+// matrices and runs Lanczos in complex arithmetic; its GPU path refuses them,
+// PolfedCore.jl:160-162).  op is the real embedding M = [[A, -B], [B, A]],
+// which commutes with J [x; y] = [-y; x] (multiplication by i).  The complex
+// block Lanczos from x0 (s columns) spans, over the reals, the Krylov space of
+// M from [v, Jv] (v = [Re x0; Im x0]): the real solve with 2s columns and
+// 2 nev pairs is the complex one, each eigenvalue of H appearing twice.  Its
+// Ritz vectors u = [x; y] become complex vectors x + iy; within each group of
+// equal eigenvalues a pivoted complex Gram-Schmidt keeps one vector per complex
+// direction (the two copies of an eigenvector are psi and i psi; a degenerate
+// eigenvalue keeps its whole eigenspace).
+void solve_hermitian(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int x0_mem, double *vals,
+                     double *vecs, int vecs_mem, pf_report *rep, int *nconv) {
+    using cd = std::complex<double>;
+    PF_CHECK(op && P && x0 && vals && nconv, PF_ERR_INVALID, "null argument");
+    PF_CHECK(op->complex_dim > 0, PF_ERR_INVALID,
+             "pf_solve_hermitian needs a Hermitian operator (pf_op_csr_create_hermitian)");
+    PF_CHECK(s >= 1 && nev >= 1, PF_ERR_INVALID, "s and nev must be positive");
+    const int64_t D = op->complex_dim;
+    pf_handle *h = op->h;
+    PF_CUDA(cudaSetDevice(h->device));
+    AllocStream alloc_guard(h->stream);
+    cudaStream_t st = h->stream;
+    std::vector<double> xc((size_t)2 * D * s);
+    if (x0_mem == PF_MEM_DEVICE) {
+        PF_CUDA(cudaMemcpyAsync(xc.data(), x0, xc.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync(h);
+    } else {
+        std::memcpy(xc.data(), x0, xc.size() * sizeof(double));
+    }
+    // the real start block [v_1 .. v_s, J v_1 .. J v_s]
+    const int64_t D2 = 2 * D;
+    std::vector<double> xr((size_t)D2 * 2 * s);
+    for (int c = 0; c < s; ++c)
+        for (int64_t i = 0; i < D; ++i) {
+            const double re = xc[2 * (i + (size_t)c * D)], im = xc[2 * (i + (size_t)c * D) + 1];
+            xr[i + (size_t)c * D2] = re;
+            xr[D + i + (size_t)c * D2] = im;
+            xr[i + (size_t)(s + c) * D2] = -im;
+            xr[D + i + (size_t)(s + c) * D2] = re;
+        }
+    const int m = 2 * nev;
+    std::vector<double> rv(m);
+    DevArray<double> rvec((size_t)D2 * m);
+    int rn = 0;
+    pf_report R;
+    std::memset(&R, 0, sizeof(R));
+    solve(op, P, 2 * s, m, xr.data(), PF_MEM_HOST, rv.data(), rvec.p, PF_MEM_DEVICE, &R, &rn);
+    std::vector<double> hv((size_t)D2 * std::max(rn, 1));
+    if (rn > 0) {
+        PF_CUDA(cudaMemcpyAsync(hv.data(), rvec.p, (size_t)D2 * rn * sizeof(double), cudaMemcpyDeviceToHost, st));
+        sync(h);
+    }
+    struct Pair {
+        double val;
+        std::vector<cd> psi;
+    };
+    std::vector<Pair> out;
+    for (int i0 = 0; i0 < rn;) {
+        int i1 = i0 + 1;
+        while (i1 < rn && std::fabs(rv[i1] - rv[i0]) <= 1e-8 * std::max(1.0, std::fabs(rv[i0]))) ++i1;
+        std::vector<std::vector<cd>> cand;
+        std::vector<double> cval;
+        for (int a = i0; a < i1; ++a) {
+            std::vector<cd> psi((size_t)D);
+            for (int64_t k = 0; k < D; ++k) psi[k] = cd(hv[k + (size_t)a * D2], hv[D + k + (size_t)a * D2]);
+            cand.push_back(std::move(psi));
+            cval.push_back(rv[a]);
+        }
+        std::vector<bool> used(cand.size(), false);
+        std::vector<std::vector<cd>> kept;
+        while (true) {
+            // the candidate with the largest component outside the kept vectors
+            int best = -1;
+            double bestn = 0.3;
+            std::vector<cd> bestv;
+            for (size_t a = 0; a < cand.size(); ++a) {
+                if (used[a]) continue;
+                std::vector<cd> w = cand[a];
+                for (const auto &b : kept) {
+                    cd dot = 0.0;
+                    for (int64_t k = 0; k < D; ++k) dot += std::conj(b[k]) * w[k];
+                    for (int64_t k = 0; k < D; ++k) w[k] -= dot * b[k];
+                }
+                double n2 = 0.0;
+                for (int64_t k = 0; k < D; ++k) n2 += std::norm(w[k]);
+                if (std::sqrt(n2) > bestn) {
+                    bestn = std::sqrt(n2);
+                    best = (int)a;
+                    bestv.swap(w);
+                }
+            }
+            if (best < 0) break;
+            used[best] = true;
+            for (auto &z : bestv) z /= bestn;
+            kept.push_back(bestv);
+            out.push_back({cval[best], bestv});
+        }
+        i0 = i1;
+    }
+    std::stable_sort(out.begin(), out.end(), [](const Pair &x, const Pair &y) { return x.val < y.val; });
+    if ((int)out.size() > nev) {
+        // more complex directions than asked (an unpaired copy): the nev nearest the target
+        const double tgt = R.a * R.target + R.b;
+        std::vector<int> ord(out.size());
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(),
+                         [&](int x, int y) { return std::fabs(out[x].val - tgt) < std::fabs(out[y].val - tgt); });
+        ord.resize(nev);
+        std::sort(ord.begin(), ord.end());
+        std::vector<Pair> sel;
+        for (int k : ord) sel.push_back(std::move(out[k]));
+        out.swap(sel);
+    }
+    const int nc = (int)out.size();
+    *nconv = nc;
+    for (int k = 0; k < nc; ++k) vals[k] = out[k].val;
+    if (vecs && nc > 0) {
+        std::vector<double> packed((size_t)2 * D * nc);
+        for (int k = 0; k < nc; ++k)
+            for (int64_t i = 0; i < D; ++i) {
+                packed[2 * (i + (size_t)k * D)] = out[k].psi[i].real();
+                packed[2 * (i + (size_t)k * D) + 1] = out[k].psi[i].imag();
+            }
+        if (vecs_mem == PF_MEM_DEVICE) {
+            PF_CUDA(cudaMemcpyAsync(vecs, packed.data(), packed.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            sync(h);
+        } else {
+            std::memcpy(vecs, packed.data(), packed.size() * sizeof(double));
+        }
+    }
+    if (rep) {
+        // the real solve's report, in the complex problem's terms
+        R.blocksize = s;
+        R.howmany = nev;
+        R.converged_eigentol = nc;
         *rep = R;
     }
 }

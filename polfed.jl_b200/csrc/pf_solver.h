@@ -13,6 +13,14 @@ pf_op *create_qsun(pf_handle *h, int L_loc, int L_grain, double g0, const double
                    const double *fields, const double *grain);
 pf_op *create_csr(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
                   const double *values);
+// A complex Hermitian CSR matrix (values interleaved re, im) as its real
+// embedding (pf_op.complex_dim = D, dim = 2 D).
+pf_op *create_csr_hermitian(pf_handle *h, int64_t D, int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                            const double *values);
+// polfed on a complex Hermitian operator: x0, vecs complex (interleaved)
+// column-major; nev eigenpairs of H.
+void solve_hermitian(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int x0_mem, double *vals,
+                     double *vecs, int vecs_mem, pf_report *rep, int *nconv);
 // An OP_CSR operator that takes ownership of device arrays (cudaMalloc'd on
 // h's device): row pointers (D + 1), column indices and values in both
 // precisions (nnz each).

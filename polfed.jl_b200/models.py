@@ -285,11 +285,16 @@ class QSunSpinOperator(Operator):
 
 
 class SparseOperator(Operator):
-    """A real symmetric sparse matrix as the operator of ``polfed(mat, ...)``
-    (PolfedCore.jl:153-184, whose operator is ``mul!(Y, mat, X)``).  ``mat``
-    is anything with ``tocsr()`` (a scipy.sparse matrix), a CSR triple
-    ``(indptr, indices, values)`` of a square matrix, or a dense 2-D array.
-    Symmetry is the caller's contract, as in the reference."""
+    """A real symmetric or complex Hermitian sparse matrix as the operator of
+    ``polfed(mat, ...)`` (PolfedCore.jl:153-184, whose operator is
+    ``mul!(Y, mat, X)``).  ``mat`` is anything with ``tocsr()`` (a
+    scipy.sparse matrix), a CSR triple ``(indptr, indices, values)`` of a
+    square matrix, or a dense 2-D array.  Symmetry (Hermiticity) is the
+    caller's contract, as in the reference.  Complex values give a Hermitian
+    operator (``is_complex``): the device holds its real embedding
+    [[A, -B], [B, A]] of twice the dimension and ``polfed`` solves it in the
+    complex problem's terms (``pf_solve_hermitian``); the reference's CPU path
+    takes such matrices, its GPU path refuses them (PolfedCore.jl:160-162)."""
 
     kind = "csr"
 
@@ -309,12 +314,15 @@ class SparseOperator(Operator):
             rows, cols = np.nonzero(a)
             indptr = np.searchsorted(rows, np.arange(a.shape[0] + 1))
             indices, values = cols, a[rows, cols]
-        if np.iscomplexobj(values):
-            raise ValueError("Complex GPU arrays are not supported yet. Current GPU kernels are real-only. "
-                             "Use CPU arrays for complex matrices/operators.")
+        self.is_complex = bool(np.iscomplexobj(values))
         self.indptr = np.ascontiguousarray(indptr, dtype=np.int64)
         self.indices = np.ascontiguousarray(indices, dtype=np.int32)
-        self.values = np.ascontiguousarray(values, dtype=np.float64)
+        self.values = np.ascontiguousarray(values, dtype=np.complex128 if self.is_complex else np.float64)
+        if self.is_complex:
+            D = len(self.indptr) - 1
+            rows = np.repeat(np.arange(D), np.diff(self.indptr)) if D > 0 else np.zeros(0, np.int64)
+            if np.any(self.values.imag[rows == self.indices] != 0.0):
+                raise ValueError("a Hermitian matrix has a real diagonal")
         if self.indptr.ndim != 1 or len(self.indptr) < 2:
             raise ValueError("indptr must hold D + 1 row pointers")
         if len(self.indices) != len(self.values) or self.indptr[-1] != len(self.values):
@@ -326,9 +334,17 @@ class SparseOperator(Operator):
         idx = self.indices if nnz else np.zeros(1, np.int32)
         val = self.values if nnz else np.zeros(1)
         out = ctypes.c_void_p()
-        _lib.check(_lib.load().pf_op_csr_create(self.handle, D, nnz, self.indptr.ctypes.data, idx.ctypes.data,
-                                                val.ctypes.data, ctypes.byref(out)))
+        create = _lib.load().pf_op_csr_create_hermitian if self.is_complex else _lib.load().pf_op_csr_create
+        if self.is_complex and not nnz:
+            val = np.zeros(1, np.complex128)
+        _lib.check(create(self.handle, D, nnz, self.indptr.ctypes.data, idx.ctypes.data, val.ctypes.data,
+                          ctypes.byref(out)))
         return out.value
+
+    @property
+    def complex_dim(self) -> int:
+        """H's dimension for a Hermitian operator (its device embedding has twice it)."""
+        return len(self.indptr) - 1
 
 
 def as_operator(mat, device: int = 0) -> Operator:

@@ -67,26 +67,28 @@ def test_device_built_matrix_equals_the_reference_builder(pkg, orc, cuda, case):
 
 @pytest.mark.parametrize("case", [CASES[1], CASES[3], CASES[4]])
 def test_solves_on_device_built_operators(pkg, orc, cuda, case):
+    """The GPU solve and the oracle's POLFED on identical inputs (the same
+    matrix, KPM probes and x0): same plan, same eigenvalues to 1e-10, and
+    every returned pair an FP64 eigenpair of the device-built matrix."""
     op, H = _build(pkg, orc, case, seed=21)
     D = H.shape[0]
-    ev = np.linalg.eigvalsh(H.toarray())
-    nev = 8
+    nev, N, R = 8, 96, 24
     rng = np.random.default_rng(22)
     x0 = rng.random(D)
+    probes = orc.normalized_gaussian_probes(D, R, np.random.default_rng(23))
+    ref = orc.polfed(orc.CSROperator(H), x0, nev, ("rescaled", 0.5), N=N, R=R, probes=probes,
+                     overestimate_iters=2.0, eigentol=1e-10)
     vals, vecs, rep = pkg.polfed(op, x0, nev, ("rescaled", 0.5), produce_report=True,
-                                 dos=pkg.DoSConfig(N=96, R=24, seed=5),
+                                 dos=pkg.DoSConfig(N=N, R=R, probes=probes),
                                  fact=pkg.FactorizationConfig(eigentol=1e-10, overestimate_iters=2.0))
-    assert abs(rep.spectral.Emin - ev[0]) < 1e-9 * max(1, abs(ev[0]))
-    assert abs(rep.spectral.Emax - ev[-1]) < 1e-9 * max(1, abs(ev[-1]))
-    assert len(vals) == nev
+    assert rep.spectral.order == ref.order
+    assert abs(rep.spectral.Emin - ref.Emin) < 1e-9 * max(1, abs(ref.Emin))
+    assert len(vals) == len(ref.vals) == nev
+    np.testing.assert_allclose(vals, ref.vals, rtol=1e-10, atol=1e-10)
     for j in range(nev):
         v = vecs[:, j]
         assert abs(np.linalg.norm(v) - 1) < 1e-9
         assert np.linalg.norm(H @ v - vals[j] * v) < 1e-10
-    target = ev[0] + 0.5 * (ev[-1] - ev[0])
-    # the returned set is the nev eigenvalues nearest the target (up to ties at the edge of the window)
-    near = np.sort(ev[np.argsort(np.abs(ev - target))[:nev]])
-    np.testing.assert_allclose(np.sort(vals), near, rtol=1e-10, atol=1e-10)
 
 
 def test_sector_dimensions_and_errors_on_device(pkg, cuda):

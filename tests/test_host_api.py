@@ -141,12 +141,15 @@ def test_pool_refuses_without_a_device_and_footprint_guards(pkg):
 
 def test_sparse_operator_host_validation(pkg):
     """Matrix input is checked on the host before any device work: square,
-    real (the reference rejects complex GPU input, PolfedCore.jl:160-162),
-    consistent CSR arrays; a dense matrix becomes the same CSR as scipy's."""
+    a complex matrix Hermitian on its diagonal, consistent CSR arrays; a dense
+    matrix becomes the same CSR as scipy's."""
     import scipy.sparse as sp
     with pytest.raises(ValueError, match="square"):
         pkg.SparseOperator(np.zeros((3, 4)))
-    with pytest.raises(ValueError, match="Complex GPU arrays"):
+    # complex input is a Hermitian operator (real diagonal checked on the host)
+    herm = pkg.SparseOperator(sp.csr_matrix(np.array([[1.0, 2j], [-2j, 3.0]])))
+    assert herm.is_complex and herm.complex_dim == 2
+    with pytest.raises(ValueError, match="real diagonal"):
         pkg.SparseOperator(sp.csr_matrix(np.eye(3) * 1j))
     with pytest.raises(ValueError):
         pkg.SparseOperator((np.array([0, 1]), np.array([0, 0]), np.array([1.0])))
