@@ -489,19 +489,21 @@ def served_sample(pkg, local_rank, requests=12, rate=2.0, workers=4):
         ids.append(pool.submit(op, x0, nev, ("rescaled", eps), vecs=False,
                                dos=pkg.DoSConfig(N=SERVE["dos_N"], R=SERVE["dos_R"], seed=SERVE["seed"] + i),
                                fact=pkg.FactorizationConfig(eigentol=SERVE["eigentol"])))
-    nconv, rejected, failed = 0, 0, 0
+    nconv, rejected, failed, errors = 0, 0, 0, []
     for rid in ids:
         try:
             vals, _ = pool.result(rid)
             nconv += len(vals)
-        except pkg._lib.PolfedRejected:
+        except pkg._lib.PolfedRejected as e:
             rejected += 1
-        except pkg._lib.PolfedError:
+            errors.append(str(e))
+        except pkg._lib.PolfedError as e:
             failed += 1
+            errors.append(str(e))
     wall = time.perf_counter() - t0
     st = pool.stats()
     pool.close()
-    return {"requests": requests, "rate_per_s": rate, "workers": workers, "admission": "shortest",
+    return {"requests": requests, "rate_per_s": rate, "workers": workers, "admission": "shortest", "errors": errors,
             "mix": "XXZ L=14..16 (Sz=0 or -1/2) and Quantum Sun L_loc=10..13, eps~U[0.1,0.9], nev in {50,100,200}, "
                    "s in {4,8,16}, seeded Poisson arrivals",
             "eigenpairs_per_s": nconv / wall, "converged": nconv, "rejected": rejected, "failed": failed,
@@ -772,6 +774,52 @@ def profile_step():
     return 0
 
 
+# The reference's published single-vector XXZ H-apply times, FP64, Delta = 0.55,
+# PBC, Sz = 0 (docs/src/tutorials/advanced/custom-mapping/index.md:92-115; CPU,
+# hardware not stated): generic sparse mul! and its bucketed custom mapping, us.
+PUBLISHED_APPLY = {18: (856.653, 579.533), 20: (5402.0, 2340.0), 22: (25727.0, 10202.0), 24: (109943.0, 41825.0)}
+
+
+def apply_sweep():
+    """The reference's only published timings on this path, re-measured here:
+    one H-apply of a single vector (s = 1) of the XXZ chain at L = 18..24,
+    Delta = 0.55, PBC, Sz = 0, FP64, through pf_apply (graph-free, one launch
+    per apply).  CUDA events on the library stream around 200 applies issued
+    back to back through the C entry point after 20 warm-up applies (at small
+    L the host's issue rate can bound it); inputs larger than L2 at L >= 22,
+    L2-resident below."""
+    import torch
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+    from polfed_b200 import _lib
+    st = torch.cuda.ExternalStream(_lib.stream_of(_lib.handle(0)), device="cuda:0")
+    for L, (generic, custom) in PUBLISHED_APPLY.items():
+        op = pkg.xxz_hamiltonian(L, L // 2, 1.0, 0.55, 0.0, fields=[0.0] * L)
+        D = op.dim
+        X = pkg.col_major(D, 1)
+        X.copy_(torch.rand(D, 1, dtype=torch.float64, device="cuda:0"))
+        Y = pkg.col_major(D, 1)
+        pkg.apply(op, Y, X)   # creates the operator and joins the streams once
+        torch.cuda.synchronize()
+        lib, h = _lib.load(), op.op
+        args = (h, _lib.PF_F64, 1.0, 0.0, 1, X.data_ptr(), D, Y.data_ptr(), D)
+        for _ in range(20):
+            _lib.check(lib.pf_apply(*args))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = 200
+        e0.record(st)
+        for _ in range(n):
+            _lib.check(lib.pf_apply(*args))
+        e1.record(st)
+        e1.synchronize()
+        us = e0.elapsed_time(e1) * 1e3 / n
+        print(json.dumps({"apply_sweep": True, "model": "xxz", "L": L, "D": D, "s": 1, "dtype": "f64",
+                          "us_per_apply": us, "rows_per_s": D / us * 1e6,
+                          "published_us": {"generic_mul": generic, "custom_mapping": custom},
+                          "speedup_vs_custom": custom / us}), flush=True)
+    return 0
+
+
 def profile_kpm():
     """KPM on the workload's operator at its block width: one 64-probe block of
     normalised Gaussian probes, 40 moments (20 doubling steps with fused
@@ -791,9 +839,9 @@ def profile_gram():
     final Krylov size (D = 65536, 624 basis columns, s = 8), twice -- a
     bounded case for ncu captures of k_gram_bf16x3."""
     import torch
-    from polfed_b200 import _lib
     import __graft_entry__ as ge
     ge.load_package()
+    from polfed_b200 import _lib
     D, nB, s = 65536, 624, WORKLOAD["blocksize"]
     g = torch.Generator(device="cuda:0").manual_seed(5)
     B = torch.randn(D, nB, dtype=torch.float64, device="cuda:0", generator=g)
@@ -911,6 +959,8 @@ def main():
                     help="two order-2 filters on J1-J2 L=24 (a bounded large-D case for ncu)")
     ap.add_argument("--profile-step", action="store_true",
                     help="only run two short Chebyshev filters on one realisation (a bounded case for ncu)")
+    ap.add_argument("--apply-sweep", action="store_true",
+                    help="single-vector XXZ H-apply at L=18..24 (the reference's published timings)")
     ap.add_argument("--profile-kpm", action="store_true",
                     help="only run 40 KPM moments of one 64-probe block (a bounded case for ncu)")
     ap.add_argument("--profile-gram", action="store_true",
@@ -924,6 +974,8 @@ def main():
         return run_reference(args, rank, world)
     if args.profile_step:
         return profile_step()
+    if args.apply_sweep:
+        return apply_sweep()
     if args.profile_kpm:
         return profile_kpm()
     if args.profile_gram:

@@ -24,8 +24,9 @@ namespace pf {
 // ---------------------------------------------------------------- errors
 struct Error : std::runtime_error {
     int code;
-    // set when the request itself cannot be met (the DoS holds fewer than nev
-    // states within reach of the target), as opposed to a failure while solving
+    // set when the request itself cannot be met (a planning bisection has no
+    // bracket: no interval around the target holds nev states, or no order
+    // meets the cutoff there), as opposed to a failure while solving
     bool infeasible = false;
     Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
 };

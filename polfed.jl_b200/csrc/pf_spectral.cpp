@@ -71,9 +71,16 @@ double Dos::operator()(double x) const {
     return cheb_clenshaw(coeffs_.data(), N_ - 1, x) / (M_PI * std::sqrt(1.0 - x * x));
 }
 
+// Bisection.jl:18-40.  Every caller is a planning step (the interval from
+// the DoS, the order in the interval, the interval from the order): a bracket
+// without a sign change means no filter meets the request's target and
+// howmany, so the error is marked infeasible (a pool rejects the request).
 double bisection(const std::function<int(double)> &f, double x1, double x2, double tol, int max_iter) {
-    if ((double)f(x1) * (double)f(x2) > 0)
-        throw Error(PF_ERR_NUMERIC, "The function must have opposite signs at a and b");
+    if ((double)f(x1) * (double)f(x2) > 0) {
+        Error e(PF_ERR_NUMERIC, "The function must have opposite signs at a and b");
+        e.infeasible = true;
+        throw e;
+    }
     int it = 0;
     while ((x2 - x1) / 2 >= tol && it < max_iter) {
         const double x = (x1 + x2) / 2;
@@ -162,14 +169,7 @@ void bounds_from_dos(TransformState &t, const Dos &rho) {
         const double n = quadgk([&](double x) { return rho(x); }, lo, hi, 1e-12, 1e-12, 10000000L);
         return n >= t.howmany ? -1 : +1;
     };
-    double d = 0.0;
-    try {
-        d = bisection(f, 0.0, 1.0, 1e-8, 500);
-    } catch (Error &e) {
-        // no interval around the target holds howmany states: the request is infeasible
-        e.infeasible = true;
-        throw;
-    }
+    const double d = bisection(f, 0.0, 1.0, 1e-8, 500);   // infeasible: no interval holds howmany states
     bound_fns(0, t.target, d, t.left, t.right);
 }
 

@@ -179,22 +179,32 @@ def test_fifo_admission_keeps_arrival_order(pkg, orc, cuda):
 
 
 def test_infeasible_request_is_rejected(pkg, orc, cuda):
-    """A request whose target cannot hold howmany states (here more states
-    than the whole space) is rejected with the reference's bisection error,
-    counted apart from failures; the pool goes on serving."""
+    """Requests the reference's planning cannot meet are rejected with its
+    bisection error, counted apart from failures, and the pool goes on
+    serving: more states than the whole space (the interval bisection), and
+    a target near the spectrum's edge for which no order meets the cutoff
+    (the order bisection; the oracle fails the same request the same way,
+    with the same explicit KPM probes)."""
     probs, rng = _problems(pkg, orc)
     op, H, s = probs[0]
     D = H.shape[0]
+    probes = orc.normalized_gaussian_probes(D, 24, np.random.default_rng(5))
+    x_edge = np.random.default_rng(4).random(D)
+    edge = ("rescaled", 0.8)
+    with pytest.raises(Exception, match="opposite signs"):
+        orc.plan_only(orc.CSROperator(H), x_edge, 50, edge, N=96, probes=probes)
     with pkg.SolverPool(workers=1) as pool:
         bad = pool.submit(op, _x0(rng, D, 1), D + 5, TARGET, **_kw(pkg, 1))
+        bad2 = pool.submit(op, x_edge, 50, edge, dos=pkg.DoSConfig(N=96, R=24, probes=probes))
         good = pool.submit(op, _x0(rng, D, 1), NEV, TARGET, **_kw(pkg, 2))
-        assert pool.wait(bad) == "rejected"
-        with pytest.raises(pkg._lib.PolfedRejected, match="opposite signs"):
-            pool.result(bad)
+        for r in (bad, bad2):
+            assert pool.wait(r) == "rejected"
+            with pytest.raises(pkg._lib.PolfedRejected, match="opposite signs"):
+                pool.result(r)
         vals, vecs = pool.result(good)
         _residuals_ok(H, vals, vecs)
         st = pool.stats()
-    assert st.rejected == 1 and st.failed == 0 and st.completed == 1
+    assert st.rejected == 2 and st.failed == 0 and st.completed == 1
 
 
 def test_destroy_wakes_waiting_threads(pkg, orc, cuda):
