@@ -16,6 +16,7 @@
 #include <cstring>
 #include <cstdio>
 #include <cstdlib>
+#include <limits>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -489,6 +490,66 @@ __global__ void k_put_beta(const double *__restrict__ R, int s, double *__restri
     }
 }
 
+// Eigenvalues of the symmetric tridiagonal matrix (diagonal d[0..n-1],
+// subdiagonal e[0..n-2]) and the last component of each eigenvector, by the
+// implicit QL iteration with shifts of tql2 (Bowdler, Martin, Reinsch and
+// Wilkinson, Numer. Math. 11, 293 (1968)), carrying only the last row of the
+// accumulated rotations.  d is replaced by the eigenvalues (unsorted), z
+// receives the matching last components.  Returns false if an eigenvalue
+// needs more than 60 iterations.
+static bool tridiag_ql_last_row(std::vector<double> &d, std::vector<double> e, std::vector<double> &z) {
+    const int n = (int)d.size();
+    z.assign(n, 0.0);
+    if (n == 0) return true;
+    z[n - 1] = 1.0;
+    e.resize(n, 0.0);
+    e[n - 1] = 0.0;
+    const double eps = std::numeric_limits<double>::epsilon();
+    for (int l = 0; l < n; ++l) {
+        int iter = 0, m;
+        do {
+            for (m = l; m < n - 1; ++m) {
+                const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+                if (std::fabs(e[m]) <= eps * dd) break;
+            }
+            if (m != l) {
+                if (iter++ == 60) return false;
+                double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+                double r = std::sqrt(g * g + 1.0);
+                g = d[m] - d[l] + e[l] / (g + (g >= 0 ? r : -r));
+                double sn = 1.0, c = 1.0, p = 0.0;
+                int i;
+                for (i = m - 1; i >= l; --i) {
+                    double f = sn * e[i];
+                    const double b = c * e[i];
+                    r = std::sqrt(f * f + g * g);
+                    e[i + 1] = r;
+                    if (r == 0.0) {
+                        d[i + 1] -= p;
+                        e[m] = 0.0;
+                        break;
+                    }
+                    sn = f / r;
+                    c = g / r;
+                    g = d[i + 1] - p;
+                    r = (d[i] - g) * sn + 2.0 * c * b;
+                    p = sn * r;
+                    d[i + 1] = g + p;
+                    g = c * r - b;
+                    f = z[i + 1];
+                    z[i + 1] = sn * z[i] + c * f;
+                    z[i] = c * z[i] - sn * f;
+                }
+                if (r == 0.0 && i >= l) continue;
+                d[l] -= p;
+                e[l] = g;
+                e[m] = 0.0;
+            }
+        } while (m != l);
+    }
+    return true;
+}
+
 static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
                          int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
                          double *stage_acc, int keep_extra, bool host_qr, bool *breakdown);
@@ -704,16 +765,44 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
         // convergence (ConvergenceInfo.jl:63-130)
         numiter += 1;
         if (nextcheck == numiter || numiter >= maxiter) {
-            // the projected matrix's leading k x k block (upper triangle read)
-            PF_CUDA(cudaMemcpy2DAsync(dT.p, (size_t)k * sizeof(double), Tfull.p, (size_t)maxdim * sizeof(double),
-                                      (size_t)k * sizeof(double), k, cudaMemcpyDeviceToDevice, st));
-            PF_CUSOLVER(cusolverDnDsyevd(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, dT.p, k, dW.p,
-                                         dwork.p, lwork, dinfo.p));
-            PF_CUDA(cudaMemcpyAsync(pinLam, dW.p, k * sizeof(double), cudaMemcpyDeviceToHost, st));
-            PF_CUDA(cudaMemcpy2DAsync(pinTail, s * sizeof(double), dT.p + (k - s), (size_t)k * sizeof(double),
-                                      s * sizeof(double), k, cudaMemcpyDeviceToHost, st));
+            std::vector<double> lam, tail, beta_last;
+            std::vector<int> idx(k);
+            auto order_idx = [&]() {
+                std::iota(idx.begin(), idx.end(), 0);
+                if (which == PF_WHICH_LR)
+                    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] > lam[y]; });
+                else
+                    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] < lam[y]; });
+            };
+            // the projected matrix's leading k x k block (upper triangle read) by
+            // the dense eigensolver: eigenvalues, and eigenvectors in dT
+            auto dense_eig = [&]() {
+                PF_CUDA(cudaMemcpy2DAsync(dT.p, (size_t)k * sizeof(double), Tfull.p, (size_t)maxdim * sizeof(double),
+                                          (size_t)k * sizeof(double), k, cudaMemcpyDeviceToDevice, st));
+                PF_CUSOLVER(cusolverDnDsyevd(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, dT.p, k,
+                                             dW.p, dwork.p, lwork, dinfo.p));
+                PF_CUDA(cudaMemcpyAsync(pinLam, dW.p, k * sizeof(double), cudaMemcpyDeviceToHost, st));
+                PF_CUDA(cudaMemcpy2DAsync(pinTail, s * sizeof(double), dT.p + (k - s), (size_t)k * sizeof(double),
+                                          s * sizeof(double), k, cudaMemcpyDeviceToHost, st));
+                PF_CUDA(cudaMemcpyAsync(pinInfo, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+                sync(h);
+                PF_CHECK(*pinInfo == 0, PF_ERR_NUMERIC, "projected eigenproblem failed to converge");
+                lam.assign(pinLam, pinLam + k);
+                tail.assign(pinTail, pinTail + (size_t)s * k);
+            };
+            // scalar Lanczos: T is tridiagonal, so the check's eigenvalues and
+            // last eigenvector components come from the host QL iteration
+            // (the converging check still takes the dense solver's vectors)
+            const bool tridiag = s == 1 && k <= 512;
+            if (tridiag) {
+                const size_t pitch = (size_t)(maxdim + 1) * sizeof(double);
+                PF_CUDA(cudaMemcpy2DAsync(pinLam, sizeof(double), Tfull.p, pitch, sizeof(double), k,
+                                          cudaMemcpyDeviceToHost, st));
+                if (k > 1)
+                    PF_CUDA(cudaMemcpy2DAsync(pinTail, sizeof(double), Tfull.p + 1, pitch, sizeof(double), k - 1,
+                                              cudaMemcpyDeviceToHost, st));
+            }
             PF_CUDA(cudaMemcpyAsync(pinB, dBeta, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
-            PF_CUDA(cudaMemcpyAsync(pinInfo, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             PF_CUDA(cudaMemcpyAsync(pinInfo + 1, dflag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
             sync(h);
             if (pinInfo[1] != 0) {
@@ -723,16 +812,15 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
                 clk.flush();
                 return;
             }
-            std::vector<double> lam(pinLam, pinLam + k), tail(pinTail, pinTail + (size_t)s * k);
-            std::vector<double> beta_last(pinB, pinB + ss);
-            const int info = *pinInfo;
-            PF_CHECK(info == 0, PF_ERR_NUMERIC, "projected eigenproblem failed to converge");
-            std::vector<int> idx(k);
-            std::iota(idx.begin(), idx.end(), 0);
-            if (which == PF_WHICH_LR)
-                std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] > lam[y]; });
-            else
-                std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] < lam[y]; });
+            beta_last.assign(pinB, pinB + ss);
+            bool have = false;
+            if (tridiag) {
+                lam.assign(pinLam, pinLam + k);
+                std::vector<double> sub(pinTail, pinTail + std::max(k - 1, 0));
+                have = tridiag_ql_last_row(lam, sub, tail);
+            }
+            if (!have) dense_eig();
+            order_idx();
             int conv = 0;
             double maxres = 0.0;
             const int nwant = std::min(howmany, k);
@@ -755,6 +843,11 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
             out.dim_hist.push_back(k);
             out.res_hist.push_back(maxres);
             if (conv == howmany || numiter >= maxiter) {
+                if (tridiag && have) {
+                    // the Ritz vectors need the eigenvectors: the dense solver, re-ordered
+                    dense_eig();
+                    order_idx();
+                }
                 // calculate_eigenvectors! (getvecs.jl:10-21): Psi = B Phi[:, idx[1:conv]]
                 if (keep_extra >= 0) conv = std::min(k, howmany + keep_extra);
                 out.vecs.alloc((size_t)D * std::max(conv, 1));
