@@ -190,12 +190,26 @@ def test_infeasible_request_is_rejected(pkg, orc, cuda):
     D = H.shape[0]
     probes = orc.normalized_gaussian_probes(D, 24, np.random.default_rng(5))
     x_edge = np.random.default_rng(4).random(D)
-    edge = ("rescaled", 0.8)
     with pytest.raises(Exception, match="opposite signs"):
-        orc.plan_only(orc.CSROperator(H), x_edge, 50, edge, N=96, probes=probes)
+        orc.plan_only(orc.CSROperator(H), x_edge, 50, ("rescaled", 0.8), N=96, probes=probes)
+    # the same kind of request with the pool's seeded probes: the first edge
+    # target that the direct solve cannot plan
+    dos = pkg.DoSConfig(N=96, R=24, seed=3)
+    edge = None
+    for eps in (0.8, 0.85, 0.9, 0.95):
+        for nev in (50, 20):
+            try:
+                pkg.polfed(op, x_edge, nev, ("rescaled", eps), vecs=False, dos=dos)
+            except pkg._lib.PolfedError as e:
+                if "opposite signs" in str(e):
+                    edge = (("rescaled", eps), nev)
+                    break
+        if edge:
+            break
+    assert edge is not None
     with pkg.SolverPool(workers=1) as pool:
         bad = pool.submit(op, _x0(rng, D, 1), D + 5, TARGET, **_kw(pkg, 1))
-        bad2 = pool.submit(op, x_edge, 50, edge, dos=pkg.DoSConfig(N=96, R=24, probes=probes))
+        bad2 = pool.submit(op, x_edge, edge[1], edge[0], vecs=False, dos=dos)
         good = pool.submit(op, _x0(rng, D, 1), NEV, TARGET, **_kw(pkg, 2))
         for r in (bad, bad2):
             assert pool.wait(r) == "rejected"
