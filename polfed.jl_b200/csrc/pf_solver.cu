@@ -550,6 +550,7 @@ static bool tridiag_ql_last_row(std::vector<double> &d, std::vector<double> e, s
     return true;
 }
 
+static pf_handle *aux_handle(pf_handle *h);
 static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double tol, double eigentol, int which,
                          int reorth_passes, const double *x0_ri, const BlockMap &fmap, LanczosOut &out,
                          double *stage_acc, int keep_extra, bool host_qr, bool *breakdown);
@@ -714,8 +715,214 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
                                             maxdim, dW.p, &lwork));
     DevArray<double> dwork((size_t)std::max(lwork, 1));
 
+    // A convergence check of the device form runs beside the next iteration:
+    // the check reads only T's leading k x k block, beta and the breakdown
+    // flag, all copied on the solve's stream before the next iteration is
+    // enqueued, and that iteration writes T outside the block and the basis
+    // beyond column k.  The next check is at least five iterations later, so
+    // the extra iteration is the one that comes next anyway; if the check
+    // says stop, it is discarded (the Ritz vectors use columns < k and the
+    // check's eigenvectors).  Block solves run the check's dense eigensolver
+    // on the auxiliary handle's stream; scalar solves run the host QL while
+    // the GPU works.  Every decision is the synchronous form's.
+    const bool speculate = !host_qr;
+    pf_handle *ah = (speculate && s > 1) ? aux_handle(h) : nullptr;
+    cudaEvent_t ev_data = nullptr, ev_eig = nullptr;
+    PF_CUDA(cudaEventCreateWithFlags(&ev_data, cudaEventDisableTiming));
+    PF_CUDA(cudaEventCreateWithFlags(&ev_eig, cudaEventDisableTiming));
+    // destroyed before the work arrays: an exception while a check is in
+    // flight on the auxiliary stream waits for it before they are freed
+    struct CheckGuard {
+        cudaEvent_t data, eig;
+        bool aux_pending = false;
+        ~CheckGuard() {
+            if (aux_pending) cudaEventSynchronize(eig);
+            cudaEventDestroy(data);
+            cudaEventDestroy(eig);
+        }
+    } guard{ev_data, ev_eig};
+
+    std::vector<double> lam, tail, beta_last;
+    std::vector<int> idx;
+    auto order_idx = [&](int kc) {
+        idx.resize(kc);
+        std::iota(idx.begin(), idx.end(), 0);
+        if (which == PF_WHICH_LR)
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] > lam[y]; });
+        else
+            std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] < lam[y]; });
+    };
+    // the dense eigensolver on T's leading kc x kc block (upper triangle
+    // read) on stream sst with solver handle sol: eigenvalues to pinLam, the
+    // last s rows of the eigenvectors to pinTail, eigenvectors kept in dT
+    auto enqueue_dense = [&](int kc, cudaStream_t sst, cusolverDnHandle_t sol) {
+        PF_CUSOLVER(cusolverDnSetStream(sol, sst));
+        PF_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, kc, dT.p, kc, dW.p,
+                                     dwork.p, lwork, dinfo.p));
+        PF_CUDA(cudaMemcpyAsync(pinLam, dW.p, kc * sizeof(double), cudaMemcpyDeviceToHost, sst));
+        PF_CUDA(cudaMemcpy2DAsync(pinTail, s * sizeof(double), dT.p + (kc - s), (size_t)kc * sizeof(double),
+                                  s * sizeof(double), kc, cudaMemcpyDeviceToHost, sst));
+        PF_CUDA(cudaMemcpyAsync(pinInfo, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, sst));
+    };
+    auto copy_block = [&](int kc) {
+        PF_CUDA(cudaMemcpy2DAsync(dT.p, (size_t)kc * sizeof(double), Tfull.p, (size_t)maxdim * sizeof(double),
+                                  (size_t)kc * sizeof(double), kc, cudaMemcpyDeviceToDevice, st));
+    };
+    auto take_dense = [&](int kc) {
+        PF_CHECK(*pinInfo == 0, PF_ERR_NUMERIC, "projected eigenproblem failed to converge");
+        lam.assign(pinLam, pinLam + kc);
+        tail.assign(pinTail, pinTail + (size_t)s * kc);
+    };
+    // the dense eigensolver now, on the solve's stream
+    auto dense_sync = [&](int kc) {
+        copy_block(kc);
+        enqueue_dense(kc, st, h->solver);
+        sync(h);
+        take_dense(kc);
+    };
+    // A check of T's leading kc x kc block.  launch: enqueue its inputs (and,
+    // for a dense check, the eigensolver: on the auxiliary stream when async).
+    struct Check {
+        int k = 0, numiter = 0;
+        bool tridiag = false, async_dense = false;
+    };
+    auto launch_check = [&](int kc, int nc, bool async) -> Check {
+        Check c;
+        c.k = kc;
+        c.numiter = nc;
+        c.tridiag = s == 1 && kc <= 512;
+        if (c.tridiag) {
+            // scalar Lanczos: T is tridiagonal -- its diagonal and subdiagonal
+            const size_t pitch = (size_t)(maxdim + 1) * sizeof(double);
+            PF_CUDA(cudaMemcpy2DAsync(pinLam, sizeof(double), Tfull.p, pitch, sizeof(double), kc,
+                                      cudaMemcpyDeviceToHost, st));
+            if (kc > 1)
+                PF_CUDA(cudaMemcpy2DAsync(pinTail, sizeof(double), Tfull.p + 1, pitch, sizeof(double), kc - 1,
+                                          cudaMemcpyDeviceToHost, st));
+        } else {
+            copy_block(kc);
+        }
+        PF_CUDA(cudaMemcpyAsync(pinB, dBeta, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
+        PF_CUDA(cudaMemcpyAsync(pinInfo + 1, dflag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PF_CUDA(cudaEventRecord(ev_data, st));
+        if (!c.tridiag) {
+            if (async && ah) {
+                PF_CUDA(cudaStreamWaitEvent(ah->stream, ev_data, 0));
+                enqueue_dense(kc, ah->stream, ah->solver);
+                PF_CUDA(cudaEventRecord(ev_eig, ah->stream));
+                c.async_dense = true;
+                guard.aux_pending = true;
+            } else {
+                enqueue_dense(kc, st, h->solver);
+                PF_CUDA(cudaEventRecord(ev_eig, st));
+            }
+        }
+        return c;
+    };
+    // finish: wait for the check's data, decide (ConvergenceInfo.jl:63-130).
+    // Returns 0 continue, 1 stop, 2 a device CholQR pass broke down.
+    auto finish_check = [&](const Check &c) -> int {
+        if (!c.tridiag) {
+            PF_CUDA(cudaEventSynchronize(ev_eig));
+            guard.aux_pending = false;
+        }
+        PF_CUDA(cudaEventSynchronize(ev_data));
+        if (pinInfo[1] != 0) {
+            PF_CHECK(breakdown != nullptr, PF_ERR_NUMERIC, "CholQR breakdown in the host-QR pass");
+            return 2;
+        }
+        beta_last.assign(pinB, pinB + ss);
+        bool have = false;
+        if (c.tridiag) {
+            lam.assign(pinLam, pinLam + c.k);
+            std::vector<double> sub(pinTail, pinTail + std::max(c.k - 1, 0));
+            have = tridiag_ql_last_row(lam, sub, tail);
+            if (!have) dense_sync(c.k);
+        } else {
+            take_dense(c.k);
+        }
+        order_idx(c.k);
+        int conv = 0;
+        double maxres = 0.0;
+        const int nwant = std::min(howmany, c.k);
+        for (int i = 0; i < nwant; ++i) {
+            const int pos = idx[i];
+            double ss2 = 0.0;
+            for (int a = 0; a < s; ++a) {
+                double v = 0.0;
+                for (int b2 = 0; b2 < s; ++b2) v += beta_last[a + b2 * s] * tail[b2 + (size_t)pos * s];
+                ss2 += v * v;
+            }
+            const double res = std::sqrt(ss2);
+            if (res > maxres || std::isnan(res)) maxres = std::isnan(res) ? res : std::max(maxres, res);
+            if (maxres < tol) ++conv;
+        }
+        out.numofchecks += 1;
+        out.converged = conv;
+        out.residual = maxres;
+        out.conv_hist.push_back(conv);
+        out.dim_hist.push_back(c.k);
+        out.res_hist.push_back(maxres);
+        // next_checking! (NextChecking.jl:23-42)
+        if (out.residual > 1e-2) nextcheck = c.numiter + 20;
+        else if (out.residual > 1e-3) nextcheck = c.numiter + 10;
+        else nextcheck = c.numiter + 5;
+        if (!(conv == howmany || c.numiter >= maxiter)) return 0;
+        if (c.tridiag && have) {
+            // the Ritz vectors need the eigenvectors: the dense solver, re-ordered
+            dense_sync(c.k);
+            order_idx(c.k);
+        }
+        return 1;
+    };
+    // calculate_eigenvectors! (getvecs.jl:10-21): Psi = B Phi[:, idx[1:conv]]
+    // for the stopping check of dimension kc
+    auto extract = [&](int kc) {
+        int conv = out.converged;
+        if (keep_extra >= 0) conv = std::min(kc, howmany + keep_extra);
+        out.vecs.alloc((size_t)D * std::max(conv, 1));
+        if (conv > 0) {
+            DevArray<double> phisel((size_t)kc * conv);
+            for (int i = 0; i < conv; ++i)
+                PF_CUDA(cudaMemcpyAsync(phisel.p + (size_t)i * kc, dT.p + (size_t)idx[i] * kc, kc * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, st));
+            PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, conv, (int)D, kc, &one, phisel.p, kc, basis.p, ldb,
+                                  &zero, out.vecs.p, conv));
+            // calculate_eigenvalues! / calculate_eigenresiduals! with the ORIGINAL H
+            DevArray<double> HV((size_t)D * conv), E(conv), res2(conv);
+            launch_step<double>(op, st, D, conv, out.vecs.p, nullptr, nullptr, HV.p, 0, 1.0, 0, 1.0, 0.0,
+                                StepFlags::Q, nullptr);
+            launch_coldots<double>(h, st, D, conv, out.vecs.p, HV.p, E.p);
+            launch_colresid(h, st, D, conv, HV.p, out.vecs.p, E.p, res2.p);
+            PF_CUDA(cudaMemcpyAsync(pinE, E.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
+            PF_CUDA(cudaMemcpyAsync(pinRes, res2.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
+            sync(h);
+            std::vector<double> hE(pinE, pinE + conv), hr(pinRes, pinRes + conv);
+            int ec = 0;
+            bool counting = true;
+            double maxe = 0.0;
+            out.resid.assign(conv, 0.0);
+            for (int i = 0; i < conv; ++i) {
+                const double rr = std::sqrt(std::max(hr[i], 0.0));
+                out.resid[i] = rr;
+                if (counting && rr < eigentol) ++ec;
+                else counting = false;
+                maxe = std::max(maxe, rr);
+            }
+            out.vals = hE;
+            out.eigenconverged = ec;
+            out.eigenresidual = maxe;
+        } else {
+            out.vals.clear();
+            out.eigenconverged = 0;
+            out.eigenresidual = 0.0;
+        }
+    };
+
     out.converged = 0;
     out.eigenconverged = 0;
+    Check pending;
+    bool have_pending = false;
     while (true) {
         // 1 tridiagonalization: QR(r) -> beta (BlockLanczosFactorization.jl:115-131)
         cudaEvent_t e0 = clk.mark();
@@ -762,140 +969,52 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
         cudaEvent_t e5 = clk.mark();
         clk.add(4, e4, e5);
 
-        // convergence (ConvergenceInfo.jl:63-130)
         numiter += 1;
-        if (nextcheck == numiter || numiter >= maxiter) {
-            std::vector<double> lam, tail, beta_last;
-            std::vector<int> idx(k);
-            auto order_idx = [&]() {
-                std::iota(idx.begin(), idx.end(), 0);
-                if (which == PF_WHICH_LR)
-                    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] > lam[y]; });
-                else
-                    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return lam[x] < lam[y]; });
-            };
-            // the projected matrix's leading k x k block (upper triangle read) by
-            // the dense eigensolver: eigenvalues, and eigenvectors in dT
-            auto dense_eig = [&]() {
-                PF_CUDA(cudaMemcpy2DAsync(dT.p, (size_t)k * sizeof(double), Tfull.p, (size_t)maxdim * sizeof(double),
-                                          (size_t)k * sizeof(double), k, cudaMemcpyDeviceToDevice, st));
-                PF_CUSOLVER(cusolverDnDsyevd(h->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, dT.p, k,
-                                             dW.p, dwork.p, lwork, dinfo.p));
-                PF_CUDA(cudaMemcpyAsync(pinLam, dW.p, k * sizeof(double), cudaMemcpyDeviceToHost, st));
-                PF_CUDA(cudaMemcpy2DAsync(pinTail, s * sizeof(double), dT.p + (k - s), (size_t)k * sizeof(double),
-                                          s * sizeof(double), k, cudaMemcpyDeviceToHost, st));
-                PF_CUDA(cudaMemcpyAsync(pinInfo, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-                sync(h);
-                PF_CHECK(*pinInfo == 0, PF_ERR_NUMERIC, "projected eigenproblem failed to converge");
-                lam.assign(pinLam, pinLam + k);
-                tail.assign(pinTail, pinTail + (size_t)s * k);
-            };
-            // scalar Lanczos: T is tridiagonal, so the check's eigenvalues and
-            // last eigenvector components come from the host QL iteration
-            // (the converging check still takes the dense solver's vectors)
-            const bool tridiag = s == 1 && k <= 512;
-            if (tridiag) {
-                const size_t pitch = (size_t)(maxdim + 1) * sizeof(double);
-                PF_CUDA(cudaMemcpy2DAsync(pinLam, sizeof(double), Tfull.p, pitch, sizeof(double), k,
-                                          cudaMemcpyDeviceToHost, st));
-                if (k > 1)
-                    PF_CUDA(cudaMemcpy2DAsync(pinTail, sizeof(double), Tfull.p + 1, pitch, sizeof(double), k - 1,
-                                              cudaMemcpyDeviceToHost, st));
-            }
-            PF_CUDA(cudaMemcpyAsync(pinB, dBeta, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
-            PF_CUDA(cudaMemcpyAsync(pinInfo + 1, dflag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-            sync(h);
-            if (pinInfo[1] != 0) {
-                // a device CholQR pass broke down since the last check
-                PF_CHECK(breakdown != nullptr, PF_ERR_NUMERIC, "CholQR breakdown in the host-QR pass");
+        // the previous iteration's check, which ran beside this iteration
+        if (have_pending) {
+            have_pending = false;
+            const int verdict = finish_check(pending);
+            if (verdict == 2) {
                 *breakdown = true;
-                clk.flush();
-                return;
+                break;
             }
-            beta_last.assign(pinB, pinB + ss);
-            bool have = false;
-            if (tridiag) {
-                lam.assign(pinLam, pinLam + k);
-                std::vector<double> sub(pinTail, pinTail + std::max(k - 1, 0));
-                have = tridiag_ql_last_row(lam, sub, tail);
+            if (verdict == 1) {
+                k = pending.k;            // this iteration is discarded
+                numiter = pending.numiter;
+                extract(k);
+                cudaEvent_t e6 = clk.mark();
+                clk.add(5, e5, e6);
+                break;
             }
-            if (!have) dense_eig();
-            order_idx();
-            int conv = 0;
-            double maxres = 0.0;
-            const int nwant = std::min(howmany, k);
-            for (int i = 0; i < nwant; ++i) {
-                const int pos = idx[i];
-                double ss2 = 0.0;
-                for (int a = 0; a < s; ++a) {
-                    double v = 0.0;
-                    for (int b2 = 0; b2 < s; ++b2) v += beta_last[a + b2 * s] * tail[b2 + (size_t)pos * s];
-                    ss2 += v * v;
-                }
-                const double res = std::sqrt(ss2);
-                if (res > maxres || std::isnan(res)) maxres = std::isnan(res) ? res : std::max(maxres, res);
-                if (maxres < tol) ++conv;
-            }
-            out.numofchecks += 1;
-            out.converged = conv;
-            out.residual = maxres;
-            out.conv_hist.push_back(conv);
-            out.dim_hist.push_back(k);
-            out.res_hist.push_back(maxres);
-            if (conv == howmany || numiter >= maxiter) {
-                if (tridiag && have) {
-                    // the Ritz vectors need the eigenvectors: the dense solver, re-ordered
-                    dense_eig();
-                    order_idx();
-                }
-                // calculate_eigenvectors! (getvecs.jl:10-21): Psi = B Phi[:, idx[1:conv]]
-                if (keep_extra >= 0) conv = std::min(k, howmany + keep_extra);
-                out.vecs.alloc((size_t)D * std::max(conv, 1));
-                if (conv > 0) {
-                    DevArray<double> phisel((size_t)k * conv);
-                    for (int i = 0; i < conv; ++i)
-                        PF_CUDA(cudaMemcpyAsync(phisel.p + (size_t)i * k, dT.p + (size_t)idx[i] * k, k * sizeof(double),
-                                                cudaMemcpyDeviceToDevice, st));
-                    PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, conv, (int)D, k, &one, phisel.p, k, basis.p, ldb,
-                                          &zero, out.vecs.p, conv));
-                    // calculate_eigenvalues! / calculate_eigenresiduals! with the ORIGINAL H
-                    DevArray<double> HV((size_t)D * conv), E(conv), res2(conv);
-                    launch_step<double>(op, st, D, conv, out.vecs.p, nullptr, nullptr, HV.p, 0, 1.0, 0, 1.0, 0.0,
-                                        StepFlags::Q, nullptr);
-                    launch_coldots<double>(h, st, D, conv, out.vecs.p, HV.p, E.p);
-                    launch_colresid(h, st, D, conv, HV.p, out.vecs.p, E.p, res2.p);
-                    PF_CUDA(cudaMemcpyAsync(pinE, E.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
-                    PF_CUDA(cudaMemcpyAsync(pinRes, res2.p, conv * sizeof(double), cudaMemcpyDeviceToHost, st));
-                    sync(h);
-                    std::vector<double> hE(pinE, pinE + conv), hr(pinRes, pinRes + conv);
-                    int ec = 0;
-                    bool counting = true;
-                    double maxe = 0.0;
-                    out.resid.assign(conv, 0.0);
-                    for (int i = 0; i < conv; ++i) {
-                        const double rr = std::sqrt(std::max(hr[i], 0.0));
-                        out.resid[i] = rr;
-                        if (counting && rr < eigentol) ++ec;
-                        else counting = false;
-                        maxe = std::max(maxe, rr);
-                    }
-                    out.vals = hE;
-                    out.eigenconverged = ec;
-                    out.eigenresidual = maxe;
-                } else {
-                    out.vals.clear();
-                    out.eigenconverged = 0;
-                    out.eigenresidual = 0.0;
-                }
-            }
-            // next_checking! (NextChecking.jl:23-42)
-            if (out.residual > 1e-2) nextcheck = numiter + 20;
-            else if (out.residual > 1e-3) nextcheck = numiter + 10;
-            else nextcheck = numiter + 5;
+        }
+        // convergence (ConvergenceInfo.jl:63-130)
+        if (nextcheck == numiter || numiter >= maxiter) {
+            const bool async = speculate && numiter < maxiter;
+            const Check c = launch_check(k, numiter, async);
             cudaEvent_t e6 = clk.mark();
             clk.add(5, e5, e6);
+            if (async) {
+                pending = c;
+                have_pending = true;
+                continue;
+            }
+            const int verdict = finish_check(c);
+            if (verdict == 2) {
+                *breakdown = true;
+                break;
+            }
+            if (verdict == 1) {
+                extract(k);
+                cudaEvent_t e7 = clk.mark();
+                clk.add(5, e6, e7);
+                break;
+            }
         }
-        if (out.converged == howmany || numiter >= maxiter) break;
+    }
+    if (breakdown && *breakdown) {
+        sync(h);
+        clk.flush();
+        return;
     }
     sync(h);
     clk.flush();
