@@ -70,12 +70,10 @@ struct DescTraits<CsrDesc<T>> {
 constexpr int kThreads = 256;
 
 // Deterministic "last block reduces" epilogue: every block writes its
-// per-column partials and the block that finishes last sums them.  Its warps
-// share the work: warp w takes values w, w + nwarps, ... (up to 16 at a time),
-// each lane sums the partials of blocks lane, lane + 32, ... in block order --
-// the loads of a lane are independent, so they are in flight together -- and a
-// fixed butterfly of shuffles combines the 32 lane sums.  Every value is summed
-// with the same association on every run.
+// per-column partials, the block that finishes last sums them in block order.
+// The partials are read through L2 (__ldcg: other blocks wrote them before
+// the counter told this block it is last) in unrolled runs, so a run's loads
+// are in flight together while the sum keeps block order.
 __device__ void finish_reduction(int nvals, const double *blockvals, double *partials,
                                  unsigned int *counter, double *out) {
     __shared__ bool last;
@@ -90,28 +88,13 @@ __device__ void finish_reduction(int nvals, const double *blockvals, double *par
     __syncthreads();
     if (last) {
         __threadfence();
-        constexpr int J = 16;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
         const unsigned int nb = gridDim.x;
-        for (int base = 0; base < nvals; base += J * nw) {
-            double acc[J];
-#pragma unroll
-            for (int j = 0; j < J; ++j) acc[j] = 0.0;
-            for (unsigned int b = lane; b < nb; b += 32) {
-                const double *row = partials + (size_t)b * nvals;
-#pragma unroll
-                for (int j = 0; j < J; ++j) {
-                    const int c = base + warp + nw * j;
-                    if (c < nvals) acc[j] += __ldcg(row + c);
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < J; ++j) {
-                double v = acc[j];
-                for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                const int c = base + warp + nw * j;
-                if (lane == 0 && c < nvals) out[c] = v;
-            }
+        for (int c = threadIdx.x; c < nvals; c += blockDim.x) {
+            double acc = 0.0;
+            const double *col = partials + c;
+#pragma unroll 8
+            for (unsigned int b = 0; b < nb; ++b) acc += __ldcg(col + (size_t)b * nvals);
+            out[c] = acc;
         }
         if (threadIdx.x == 0) *counter = 0u;
     }

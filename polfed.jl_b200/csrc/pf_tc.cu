@@ -11,7 +11,8 @@
 // first pass of CGS2: the FP64 second pass removes what the first leaves.
 //
 // One CTA of 128 threads owns 128 basis columns (the MMA's M) and a chunk of
-// rows (the contraction K, split over CTAs).  Per stage of 64 rows the threads
+// rows (the contraction K, split over CTAs: chunks of at least 256 rows, about
+// a thousand of them at large D, so that several CTAs share each SM).  Per stage of 64 rows the threads
 // read the FP64 values (coalesced along the basis columns), split them and
 // write the BF16 tiles to shared memory in the MMA's K-major core-matrix
 // layout (8 rows x 16 bytes per core matrix, no swizzle); one elected thread
@@ -31,7 +32,6 @@ namespace pf {
 constexpr int kTcThreads = 128;
 constexpr int kTcM = 128;        // basis columns per CTA (MMA M)
 constexpr int kTcStage = 64;     // rows of D per stage (4 MMA k-steps of 16)
-constexpr int kTcChunk = 2048;   // rows of D per CTA
 constexpr long kTcWaitLimit = 1L << 22;
 
 // Shared memory: A hi / lo tiles (128 x 64 BF16 each), B hi / lo tiles
@@ -120,7 +120,7 @@ __device__ __forceinline__ void split_bf16(double v, __nv_bfloat16 &hi, __nv_bfl
 template <int NT>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_gram_bf16x3(const double *__restrict__ B, int ldb, int nB, const double *__restrict__ r, int s, uint32_t D,
-                  float *__restrict__ part, int Mpad, int *err) {
+                  uint32_t chunk, float *__restrict__ part, int Mpad, int *err) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *a_hi = smem, *a_lo = smem + TcSmem::a_bytes;
     unsigned char *b_hi = smem + 2 * TcSmem::a_bytes, *b_lo = b_hi + TcSmem::b_bytes(NT);
@@ -144,11 +144,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     // kind::f16 with BF16 A and B, FP32 accumulator, both K-major, M = 128, N = NT
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
     const int m0 = blockIdx.x * kTcM;
-    const uint32_t k_beg = blockIdx.y * (uint32_t)kTcChunk;
-    const uint32_t k_end = min(D, k_beg + (uint32_t)kTcChunk);
+    const uint32_t k_beg = blockIdx.y * chunk;
+    const uint32_t k_end = min(D, k_beg + chunk);
     uint32_t phase = 0;
     bool ok = true, any = false;
     for (uint32_t k = k_beg; k < k_end && ok; k += kTcStage) {
+#pragma unroll 8
         for (int idx = tid; idx < kTcM * kTcStage; idx += kTcThreads) {
             const int m = idx % kTcM, kk = idx / kTcM;
             const uint32_t row = k + kk;
@@ -159,6 +160,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             *reinterpret_cast<__nv_bfloat16 *>(a_hi + off) = hi;
             *reinterpret_cast<__nv_bfloat16 *>(a_lo + off) = lo;
         }
+#pragma unroll 4
         for (int idx = tid; idx < NT * kTcStage; idx += kTcThreads) {
             const int n = idx % NT, kk = idx / NT;
             const uint32_t row = k + kk;
@@ -210,27 +212,42 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;\n" ::"r"(tmem) : "memory");
 }
 
-// G[i + c * nB] = sum over row chunks of part (FP64 sums in chunk order).
+// G[i + c * nB] = sum over row chunks of part, one warp per entry: lane l
+// sums chunks l, l + 32, ... in FP64, then a fixed butterfly of shuffles
+// (the same association every run).
 __global__ void k_gram_reduce(const float *__restrict__ part, int nchunks, int Mpad, int NT, int nB, int s,
                               double *__restrict__ G) {
-    const int n = nB * s;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-        const int i = t % nB, c = t / nB;
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t n = (int64_t)nB * s;
+    for (int64_t t = w0; t < n; t += nw) {
+        const int i = (int)(t % nB), c = (int)(t / nB);
         double acc = 0.0;
-        for (int q = 0; q < nchunks; ++q) acc += (double)part[((size_t)q * Mpad + i) * NT + c];
-        G[t] = acc;
+        for (int q = lane; q < nchunks; q += 32) acc += (double)part[((size_t)q * Mpad + i) * NT + c];
+        for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) G[t] = acc;
     }
+}
+
+// Rows of D per CTA: D / 1024 rounded up to whole 64-row stages, at least 256.
+static int64_t gram_chunk_rows(int64_t D) {
+    int64_t c = (D + 1023) / 1024;
+    c = (c + kTcStage - 1) / kTcStage * kTcStage;
+    return std::max<int64_t>(c, 256);
 }
 
 template <int NT>
 static void launch_gram(pf_handle *h, cudaStream_t st, int64_t D, int nB, const double *B, int ldb, const double *r,
-                        int s, double *G, float *part, int mtiles, int nchunks, int *err) {
+                        int s, double *G, float *part, int mtiles, int nchunks, int64_t chunk, int *err) {
     auto kern = k_gram_bf16x3<NT>;
     const int smem = TcSmem::total(NT);
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    kern<<<dim3(mtiles, nchunks), kTcThreads, smem, st>>>(B, ldb, nB, r, s, (uint32_t)D, part, mtiles * kTcM, err);
+    kern<<<dim3(mtiles, nchunks), kTcThreads, smem, st>>>(B, ldb, nB, r, s, (uint32_t)D, (uint32_t)chunk, part,
+                                                          mtiles * kTcM, err);
     PF_CUDA(cudaGetLastError());
-    const int grid = std::max(1, std::min(h->num_sms * 4, (nB * s + 255) / 256));
+    const int64_t warps = (int64_t)nB * s;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)h->num_sms * 8, (warps + 7) / 8));
     k_gram_reduce<<<grid, 256, 0, st>>>(part, nchunks, mtiles * kTcM, NT, nB, s, G);
     PF_CUDA(cudaGetLastError());
     count_launches(2);
@@ -238,7 +255,8 @@ static void launch_gram(pf_handle *h, cudaStream_t st, int64_t D, int nB, const 
 
 size_t gram_bf16_workspace(int64_t D, int nB, int s) {
     const int NT = s <= 8 ? 8 : (s <= 16 ? 16 : 32);
-    const int64_t mtiles = (nB + kTcM - 1) / kTcM, nchunks = (D + kTcChunk - 1) / kTcChunk;
+    const int64_t chunk = gram_chunk_rows(D);
+    const int64_t mtiles = (nB + kTcM - 1) / kTcM, nchunks = (D + chunk - 1) / chunk;
     return (size_t)nchunks * mtiles * kTcM * NT * sizeof(float) + 256;
 }
 
@@ -251,12 +269,13 @@ void gram_bf16x3(pf_handle *h, cudaStream_t st, int64_t D, int nB, const double 
     PF_CHECK(s >= 1 && s <= 32, PF_ERR_UNSUPPORTED, "the tensor-core Gram product needs 1 <= s <= 32");
     PF_CHECK(nB >= 1 && D >= 1 && ldb >= nB, PF_ERR_INVALID, "invalid Gram product shape");
     const int mtiles = (nB + kTcM - 1) / kTcM;
-    const int nchunks = (int)((D + kTcChunk - 1) / kTcChunk);
+    const int64_t chunk = gram_chunk_rows(D);
+    const int nchunks = (int)((D + chunk - 1) / chunk);
     PF_CHECK(nchunks <= 65535, PF_ERR_UNSUPPORTED, "block too tall for the tensor-core Gram product");
     float *part = static_cast<float *>(work);
-    if (s <= 8) launch_gram<8>(h, st, D, nB, B, ldb, r, s, G, part, mtiles, nchunks, err);
-    else if (s <= 16) launch_gram<16>(h, st, D, nB, B, ldb, r, s, G, part, mtiles, nchunks, err);
-    else launch_gram<32>(h, st, D, nB, B, ldb, r, s, G, part, mtiles, nchunks, err);
+    if (s <= 8) launch_gram<8>(h, st, D, nB, B, ldb, r, s, G, part, mtiles, nchunks, chunk, err);
+    else if (s <= 16) launch_gram<16>(h, st, D, nB, B, ldb, r, s, G, part, mtiles, nchunks, chunk, err);
+    else launch_gram<32>(h, st, D, nB, B, ldb, r, s, G, part, mtiles, nchunks, chunk, err);
 }
 
 }  // namespace pf
