@@ -820,6 +820,19 @@ def apply_sweep():
     return 0
 
 
+def profile_solve():
+    """One complete solve of the workload (a fresh realisation) through
+    pkg.polfed, no pool: a bounded case for an ncu launch list of a solve."""
+    import __graft_entry__ as ge
+    pkg = ge.load_package()
+    ops, x0s = make_realisations(pkg, 2, 1000)
+    for i in range(2):
+        vals, _, rep = solve(pkg, ops[i], x0s[i], seed=17 + i)
+    print(json.dumps({"profile_solve": True, "pairs": len(vals), "order": rep.spectral.order,
+                      "launches": int(rep.benchmark.kernel_launches)}))
+    return 0
+
+
 def profile_kpm():
     """KPM on the workload's operator at its block width: one 64-probe block of
     normalised Gaussian probes, 40 moments (20 doubling steps with fused
@@ -961,6 +974,8 @@ def main():
                     help="only run two short Chebyshev filters on one realisation (a bounded case for ncu)")
     ap.add_argument("--apply-sweep", action="store_true",
                     help="single-vector XXZ H-apply at L=18..24 (the reference's published timings)")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="only run two complete solves of the workload, no pool (a bounded case for ncu)")
     ap.add_argument("--profile-kpm", action="store_true",
                     help="only run 40 KPM moments of one 64-probe block (a bounded case for ncu)")
     ap.add_argument("--profile-gram", action="store_true",
@@ -976,6 +991,8 @@ def main():
         return profile_step()
     if args.apply_sweep:
         return apply_sweep()
+    if args.profile_solve:
+        return profile_solve()
     if args.profile_kpm:
         return profile_kpm()
     if args.profile_gram:

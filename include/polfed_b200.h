@@ -298,9 +298,11 @@ typedef struct pf_params {
                                     once all nev targets meet eigentol. */
     int    autotune;             /* 1: time the step-kernel variants once per (op, s, dtype) */
     int    host_qr;              /* 0: the s x s algebra of a Lanczos iteration stays on the device
-                                    (a CholQR breakdown restarts the run with the host QR); 1: every
+                                    (a CholQR breakdown restarts the run with the host QR) and each
+                                    convergence check runs beside the next iteration; 1: every
                                     iteration reads its Gram matrices back and factors them on the
-                                    host (the same R bit for bit; Householder QR on a breakdown) */
+                                    host (the same R bit for bit; Householder QR on a breakdown) and
+                                    checks run in turn.  Both give the same results. */
 } pf_params;
 
 #define PF_REPORT_MAX_CHECKS 128
@@ -462,7 +464,9 @@ int pf_pool_wait(pf_pool *pool, int64_t request, double timeout_s, int *state);
  * started and finished (times[3]; -1 for what has not happened yet).  Valid
  * until the request is fetched, cancelled or collected. */
 int pf_pool_request_times(pf_pool *pool, int64_t request, double *times);
-/* Drop a queued request (a running one finishes and is then discarded). */
+/* Drop a queued request.  A running one finishes and is then discarded: its
+ * worker still writes the host output arrays given at submission, which must
+ * stay valid until the pool is destroyed. */
 int pf_pool_cancel(pf_pool *pool, int64_t request);
 int pf_pool_get_stats(pf_pool *pool, pf_pool_stats *stats);
 

@@ -487,6 +487,7 @@ class SolverPool:
         _lib.check(_lib.load().pf_pool_create(device, int(workers), float(hbm_budget or 0.0), ctypes.byref(h)))
         self._pool = h
         self._pending: dict = {}
+        self._cancelled: list = []   # result arrays of cancelled requests a worker may still write
         # native calls in flight from any Python thread; close() frees the pool
         # only after the last of them has returned
         self._cv = threading.Condition()
@@ -543,6 +544,7 @@ class SolverPool:
         _lib.check(_lib.load().pf_pool_destroy(pool))
         self._pool = None
         self._pending.clear()
+        self._cancelled.clear()
 
     def __enter__(self):
         return self
@@ -695,8 +697,13 @@ class SolverPool:
         return res
 
     def cancel(self, request: int):
+        """Drop a queued request.  A request that has already started runs to
+        the end and is then discarded; its worker still writes the result
+        arrays, so they stay referenced until the pool is closed."""
         _lib.check(self._native("cancel", int(request)))
-        self._pending.pop(request, None)
+        held = self._pending.pop(request, None)
+        if held is not None:
+            self._cancelled.append(held)
 
     def stats(self) -> PoolStats:
         st = _lib.pf_pool_stats()

@@ -8,6 +8,8 @@ served path (submit / poll / result) must admit requests only while their
 footprints fit the HBM budget, keep FIFO order, release failed and cancelled
 requests, and report latency percentiles.
 """
+import time
+
 import numpy as np
 import pytest
 
@@ -131,6 +133,27 @@ def test_failed_and_cancelled_requests_are_released(pkg, orc, cuda):
             pool.poll(dropped)
         st = pool.stats()
     assert st.failed == 1 and st.completed == 1 and st.submitted == 3
+
+
+def test_cancelling_a_running_request_keeps_its_arrays(pkg, orc, cuda):
+    """A request that has already started runs to the end after cancel and its
+    worker still writes the host result arrays: the pool keeps them alive
+    until it is closed, and goes on serving."""
+    probs, rng = _problems(pkg, orc)
+    op, H, s = probs[0]
+    D = H.shape[0]
+    big = pkg.xxz_hamiltonian(16, 8, 1.0, 1.0, 5.0, rng=np.random.default_rng(3))
+    with pkg.SolverPool(workers=1) as pool:
+        r = pool.submit(big, np.random.default_rng(4).random(big.dim), NEV, TARGET, **_kw(pkg, 5))
+        for _ in range(2000):
+            if pool.poll(r) != "queued":
+                break
+            time.sleep(0.005)
+        pool.cancel(r)
+        assert len(pool._cancelled) == 1
+        vals, vecs = pool.result(pool.submit(op, _x0(rng, D, 1), NEV, TARGET, **_kw(pkg, 6)))
+        _residuals_ok(H, vals, vecs)
+    assert pool._cancelled == []
 
 
 def _blocked_pool_order(pkg, policy, max_wait):
