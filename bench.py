@@ -751,17 +751,22 @@ def run_c3(args, local_rank):
     return 0
 
 
-def profile_step():
+def profile_step(width=None, profile=0):
     """Two order-30 Chebyshev filters on one realisation of the workload's
-    operator (s = 8, FP64) with the autotuned step: a small, bounded case for
-    ncu captures of the step kernel."""
+    operator (s = 8, FP64) with the autotuned step, or with the given step
+    width and profile (the autotuner's timings are not those of a run under
+    ncu, which serialises every launch): a small, bounded case for ncu
+    captures of the step kernel."""
     import numpy as np
     import torch
     import __graft_entry__ as ge
     pkg = ge.load_package()
     ops, x0s = make_realisations(pkg, 1, 1000)
     op = ops[0]
-    width, _ = pkg.autotune(op, WORKLOAD["blocksize"], "fp64")
+    if width is None:
+        width, _ = pkg.autotune(op, WORKLOAD["blocksize"], "fp64")
+    else:
+        pkg.set_step_width(op, WORKLOAD["blocksize"], width, "fp64", profile)
     D, s = op.dim, WORKLOAD["blocksize"]
     X = pkg.col_major(D, s)
     X.copy_(torch.from_numpy(np.ascontiguousarray(x0s[0])).cuda())
@@ -962,7 +967,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch", type=int, default=4, help="solves in flight together per step")
+    ap.add_argument("--batch", type=int, default=16, help="solves in flight together per step")
     ap.add_argument("--serve", action="store_true", help="run the seeded Poisson request stream instead")
     ap.add_argument("--disorder", action="store_true", help="run the 288-realisation disorder batch instead")
     ap.add_argument("--requests", type=int, default=24)
@@ -977,6 +982,9 @@ def main():
                     help="two order-2 filters on J1-J2 L=24 (a bounded large-D case for ncu)")
     ap.add_argument("--profile-step", action="store_true",
                     help="only run two short Chebyshev filters on one realisation (a bounded case for ncu)")
+    ap.add_argument("--step-width", type=int, default=None,
+                    help="with --profile-step: this step width (columns per thread) instead of the autotuner's")
+    ap.add_argument("--step-profile", type=int, default=0, help="with --step-width: the step profile")
     ap.add_argument("--apply-sweep", action="store_true",
                     help="single-vector XXZ H-apply at L=18..24 (the reference's published timings)")
     ap.add_argument("--profile-solve", action="store_true",
@@ -993,7 +1001,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.profile_step:
-        return profile_step()
+        return profile_step(args.step_width, args.step_profile)
     if args.apply_sweep:
         return apply_sweep()
     if args.profile_solve:

@@ -413,58 +413,12 @@ static void ascending_prefix(pf_handle *h, int64_t D, int nconv, std::vector<dou
 // the solve's stream, so an iteration makes no host round trip: the host
 // reads the device only at convergence checks.
 
-// One CholQR pass: G = R^T R (upper R, column-major s x s) from the upper
-// triangle of G, with host_cholesky's operations in its order, each rounded
-// on its own (no fused multiply-adds), so R equals host_cholesky's bit for
-// bit; and rtot_out = R * rtot_in (rtot_in null: the identity) with the
-// host's product loop.  A pivot host_cholesky rejects sets *flag and gives
-// R = I (the triangular solve then leaves the block as it is).
-__global__ void k_small_chol(const double *__restrict__ G, int s, double *__restrict__ R,
-                             const double *__restrict__ rtot_in, double *__restrict__ rtot_out, int *flag) {
-    extern __shared__ double sh[];
-    double *g = sh, *r = sh + s * s;
-    __shared__ int bad;
-    const int n = s * s;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        g[i] = G[i];
-        r[i] = 0.0;
-    }
-    if (threadIdx.x == 0) bad = 0;
-    __syncthreads();
-    for (int j = 0; j < s; ++j) {
-        if (threadIdx.x == 0) {
-            const double gjj = g[j + j * s];
-            double d = gjj;
-            for (int k = 0; k < j; ++k) d = __dsub_rn(d, __dmul_rn(r[k + j * s], r[k + j * s]));
-            if (!(d > 1e-28 * fmax(1.0, fabs(gjj))) || !isfinite(d) || d <= 1e-13 * fabs(gjj)) bad = 1;
-            else r[j + j * s] = sqrt(d);
-        }
-        __syncthreads();
-        if (bad) break;
-        const double rjj = r[j + j * s];
-        for (int i = j + 1 + threadIdx.x; i < s; i += blockDim.x) {
-            double v = g[j + i * s];
-            for (int k = 0; k < j; ++k) v = __dsub_rn(v, __dmul_rn(r[k + j * s], r[k + i * s]));
-            r[j + i * s] = __ddiv_rn(v, rjj);
-        }
-        __syncthreads();
-    }
-    if (bad) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) r[i] = (i % (s + 1) == 0) ? 1.0 : 0.0;
-        if (threadIdx.x == 0) *flag = 1;
-        __syncthreads();
-    }
-    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-        R[idx] = r[idx];
-        const int i = idx % s, j = idx / s;
-        double v = 0.0;
-        for (int k = i; k <= j; ++k) {
-            const double t = rtot_in ? rtot_in[k + j * s] : (k == j ? 1.0 : 0.0);
-            v = __dadd_rn(v, __dmul_rn(r[i + k * s], t));
-        }
-        rtot_out[idx] = v;
-    }
-}
+// One CholQR pass for blocks wider than the fused passes take (s > 32):
+// small_chol (pf_blocks.cu) factors the Gram matrix with host_cholesky's
+// operations in its order, each rounded on its own, so R equals
+// host_cholesky's bit for bit, and forms the running product R * rtot_in
+// with the host's product loop.  A pivot host_cholesky rejects sets *flag
+// and gives R = I (the triangular solve then leaves the block as it is).
 
 // alpha (the overlap V^T W, s x s column-major) made symmetric from its upper
 // triangle in place, and written as the diagonal block of T at (k0, k0).
@@ -599,8 +553,14 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
     const size_t ss = (size_t)s * s;
     // small device state: alpha, the pass's R, two running products, beta,
     // the Gram matrix, the breakdown flag
-    DevArray<double> small(6 * ss), G((size_t)maxdim * s);
+    DevArray<double> small(7 * ss), G((size_t)maxdim * s);
     double *dA = small.p, *dR = dA + ss, *dRt0 = dR + ss, *dRt1 = dRt0 + ss, *dBeta = dRt1 + ss, *dG = dBeta + ss;
+    double *dR2 = dG + ss;
+    // blocks of up to 32 columns take the fused block passes (pf_blocks.cu)
+    const bool fused = s <= kBlkMaxS;
+    DevArray<double> bpart(fused ? blk_partial_doubles(D, s) : 0);
+    DevArray<unsigned> bcount(fused ? 1 : 0);
+    if (fused) PF_CUDA(cudaMemsetAsync(bcount.p, 0, sizeof(unsigned), st));
     DevArray<int> dflag(1);
     PF_CUDA(cudaMemsetAsync(dflag.p, 0, sizeof(int), st));
     DevArray<double> Tfull((size_t)maxdim * maxdim);   // the projected matrix, column-major
@@ -622,42 +582,105 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
     double *pinE = pinTail + (size_t)s * maxdim;        // maxdim
     double *pinRes = pinE + maxdim;                     // maxdim
     int *pinInfo = reinterpret_cast<int *>(pinRes + maxdim);   // [info, breakdown flag]
-    const int small_smem = (int)(2 * ss * sizeof(double));
-    if (!host_qr && small_smem > 48 * 1024)
-        PF_CUDA(cudaFuncSetAttribute(k_small_chol, cudaFuncAttributeMaxDynamicSharedMemorySize, small_smem));
 
     auto append = [&](const double *src, int col) {
         PF_CUDA(cudaMemcpy2DAsync(basis.p + col, (size_t)ldb * sizeof(double), src, (size_t)s * sizeof(double),
                                   (size_t)s * sizeof(double), (size_t)D, cudaMemcpyDeviceToDevice, st));
     };
+    auto pass_args = [&](double *W) {
+        BlkPass p;
+        p.D = D;
+        p.s = s;
+        p.W = W;
+        p.partial = bpart.p;
+        p.counter = bcount.p;
+        p.G = dG;
+        p.flag = dflag.p;
+        p.T = Tfull.p;
+        p.ldT = maxdim;
+        return p;
+    };
     // alpha = V^T W (s x s), upper triangle symmetrised, into T at (k0, k0)
     auto overlap = [&](const double *Vb, const double *Wb, int k0) {
+        if (fused) {
+            BlkPass p = pass_args(const_cast<double *>(Vb));
+            p.Y = Wb;
+            p.flags = BLK_GRAM;
+            p.epi = EPI_ALPHA;
+            p.k = k0;
+            p.keep = dA;
+            blk_pass(st, p);
+            return;
+        }
         PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, Vb, s, Wb, s, &zero, dA, s));
         k_put_alpha<<<1, 256, 0, st>>>(dA, s, Tfull.p, maxdim, k0);
         PF_CUDA(cudaGetLastError());
         count_launches(1);
     };
-    // Q R = W in place (CholQR2) on the device; R ends in dRt1
-    auto qr_device = [&](double *W) {
+    // r -= vlast alpha + vprev beta^T (orthogonalization.jl:31-33; vprev null:
+    // the first iteration, no beta term)
+    auto update = [&](double *rb, const double *Vb, const double *Vp) {
+        if (fused) {
+            blk_update(st, D, s, rb, Vb, Vp, dA, dBeta);
+            return;
+        }
+        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, dA, s, Vb, s, &one, rb, s));
+        if (Vp)
+            PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, s, (int)D, s, &mone, dBeta, s, Vp, s, &one, rb, s));
+    };
+    // Q R = W in place (CholQR2) on the device; R ends in dRt1.  Fused: Q is
+    // also written into the basis at column kcol and beta = R into T.
+    auto qr_device = [&](double *W, int kcol) {
+        if (fused) {
+            BlkPass p = pass_args(W);
+            p.flags = BLK_GRAM;
+            p.epi = EPI_CHOL;
+            p.R = dR;
+            p.rtot_out = dRt0;
+            blk_pass(st, p);
+            p.flags = BLK_SOLVE | BLK_GRAM;
+            p.epi = EPI_CHOL_BETA;
+            p.Rs = dR;
+            p.R = dR2;
+            p.rtot_in = dRt0;
+            p.rtot_out = dRt1;
+            p.k = kcol;
+            p.keep = dBeta;
+            blk_pass(st, p);
+            BlkPass q = pass_args(W);
+            q.flags = BLK_SOLVE | BLK_APPEND;
+            q.Rs = dR2;
+            q.basis = basis.p;
+            q.ldb = ldb;
+            q.col = kcol;
+            blk_pass(st, q);
+            return;
+        }
         for (int pass = 0; pass < 2; ++pass) {
             PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, dG, s));
-            k_small_chol<<<1, 64, small_smem, st>>>(dG, s, dR, pass == 0 ? nullptr : dRt0, pass == 0 ? dRt0 : dRt1,
-                                                   dflag.p);
-            PF_CUDA(cudaGetLastError());
-            count_launches(1);
+            small_chol(st, dG, s, dR, pass == 0 ? nullptr : dRt0, pass == 0 ? dRt0 : dRt1, dflag.p);
             // W^T <- R^{-T} W^T  (i.e. W <- W R^{-1})
             PF_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, s,
                                   (int)D, &one, dR, s, W, s));
         }
     };
     // Q R = W in place with the Gram matrices read back (CholQR2; Householder
-    // on the host if it breaks down); R ends in dRt1
-    auto qr_host = [&](double *W) {
+    // on the host if it breaks down); R ends in dRt1.  Returns whether Q was
+    // also written into the basis at column kcol (the fused passes).
+    auto qr_host = [&](double *W, int kcol) -> bool {
         std::vector<double> Rtot((size_t)s * s, 0.0);
         for (int i = 0; i < s; ++i) Rtot[i + i * s] = 1.0;
         bool ok = true;
         for (int pass = 0; pass < 2 && ok; ++pass) {
-            PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, dG, s));
+            if (fused) {
+                // the Gram matrix of W (pass 0) or of W R1^{-1} (pass 1, solved in place)
+                BlkPass p = pass_args(W);
+                p.flags = pass == 0 ? BLK_GRAM : (BLK_SOLVE | BLK_GRAM);
+                p.Rs = dR;
+                blk_pass(st, p);
+            } else {
+                PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, s, s, (int)D, &one, W, s, W, s, &zero, dG, s));
+            }
             std::vector<double> hG((size_t)s * s), Rp;
             PF_CUDA(cudaMemcpyAsync(pinG, dG, ss * sizeof(double), cudaMemcpyDeviceToHost, st));
             sync(h);
@@ -667,8 +690,9 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
             if (!host_cholesky(hG, s, Rp)) { ok = false; break; }
             std::memcpy(pinR, Rp.data(), ss * sizeof(double));
             PF_CUDA(cudaMemcpyAsync(dR, pinR, ss * sizeof(double), cudaMemcpyHostToDevice, st));
-            PF_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, s,
-                                  (int)D, &one, dR, s, W, s));
+            if (!fused)
+                PF_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                                      s, (int)D, &one, dR, s, W, s));
             // Rtot <- Rp * Rtot
             std::vector<double> Rn((size_t)s * s, 0.0);
             for (int j = 0; j < s; ++j)
@@ -680,6 +704,18 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
             Rtot.swap(Rn);
             sync(h);   // pinR is rewritten by the next pass
         }
+        bool appended = false;
+        if (ok && fused) {
+            // W <- W R2^{-1}, also into the basis
+            BlkPass q = pass_args(W);
+            q.flags = BLK_SOLVE | BLK_APPEND;
+            q.Rs = dR;
+            q.basis = basis.p;
+            q.ldb = ldb;
+            q.col = kcol;
+            blk_pass(st, q);
+            appended = true;
+        }
         if (!ok) {
             std::vector<double> hW((size_t)D * s);
             PF_CUDA(cudaMemcpyAsync(hW.data(), W, hW.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -690,6 +726,7 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
         std::memcpy(pinR, Rtot.data(), ss * sizeof(double));
         PF_CUDA(cudaMemcpyAsync(dRt1, pinR, ss * sizeof(double), cudaMemcpyHostToDevice, st));
         sync(h);
+        return appended;
     };
 
     // ---- lanczositer (Factorization.jl:50-67)
@@ -704,7 +741,7 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
     }
     overlap(vlast, r, 0);
     // r^T -= alpha^T x0^T
-    PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, dA, s, vlast, s, &one, r, s));
+    update(r, vlast, nullptr);
     int numiter = 1;
 
     // eigen workspace
@@ -926,14 +963,20 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
     while (true) {
         // 1 tridiagonalization: QR(r) -> beta (BlockLanczosFactorization.jl:115-131)
         cudaEvent_t e0 = clk.mark();
-        if (host_qr) qr_host(r);
-        else qr_device(r);
-        k_put_beta<<<1, 256, 0, st>>>(dRt1, s, Tfull.p, maxdim, k, dBeta);
-        PF_CUDA(cudaGetLastError());
-        count_launches(1);
+        bool appended = false;
+        if (host_qr || !fused) {
+            if (host_qr) appended = qr_host(r, k);
+            else qr_device(r, k);
+            k_put_beta<<<1, 256, 0, st>>>(dRt1, s, Tfull.p, maxdim, k, dBeta);
+            PF_CUDA(cudaGetLastError());
+            count_launches(1);
+        } else {
+            qr_device(r, k);   // beta into T and Q into the basis in its passes
+            appended = true;
+        }
         std::swap(vprev, vlast);
         std::swap(vlast, r);  // vlast <- Q ; r <- old vprev storage
-        append(vlast, k);
+        if (!appended) append(vlast, k);
         k += s;
         cudaEvent_t e1 = clk.mark();
         clk.add(0, e0, e1);
@@ -946,8 +989,7 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
         cudaEvent_t e3 = clk.mark();
         clk.add(2, e2, e3);
         // 4 orthogonalization: r -= vlast alpha + vprev beta^T  (orthogonalization.jl:31-33)
-        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, s, (int)D, s, &mone, dA, s, vlast, s, &one, r, s));
-        PF_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, s, (int)D, s, &mone, dBeta, s, vprev, s, &one, r, s));
+        update(r, vlast, vprev);
         cudaEvent_t e4 = clk.mark();
         clk.add(3, e3, e4);
         // 5 reorthogonalization: r -= B (B^T r), B = all but the last two blocks

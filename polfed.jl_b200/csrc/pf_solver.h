@@ -61,6 +61,37 @@ void gram_bf16x3(pf_handle *h, cudaStream_t st, int64_t D, int nB, const double 
                  double *G, void *work, int *err);
 void op_gram_bf16x3(pf_handle *h, int64_t D, int nB, const double *B, int64_t ldb, const double *r, int s, double *G);
 
+// fused s-column block passes of a Lanczos iteration (pf_blocks.cu)
+constexpr int kBlkMaxS = 32;
+enum : int { BLK_SOLVE = 1, BLK_GRAM = 2, BLK_APPEND = 4 };
+enum : int { EPI_GRAM = 0, EPI_CHOL = 1, EPI_CHOL_BETA = 2, EPI_ALPHA = 3 };
+struct BlkPass {
+    int64_t D = 0;
+    int s = 0, flags = 0, epi = EPI_GRAM;
+    double *W = nullptr;               // RI block (D x s); solved in place with BLK_SOLVE
+    const double *Y = nullptr;         // Gram W^T Y (overlap); null: W^T W
+    const double *Rs = nullptr;        // BLK_SOLVE: R (upper, column-major s x s)
+    double *basis = nullptr;           // BLK_APPEND: row-major basis, row stride ldb, at column col
+    int64_t ldb = 0;
+    int col = 0;
+    double *partial = nullptr;         // blk_partial_doubles(D, s)
+    unsigned *counter = nullptr;       // zero before the first pass (each pass leaves it zero)
+    double *G = nullptr;               // BLK_GRAM: the Gram matrix (full, column-major s x s)
+    double *R = nullptr;               // EPI_CHOL*: this pass's Cholesky factor
+    const double *rtot_in = nullptr;   // EPI_CHOL*: running product so far (null: I)
+    double *rtot_out = nullptr;        // EPI_CHOL*: R * rtot_in
+    int *flag = nullptr;               // EPI_CHOL*: set on a rejected pivot (then R = I)
+    double *T = nullptr;               // EPI_CHOL_BETA / EPI_ALPHA: T (column-major, ldT)
+    int ldT = 0, k = 0;                // beta at rows k, columns k - s (and transpose); alpha at (k, k)
+    double *keep = nullptr;            // EPI_CHOL_BETA: beta; EPI_ALPHA: alpha (symmetric)
+};
+size_t blk_partial_doubles(int64_t D, int s);
+void blk_pass(cudaStream_t st, const BlkPass &p);
+void blk_update(cudaStream_t st, int64_t D, int s, double *r, const double *V, const double *Vp, const double *alpha,
+                const double *beta);
+void small_chol(cudaStream_t st, const double *G, int s, double *R, const double *rtot_in, double *rtot_out,
+                int *flag);
+
 // filter engine (pf_engine.cu): one step launch for every filter in flight
 void build_multi_tables(pf_op *op);
 bool multi_eligible(const pf_op *op, int dtype);

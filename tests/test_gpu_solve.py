@@ -66,7 +66,7 @@ def test_xxz_scalar_lanczos_matches_oracle(pkg, orc, cuda):
     assert rep.spectral.matrixvec_muls == s.order * rep.factorization.itersneeded + 10
 
 
-@pytest.mark.parametrize("s", [2, 4, 8])
+@pytest.mark.parametrize("s", [2, 3, 4, 8, 20])
 def test_qsun_block_lanczos_matches_oracle(pkg, orc, cuda, s):
     rng = np.random.default_rng(10 + s)
     f, n, c, g = pkg.qsun_parameters(7, 3, 0.75, rng=rng)
@@ -263,12 +263,14 @@ def test_cgs2_with_tensor_core_first_pass(pkg, orc, cuda):
     _check_pairs(H, v3, w3, 1e-10)
 
 
-@pytest.mark.parametrize("s", [1, 4])
+@pytest.mark.parametrize("s", [1, 3, 4, 20, 40])
 def test_device_lanczos_algebra_equals_the_host_qr(pkg, orc, cuda, s):
     """The s x s algebra of an iteration (alpha, the CholQR passes, the
     projected matrix) runs on the device; its Cholesky repeats the host
     factorisation's rounded operations in order, so a solve gives bit for bit
-    what the host QR (Gram matrices read back every iteration) gives."""
+    what the host QR (Gram matrices read back every iteration) gives.  Blocks
+    of up to 32 columns take the fused block passes in both forms (s = 20:
+    64-row tiles), wider ones the library products (s = 40)."""
     rng = np.random.default_rng(30 + s)
     f, n, c, g = pkg.qsun_parameters(8, 3, 0.75, rng=rng)
     op = pkg.QSunOperator(8, 3, 1.0, c, n, f, g)
