@@ -37,6 +37,19 @@ namespace pf {
 namespace {
 
 constexpr int kBlkThreads = 256;
+constexpr int kBlkPhases = 16;   // at most this many row phases per Gram entry in a tile
+constexpr int kBlkRuns = 32;     // at most this many strided runs per entry over the CTA partials
+
+// row phases of a tile per Gram entry, and strided runs over the CTA
+// partials per entry, for E = s (s + 1) / 2 entries
+__host__ __device__ inline int blk_phases(int E) {
+    const int p = E >= kBlkThreads ? 1 : kBlkThreads / E;
+    return p < kBlkPhases ? p : kBlkPhases;
+}
+__host__ __device__ inline int blk_runs(int E) {
+    const int q = E >= kBlkThreads ? 1 : kBlkThreads / E;
+    return q < kBlkRuns ? q : kBlkRuns;
+}
 
 __host__ __device__ inline int blk_rows(int s) { return s <= 16 ? 128 : 64; }
 __host__ __device__ inline int blk_pitch(int s) { return s | 1; }   // odd: no bank conflicts
@@ -130,7 +143,7 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_pass(const BlkPass p) {
     double *rs = yt + (two ? rows * pitch : 0);
     double *red = rs + s * s;   // kBlkThreads
     const int E = s * (s + 1) / 2;
-    const int P = E >= kBlkThreads ? 1 : kBlkThreads / E;   // row phases of a tile
+    const int P = blk_phases(E);   // row phases of a tile
     const int t = threadIdx.x;
     if (solve)
         for (int i = t; i < s * s; i += kBlkThreads) rs[i] = p.Rs[i];
@@ -230,15 +243,24 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_pass(const BlkPass p) {
     // the total: CTA partials of each entry in CTA order, split over Q
     // strided runs that are then added in run order
     const int nb = gridDim.x;
-    const int Q = E >= kBlkThreads ? 1 : (kBlkThreads / E < 8 ? kBlkThreads / E : 8);
+    const int Q = blk_runs(E);
     double *g = smem;                 // s x s, reusing the tiles
     double *r = g + s * s;            // s x s
     double *rt = r + s * s;           // s x s
     double *runs = rt + s * s;        // Q x E
     for (int w = t; w < Q * E; w += kBlkThreads) {
         const int e = w % E, q = w / E;
+        // eight loads in flight, added in CTA order
         double v = 0.0;
-        for (int b = q; b < nb; b += Q) v = __dadd_rn(v, __ldcg(p.partial + (size_t)b * E + e));
+        int b = q;
+        for (; b + 7 * Q < nb; b += 8 * Q) {
+            double x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) x[u] = __ldcg(p.partial + (size_t)(b + u * Q) * E + e);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v = __dadd_rn(v, x[u]);
+        }
+        for (; b < nb; b += Q) v = __dadd_rn(v, __ldcg(p.partial + (size_t)b * E + e));
         runs[q * E + e] = v;
     }
     __syncthreads();
@@ -317,7 +339,7 @@ size_t blk_partial_doubles(int64_t D, int s) { return (size_t)blk_grid(D, s) * (
 
 static size_t blk_smem(int s, bool two) {
     const int rows = blk_rows(s), pitch = blk_pitch(s), E = s * (s + 1) / 2;
-    const int Q = E >= kBlkThreads ? 1 : std::min(kBlkThreads / E, 8);
+    const int Q = blk_runs(E);
     const size_t pass = (size_t)rows * pitch * (two ? 2 : 1) + (size_t)s * s + kBlkThreads;
     const size_t epi = 3 * (size_t)s * s + (size_t)Q * E;
     return std::max(pass, epi) * sizeof(double);
