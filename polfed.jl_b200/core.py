@@ -329,7 +329,7 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
         s = 1 if x.ndim == 1 else x.shape[1]
         keep_x = np.asfortranarray(x.reshape(D, s))
         x_ptr, x_mem = keep_x.ctypes.data, _lib.PF_MEM_HOST
-        V = np.zeros((D, howmany), order="F") if vecs else None
+        V = _host_out(D, howmany) if vecs else None
         v_ptr, v_mem = (V.ctypes.data if vecs else None), _lib.PF_MEM_HOST
     p, keep, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
     vals = np.zeros(howmany)
@@ -341,7 +341,7 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
     k = n.value
     out_vals = vals[:k].copy()
     if vecs:
-        out_vecs = V[:, :k] if on_device else V[:, :k].copy()
+        out_vecs = V[:, :k]   # the first k columns: contiguous, no second pass over D x k
     else:
         out_vecs = None
     if produce_report:
@@ -374,7 +374,7 @@ def _polfed_hermitian(op, x0, howmany, target, produce_report, mapping, transfor
         s = 1 if x.ndim == 1 else x.shape[1]
         keep_x = np.asfortranarray(x.reshape(D, s))
         x_ptr, x_mem = keep_x.ctypes.data, _lib.PF_MEM_HOST
-        V = np.zeros((D, howmany), dtype=np.complex128, order="F") if vecs else None
+        V = _host_out(D, howmany, np.complex128) if vecs else None
         v_ptr, v_mem = (V.ctypes.data if vecs else None), _lib.PF_MEM_HOST
     if dos.probes is not None:
         pr = np.asarray(dos.probes)
@@ -390,7 +390,7 @@ def _polfed_hermitian(op, x0, howmany, target, produce_report, mapping, transfor
                                               v_ptr, v_mem, ctypes.byref(rep), ctypes.byref(n)))
     del keep, keep_x
     k = n.value
-    out_vecs = (V[:, :k] if on_device else V[:, :k].copy()) if vecs else None
+    out_vecs = V[:, :k] if vecs else None
     if produce_report:
         return vals[:k].copy(), out_vecs, _make_report(rep, kind, val)
     return vals[:k].copy(), out_vecs
@@ -405,6 +405,22 @@ def worker_handles(n: int, device: int = 0):
     while len(hs) < n:
         hs.append(_lib.new_handle(device))
     return hs[:n]
+
+
+def _host_out(D: int, m: int, dtype=np.float64):
+    """A column-major D x m host array for eigenvectors, in page-locked
+    memory from torch's caching host allocator when CUDA is available, so the
+    device-to-host copy of the results runs at the link's speed and the
+    buffers of earlier results are reused; plain memory otherwise.  Only the
+    returned columns are written."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.complex128
+            return torch.empty((m, D), dtype=tdt, pin_memory=True).numpy().T
+    except (ImportError, RuntimeError):
+        pass
+    return np.zeros((D, m), dtype=dtype, order="F")
 
 
 def _host_x0(op: Operator, x0):
@@ -603,7 +619,7 @@ class SolverPool:
             else:
                 x, s = _host_x0(op, x0)
                 xptr.append(x.ctypes.data)
-                V = np.zeros((op.dim, howmany), order="F") if want_vecs else None
+                V = _host_out(op.dim, howmany) if want_vecs else None
             p, kp, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
             keep += [x, kp]
             params.append(p)
@@ -644,7 +660,7 @@ class SolverPool:
             raise ValueError("served requests draw their KPM probes from dos.seed")
         x, s = _host_x0(op, x0)
         p, _, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
-        V = np.zeros((op.dim, howmany), order="F") if want_vecs else None
+        V = _host_out(op.dim, howmany) if want_vecs else None
         rid = ctypes.c_int64()
         _lib.check(self._native("submit", op.op, ctypes.byref(p), s, int(howmany), x.ctypes.data,
                                 V.ctypes.data if want_vecs else None, _lib.PF_MEM_HOST, ctypes.byref(rid)))
@@ -691,7 +707,7 @@ class SolverPool:
             raise _lib.PolfedRejected(st, _lib.load().pf_last_error().decode(errors="replace"))
         _lib.check(st)
         k = n.value
-        res = (vals[:k].copy(), V[:, :k].copy() if V is not None else None)
+        res = (vals[:k].copy(), V[:, :k] if V is not None else None)
         if want_rep:
             res = res + (_make_report(rep, kind, val),)
         return res
