@@ -330,6 +330,48 @@ __global__ void __launch_bounds__(kBlkThreads)
     }
 }
 
+// The same update with one row per thread for s in {1, 2, 4, 8, 16} (the
+// row's values in registers, read once), with the element form's operations
+// in its order, so both give the same bits.
+template <int S>
+__global__ void __launch_bounds__(kBlkThreads)
+    k_blk_update_rows(int64_t D, double *__restrict__ r, const double *__restrict__ V,
+                      const double *__restrict__ Vp, const double *__restrict__ alpha,
+                      const double *__restrict__ beta) {
+    __shared__ double ab[2 * S * S];
+    for (int i = threadIdx.x; i < S * S; i += blockDim.x) {
+        ab[i] = alpha[i];
+        if (Vp) ab[S * S + i] = beta[i];
+    }
+    __syncthreads();
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < D;
+         row += (int64_t)gridDim.x * blockDim.x) {
+        double v[S], w[S], x[S];
+#pragma unroll
+        for (int c = 0; c < S; ++c) v[c] = __ldg(V + row * S + c);
+        if (Vp) {
+#pragma unroll
+            for (int c = 0; c < S; ++c) w[c] = __ldg(Vp + row * S + c);
+        }
+#pragma unroll
+        for (int c = 0; c < S; ++c) x[c] = r[row * S + c];
+#pragma unroll
+        for (int c = 0; c < S; ++c) {
+            double a = 0.0;
+#pragma unroll
+            for (int i = 0; i < S; ++i) a = __fma_rn(ab[i + c * S], v[i], a);
+            double val = __dsub_rn(x[c], a);
+            if (Vp) {
+                double bb = 0.0;
+#pragma unroll
+                for (int i = 0; i < S; ++i) bb = __fma_rn(ab[S * S + c + i * S], w[i], bb);
+                val = __dsub_rn(val, bb);
+            }
+            r[row * S + c] = val;
+        }
+    }
+}
+
 int blk_grid(int64_t D, int s) {
     const int64_t tiles = (D + blk_rows(s) - 1) / blk_rows(s);
     return (int)std::min<int64_t>(tiles, 592);
@@ -356,9 +398,19 @@ void blk_pass(cudaStream_t st, const BlkPass &p) {
 
 void blk_update(cudaStream_t st, int64_t D, int s, double *r, const double *V, const double *Vp, const double *alpha,
                 const double *beta) {
-    const int64_t n = D * s;
-    const int grid = (int)std::min<int64_t>((n + kBlkThreads - 1) / kBlkThreads, 148 * 8);
-    k_blk_update<<<grid, kBlkThreads, 2 * (size_t)s * s * sizeof(double), st>>>(D, s, r, V, Vp, alpha, beta);
+    const int rgrid = (int)std::min<int64_t>((D + kBlkThreads - 1) / kBlkThreads, 148 * 8);
+    switch (s) {
+        case 1: k_blk_update_rows<1><<<rgrid, kBlkThreads, 0, st>>>(D, r, V, Vp, alpha, beta); break;
+        case 2: k_blk_update_rows<2><<<rgrid, kBlkThreads, 0, st>>>(D, r, V, Vp, alpha, beta); break;
+        case 4: k_blk_update_rows<4><<<rgrid, kBlkThreads, 0, st>>>(D, r, V, Vp, alpha, beta); break;
+        case 8: k_blk_update_rows<8><<<rgrid, kBlkThreads, 0, st>>>(D, r, V, Vp, alpha, beta); break;
+        case 16: k_blk_update_rows<16><<<rgrid, kBlkThreads, 0, st>>>(D, r, V, Vp, alpha, beta); break;
+        default: {
+            const int64_t n = D * s;
+            const int grid = (int)std::min<int64_t>((n + kBlkThreads - 1) / kBlkThreads, 148 * 8);
+            k_blk_update<<<grid, kBlkThreads, 2 * (size_t)s * s * sizeof(double), st>>>(D, s, r, V, Vp, alpha, beta);
+        }
+    }
     PF_CUDA(cudaGetLastError());
     count_launches(1);
 }
