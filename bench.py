@@ -8,9 +8,11 @@ alpha^{u_j} with alpha=0.75, u_j = (j-1) + U[-0.2, 0.2], fields U[0.5, 1.5],
 g0=1; block Lanczos with block size s=8, nev=200 at rescaled energy 0.5,
 FP64 throughout; KPM DoS with the reference defaults (N=250, R=300, Jackson).
 
-One step = one complete POLFED solve of a fresh disorder realisation
-(Emin/Emax Lanczos probes, KPM, interval and order, Chebyshev-filtered block
-Lanczos, Ritz extraction, FP64 Rayleigh quotients and residuals).  An
+One step = a batch of complete POLFED solves of fresh disorder realisations
+(16 by default, ``--batch``) in flight together on a request pool's worker
+streams; each solve runs the Emin/Emax Lanczos probes, KPM, interval and
+order, the Chebyshev-filtered block Lanczos, Ritz extraction, FP64 Rayleigh
+quotients and residuals.  An
 eigenpair counts iff its FP64 residual ||H psi - E psi|| <= 1e-10 (eigentol).
 
 * ``value``  -- whole-job eigenpairs/s with x0 and the outputs resident in HBM;
@@ -404,7 +406,8 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(WORKLOAD, **{"l2": "256 MB buffer written between steps (inside the timed region)",
                                     "step": f"a batch of {B} full POLFED solves in flight together, "
                                             f"one per worker stream",
-                                    "batch": B, "parallelism": f"replicas x{world}", "step_width": width}),
+                                    "batch": B, "parallelism": f"replicas x{world}", "step_width": width,
+                                    "step_profile": pkg.step_profile(ops[0], WORKLOAD["blocksize"])}),
         "e2e": {"value": e_value, "unit": "eigenpairs/s", "h2d_bytes_per_step": B * D * s * 8,
                 "d2h_bytes_per_step": int(statistics.mean(e_nconv) * B * (D * 8 + 8)), "wall_seconds": e_wall},
         "single_solve": {"value": single_value, "unit": "eigenpairs/s",
@@ -780,7 +783,8 @@ def profile_step(width=None, profile=0):
         pkg.chebyshev_filter(op, Y, X, c, a=8.0, b=0.0)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
-    print(json.dumps({"profile_step": True, "D": D, "s": s, "width": width, "norm": float(Y.norm())}))
+    print(json.dumps({"profile_step": True, "D": D, "s": s, "width": width,
+                      "profile": pkg.step_profile(op, s), "norm": float(Y.norm())}))
     return 0
 
 
@@ -938,9 +942,11 @@ def step_sweep(large_only=False):
     return 0
 
 
-def profile_step_large(dtype="fp64"):
+def profile_step_large(dtype="fp64", width=None, profile=0):
     """Two order-2 Chebyshev filters on the J1-J2 L=24 Sz=0 operator
-    (D = 2,704,156, s = 16): a bounded large-D case for ncu captures."""
+    (D = 2,704,156, s = 16) with the autotuned step or the given width and
+    profile, inside an NVTX range "filters": a bounded large-D case for ncu
+    captures."""
     import numpy as np
     import torch
     import __graft_entry__ as ge
@@ -948,15 +954,22 @@ def profile_step_large(dtype="fp64"):
     name, make, s = STEP_CASES[-1]
     op = make(pkg, np.random.default_rng(3))
     tdt = torch.float64 if dtype == "fp64" else torch.float32
-    width, _ = pkg.autotune(op, s, dtype)
+    if width is None:
+        width, _ = pkg.autotune(op, s, dtype)
+    else:
+        pkg.set_step_width(op, s, width, dtype, profile)
     X = pkg.col_major(op.dim, s, dtype=tdt)
     X.copy_(torch.rand(op.dim, s, dtype=tdt, device="cuda:0"))
     Y = pkg.col_major(op.dim, s, dtype=tdt)
     c = np.array([0.1, 0.2, 0.3])
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("filters")
     for _ in range(2):
         pkg.chebyshev_filter(op, Y, X, c, a=2.0 * s, b=0.0)
     torch.cuda.synchronize()
-    print(json.dumps({"profile_step_large": True, "D": op.dim, "s": s, "dtype": dtype, "width": width}))
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_step_large": True, "D": op.dim, "s": s, "dtype": dtype, "width": width,
+                      "profile": pkg.step_profile(op, s, dtype)}))
     return 0
 
 
@@ -983,7 +996,8 @@ def main():
     ap.add_argument("--profile-step", action="store_true",
                     help="only run two short Chebyshev filters on one realisation (a bounded case for ncu)")
     ap.add_argument("--step-width", type=int, default=None,
-                    help="with --profile-step: this step width (columns per thread) instead of the autotuner's")
+                    help="with --profile-step / --profile-step-large: this step width (columns per thread) "
+                         "instead of the autotuner's")
     ap.add_argument("--step-profile", type=int, default=0, help="with --step-width: the step profile")
     ap.add_argument("--apply-sweep", action="store_true",
                     help="single-vector XXZ H-apply at L=18..24 (the reference's published timings)")
@@ -1013,7 +1027,7 @@ def main():
     if args.step_sweep:
         return step_sweep(args.large_only)
     if args.profile_step_large:
-        return profile_step_large(args.profile_step_large)
+        return profile_step_large(args.profile_step_large, args.step_width, args.step_profile)
     if args.c3:
         return run_c3(args, local_rank)
     if args.serve:

@@ -241,6 +241,10 @@ int pf_gather_peak(pf_handle *h, int log2_rows, double *bytes_per_s);
  * warp-cooperative step), gathers issued per batch and the resident CTAs per
  * SM it is compiled for (its register cap). */
 int pf_step_variant(pf_op *op, int dtype, int s, int *width, int *gather_batch, int *ctas_per_sm);
+/* The profile (0..9, as for pf_set_step_variant) of the variant in use for
+ * (dtype, s), so that a variant the autotuner chose can be pinned again with
+ * pf_set_step_variant (for instance in another process). */
+int pf_step_profile(pf_op *op, int dtype, int s, int *profile);
 /* Pin the step-kernel variant for (dtype, s) without timing (a width the
  * autotuner could have chosen); later launches on this operator use it. */
 int pf_set_step_width(pf_op *op, int dtype, int s, int width);

@@ -38,7 +38,7 @@ EXPORTED = [
     "pf_pool_create", "pf_pool_destroy", "pf_solve_footprint", "pf_pool_solve_batch", "pf_pool_submit",
     "pf_pool_poll", "pf_pool_fetch", "pf_pool_cancel", "pf_pool_get_stats", "pf_pool_stream",
     "pf_pool_set_priority_dim", "pf_pool_set_admission", "pf_pool_request_times",
-    "pf_pool_wait", "pf_pool_shutdown", "pf_pool_set_batching", "pf_step_variant", "pf_set_step_variant",
+    "pf_pool_wait", "pf_pool_shutdown", "pf_pool_set_batching", "pf_step_variant", "pf_step_profile", "pf_set_step_variant",
     "pf_gather_peak", "pf_set_filter_slab", "pf_gram_bf16x3",
 ]
 PF_REQ_QUEUED, PF_REQ_RUNNING, PF_REQ_DONE, PF_REQ_FAILED, PF_REQ_REJECTED = 0, 1, 2, 3, 4
@@ -162,6 +162,7 @@ def load():
         "pf_set_filter_slab": (i32, [vp, i32]),
         "pf_gram_bf16x3": (i32, [vp, i64, i32, vp, i64, vp, i32, vp]),
         "pf_step_variant": (i32, [vp, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)]),
+        "pf_step_profile": (i32, [vp, i32, i32, ctypes.POINTER(i32)]),
         "pf_pool_create": (i32, [i32, i32, f64, ctypes.POINTER(vp)]),
         "pf_pool_destroy": (i32, [vp]),
         "pf_pool_stream": (i32, [vp, i32, ctypes.POINTER(vp)]),

@@ -915,6 +915,15 @@ def step_variant(op: Operator, s: int, dtype: str = "fp64"):
     return w.value, u.value, mb.value
 
 
+def step_profile(op: Operator, s: int, dtype: str = "fp64") -> int:
+    """The profile (0..9, as for ``set_step_width``) of the step-kernel
+    variant in use for block width ``s``."""
+    pr = ctypes.c_int()
+    dt = _lib.PF_F64 if dtype == "fp64" else _lib.PF_F32
+    _lib.check(_lib.load().pf_step_profile(op.op, dt, int(s), ctypes.byref(pr)))
+    return pr.value
+
+
 def set_step_width(op: Operator, s: int, width: int, dtype: str = "fp64", profile: int = 0):
     """Pin the step-kernel variant for block width ``s`` (see ``autotune``):
     ``width`` columns per thread (0: the warp-cooperative chain step) and a

@@ -315,6 +315,22 @@ int pf_step_variant(pf_op *op, int dtype, int s, int *width, int *gather_batch, 
     PF_API_END
 }
 
+int pf_step_profile(pf_op *op, int dtype, int s, int *profile) {
+    PF_API_BEGIN
+    PF_CHECK(op && profile, PF_ERR_INVALID, "null argument");
+    PF_CHECK(dtype == PF_F64 || dtype == PF_F32, PF_ERR_INVALID, "dtype must be PF_F64 or PF_F32");
+    PF_CHECK(s >= 1, PF_ERR_INVALID, "s must be positive");
+    const int elem = dtype == PF_F64 ? 8 : 4;
+    int code = pf::default_width(s, elem);
+    {
+        std::lock_guard<std::mutex> lock(op->tune_mu);
+        auto it = op->tuned_width.find(std::make_pair(elem, s));
+        if (it != op->tuned_width.end()) code = it->second;
+    }
+    *profile = code == PF_WIDTH_COOP ? 0 : pf::variant_profile(code);
+    PF_API_END
+}
+
 int pf_set_step_variant(pf_op *op, int dtype, int s, int width, int profile) {
     PF_API_BEGIN
     PF_CHECK(op, PF_ERR_INVALID, "null operator");
