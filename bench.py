@@ -935,6 +935,7 @@ def step_sweep(large_only=False):
             per = (t_filter(40) - t_filter(20)) / 20
             alg = 4.0 * D * s * w
             print(json.dumps({"case": name, "D": D, "s": s, "dtype": dt, "width": width,
+                              "profile": pkg.step_profile(op, s, dt),
                               "tune_us": {str(k): round(v * 1e3, 2) for k, v in tune.items()},
                               "us_per_step": per * 1e6, "alg_bytes": alg, "achieved_gbs": alg / per / 1e9,
                               "frac": alg / per / 1e9 / peak, "peak": peak, "peak_kind": peak_kind}), flush=True)
