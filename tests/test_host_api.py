@@ -182,3 +182,14 @@ def test_qsun_spin_grain_normalisation(pkg, orc, S, L_loc, L_grain, S_z):
     K = np.kron(np.eye(d ** L_loc), g)[np.ix_(sector, sector)]
     np.testing.assert_allclose(R, K, rtol=1e-13, atol=1e-15)
     assert pkg.spin_sector_count(L_loc + L_grain, d, int(round(S_z + (L_loc + L_grain) * S))) == R.shape[0]
+
+
+def test_host_result_buffers_are_column_major(pkg):
+    """Eigenvector buffers for host results: column-major D x m, real or
+    complex (page-locked through torch's caching host allocator when CUDA is
+    present, plain memory otherwise); a leading-column view stays contiguous."""
+    from polfed_b200 import core
+    for dt in (np.float64, np.complex128):
+        V = core._host_out(37, 5, dt)
+        assert V.shape == (37, 5) and V.dtype == dt and V.flags["F_CONTIGUOUS"]
+        assert V[:, :3].flags["F_CONTIGUOUS"]
