@@ -92,14 +92,19 @@ struct StageClock {
     ~StageClock() {
         for (auto e : all) cudaEventDestroy(e);
     }
+    // with no accumulator (an untimed run, e.g. the extremal probes) no
+    // events are made at all
     cudaEvent_t mark() {
+        if (!acc) return nullptr;
         cudaEvent_t e;
         PF_CUDA(cudaEventCreate(&e));
         all.push_back(e);
         PF_CUDA(cudaEventRecord(e, st));
         return e;
     }
-    void add(int stage, cudaEvent_t a, cudaEvent_t b) { pending.push_back({stage, a, b}); }
+    void add(int stage, cudaEvent_t a, cudaEvent_t b) {
+        if (acc && a && b) pending.push_back({stage, a, b});
+    }
     void flush() {
         for (auto &p : pending) {
             float ms = 0.f;
@@ -1222,7 +1227,7 @@ static pf_handle *aux_handle(pf_handle *h) {
 }
 
 static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, double tol, double eigentol, double *Emin,
-                                double *Emax, double *stage_acc, int *qr_restarts = nullptr, bool host_qr = false) {
+                                double *Emax, int *qr_restarts = nullptr, bool host_qr = false) {
     const int64_t D = op->dim;
     // The :SR probe runs here and the :LR probe at the same time on the
     // auxiliary handle (its own stream, cuBLAS and cuSOLVER): both only read
@@ -1238,9 +1243,8 @@ static void extrema_from_device(pf_op *op, const double *v0_dev, int maxdim, dou
             launch_step<double>(o, o->h->stream, D, 1, X, nullptr, nullptr, Y, 0, 1.0, 0, 1.0, 0.0, StepFlags::Q,
                                 nullptr);
         };
-        double dummy[10] = {0};
         LanczosOut lo;
-        lanczos(o, 1, 1, maxdim, tol, eigentol, which, 1, v0_dev, happly, lo, stage_acc ? dummy : nullptr, -1, host_qr);
+        lanczos(o, 1, 1, maxdim, tol, eigentol, which, 1, v0_dev, happly, lo, nullptr, -1, host_qr);
         PF_CHECK(lo.nconv >= 1, PF_ERR_NUMERIC, "Failed to estimate extremal eigenvalue with Lanczos.");
         *out = which == PF_WHICH_SR ? lo.vals.front() : lo.vals.back();
         return lo.qr_restarts;
@@ -1291,7 +1295,7 @@ void lanczos_extrema(pf_op *op, const double *x0_host, int maxdim, double tol, d
     AllocStream alloc_guard(op->h->stream);
     DevArray<double> v0(D);
     PF_CUDA(cudaMemcpyAsync(v0.p, seed.data(), D * sizeof(double), cudaMemcpyHostToDevice, op->h->stream));
-    extrema_from_device(op, v0.p, maxdim, tol, eigentol, Emin, Emax, nullptr);
+    extrema_from_device(op, v0.p, maxdim, tol, eigentol, Emin, Emax);
 }
 
 // ------------------------------------------- op-level tensor-core Gram product
@@ -1451,7 +1455,7 @@ void solve(pf_op *op, const pf_params *P, int s, int nev, const double *x0, int 
             double lo = 0, hi = 0;
             // v0 = x0[:, 1] (column 0 of the column-major copy)
             extrema_from_device(op, xcm.p, P->extrema_maxdim > 0 ? P->extrema_maxdim : 1000, 1e-14, 1e-8, &lo, &hi,
-                                nullptr, &R.qr_restarts, P->host_qr != 0);
+                                &R.qr_restarts, P->host_qr != 0);
             if (!P->has_Emin) Emin = lo;
             if (!P->has_Emax) Emax = hi;
         }
