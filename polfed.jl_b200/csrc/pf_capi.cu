@@ -115,6 +115,7 @@ int pf_handle_destroy(pf_handle *h) {
     if (h->red_partials) cudaFree(h->red_partials);
     if (h->red_counter) cudaFree(h->red_counter);
     if (h->pinned) cudaFreeHost(h->pinned);
+    for (cudaEvent_t e : h->timing_events) cudaEventDestroy(e);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     PF_API_END

@@ -143,6 +143,9 @@ struct pf_handle {
     // concurrent solves); grown on demand
     void *pinned = nullptr;
     size_t pinned_bytes = 0;
+    // timing events of the solver's stage clocks, kept for reuse (creating
+    // events every iteration costs host time that stalls the stream)
+    std::vector<cudaEvent_t> timing_events;
     // step kernels launch with programmatic dependent launch (each one's
     // launch and shared-memory set-up overlap its predecessor's tail)
     bool overlap = true;

@@ -83,21 +83,29 @@ struct DevArray {
 // Events are never reused inside one solve, so a pending pair stays valid
 // until flush() reads it after the stream has passed both events.
 struct StageClock {
+    pf_handle *h;
     cudaStream_t st;
     std::vector<cudaEvent_t> all;
     struct Pending { int stage; cudaEvent_t a, b; };
     std::vector<Pending> pending;
     double *acc;
-    StageClock(cudaStream_t s, double *acc_) : st(s), acc(acc_) {}
+    StageClock(pf_handle *h_, cudaStream_t s, double *acc_) : h(h_), st(s), acc(acc_) {}
+    // the events go back to the handle for the next solve (a later record
+    // supersedes any still pending)
     ~StageClock() {
-        for (auto e : all) cudaEventDestroy(e);
+        for (auto e : all) h->timing_events.push_back(e);
     }
     // with no accumulator (an untimed run, e.g. the extremal probes) no
-    // events are made at all
+    // events are recorded at all
     cudaEvent_t mark() {
         if (!acc) return nullptr;
         cudaEvent_t e;
-        PF_CUDA(cudaEventCreate(&e));
+        if (!h->timing_events.empty()) {
+            e = h->timing_events.back();
+            h->timing_events.pop_back();
+        } else {
+            PF_CUDA(cudaEventCreate(&e));
+        }
         all.push_back(e);
         PF_CUDA(cudaEventRecord(e, st));
         return e;
@@ -577,7 +585,7 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
     std::vector<double> hR;
     const double one = 1.0, zero = 0.0, mone = -1.0;
     const int ldb = maxdim;  // row stride of the basis
-    StageClock clk(st, stage_acc);
+    StageClock clk(h, st, stage_acc);
     // page-locked staging for the checks (rewritten only after the sync that
     // follows the copies which last used it)
     double *pin = pinned_scratch(h, 3 * ss + (size_t)maxdim * (s + 3) + 8);
