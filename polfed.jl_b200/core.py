@@ -329,7 +329,7 @@ def polfed(op: Operator, x0, howmany: int, target, *, produce_report: bool = Fal
         s = 1 if x.ndim == 1 else x.shape[1]
         keep_x = np.asfortranarray(x.reshape(D, s))
         x_ptr, x_mem = keep_x.ctypes.data, _lib.PF_MEM_HOST
-        V = _host_out(D, howmany) if vecs else None
+        V = _host_out(D, howmany, device=op.device) if vecs else None
         v_ptr, v_mem = (V.ctypes.data if vecs else None), _lib.PF_MEM_HOST
     p, keep, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
     vals = np.zeros(howmany)
@@ -374,7 +374,7 @@ def _polfed_hermitian(op, x0, howmany, target, produce_report, mapping, transfor
         s = 1 if x.ndim == 1 else x.shape[1]
         keep_x = np.asfortranarray(x.reshape(D, s))
         x_ptr, x_mem = keep_x.ctypes.data, _lib.PF_MEM_HOST
-        V = _host_out(D, howmany, np.complex128) if vecs else None
+        V = _host_out(D, howmany, np.complex128, device=op.device) if vecs else None
         v_ptr, v_mem = (V.ctypes.data if vecs else None), _lib.PF_MEM_HOST
     if dos.probes is not None:
         pr = np.asarray(dos.probes)
@@ -407,17 +407,19 @@ def worker_handles(n: int, device: int = 0):
     return hs[:n]
 
 
-def _host_out(D: int, m: int, dtype=np.float64):
+def _host_out(D: int, m: int, dtype=np.float64, device: int = 0):
     """A column-major D x m host array for eigenvectors, in page-locked
-    memory from torch's caching host allocator when CUDA is available, so the
-    device-to-host copy of the results runs at the link's speed and the
-    buffers of earlier results are reused; plain memory otherwise.  Only the
-    returned columns are written."""
+    memory from torch's caching host allocator when CUDA is available (made
+    with the operator's device current, so no other device gets a context),
+    so the device-to-host copy of the results runs at the link's speed and
+    the buffers of earlier results are reused; plain memory otherwise.  Only
+    the returned columns are written."""
     try:
         import torch
         if torch.cuda.is_available():
             tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.complex128
-            return torch.empty((m, D), dtype=tdt, pin_memory=True).numpy().T
+            with torch.cuda.device(device):
+                return torch.empty((m, D), dtype=tdt, pin_memory=True).numpy().T
     except (ImportError, RuntimeError):
         pass
     return np.zeros((D, m), dtype=dtype, order="F")
@@ -619,7 +621,7 @@ class SolverPool:
             else:
                 x, s = _host_x0(op, x0)
                 xptr.append(x.ctypes.data)
-                V = _host_out(op.dim, howmany) if want_vecs else None
+                V = _host_out(op.dim, howmany, device=op.device) if want_vecs else None
             p, kp, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
             keep += [x, kp]
             params.append(p)
@@ -660,7 +662,7 @@ class SolverPool:
             raise ValueError("served requests draw their KPM probes from dos.seed")
         x, s = _host_x0(op, x0)
         p, _, kind, val = _params(op, howmany, target, mapping, transform, fact, dos, precision)
-        V = _host_out(op.dim, howmany) if want_vecs else None
+        V = _host_out(op.dim, howmany, device=op.device) if want_vecs else None
         rid = ctypes.c_int64()
         _lib.check(self._native("submit", op.op, ctypes.byref(p), s, int(howmany), x.ctypes.data,
                                 V.ctypes.data if want_vecs else None, _lib.PF_MEM_HOST, ctypes.byref(rid)))
