@@ -625,17 +625,7 @@ def run_disorder(args, local_rank):
     # block-size tuner (outside the timed region): converged pairs per second of one solve
     best_s, tune = {}, {}
     for L, i in ((16, 0), (18, 256)):
-        op = probs[i][0]
-        rates = {}
-        for s in (4, 8, 16):
-            x0 = np.random.default_rng(7).random((op.dim, s))
-            pkg.polfed(op, x0, nev, ("rescaled", 0.5), **kw(1))   # warm-up and step-width tuning
-            torch.cuda.synchronize()
-            t = time.perf_counter()
-            vals, _ = pkg.polfed(op, x0, nev, ("rescaled", 0.5), **kw(1))
-            torch.cuda.synchronize()
-            rates[s] = len(vals) / (time.perf_counter() - t)
-        best_s[L] = max(rates, key=rates.get)
+        best_s[L], rates = pkg.tune_block_size(probs[i][0], nev, ("rescaled", 0.5), (4, 8, 16), **kw(1))
         tune[f"L{L}"] = {str(k): round(v, 2) for k, v in rates.items()}
     x0s = []
     for op, eps, rng in probs:

@@ -8,7 +8,7 @@ This directory is loaded as the Python package ``polfed_b200`` (its folder
 name carries a dot, so it is imported by path; see ``load_package``).
 """
 from . import _lib
-from .core import (autotune, set_step_width, step_variant, step_profile, set_filter_slab, set_launch_overlap, BenchmarkReport, DoSConfig, FactorizationConfig, FactorizationReport, MappingConfig,
+from .core import (autotune, set_step_width, step_variant, step_profile, tune_block_size, set_filter_slab, set_launch_overlap, BenchmarkReport, DoSConfig, FactorizationConfig, FactorizationReport, MappingConfig,
                    Report, SpectralTransformReport, TransformConfig, apply, basis_index, basis_states,
                    chebyshev_filter, clenshaw_finalsum, clenshaw_recurrence, col_major, display_report,
                    expectedkrylovdim, kpm_moments, lanczos_extrema, normalize_target_spec, polfed,
@@ -24,7 +24,7 @@ __all__ = [
     "spin_sector_count", "QSunSpinOperator", "chain_bonds",
     "goe_matrix", "SpinChainOperator", "QSunOperator", "SparseOperator", "as_operator", "apply", "clenshaw_recurrence",
     "clenshaw_finalsum", "chebyshev_filter", "kpm_moments", "basis_states", "basis_index", "col_major",
-    "normalize_target_spec", "expectedkrylovdim", "load_library", "autotune", "set_step_width", "step_variant", "step_profile", "set_filter_slab", "set_launch_overlap", "polfed_batch", "worker_handles", "SolverPool", "PoolStats", "solver_pool", "BoundOperator",
+    "normalize_target_spec", "expectedkrylovdim", "load_library", "autotune", "set_step_width", "step_variant", "step_profile", "tune_block_size", "set_filter_slab", "set_launch_overlap", "polfed_batch", "worker_handles", "SolverPool", "PoolStats", "solver_pool", "BoundOperator",
 ]
 
 

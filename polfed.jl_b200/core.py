@@ -753,6 +753,35 @@ def polfed_batch(ops, x0s, howmany: int, target, *, workers: int = 4, **kwargs):
     return solver_pool(max(1, workers), ops[0].device).solve_batch(ops, x0s, howmany, target, **kwargs)
 
 
+def tune_block_size(op: Operator, howmany: int, target, candidates=(4, 8, 16), seed: int = 7, **kwargs):
+    """The block size for solves of this operator and request: one complete
+    ``polfed`` solve at each candidate s (after an untimed one that also tunes
+    the step kernel for that s), from the same seeded random start, timed on
+    the host around a device synchronisation.  Returns ``(best_s, {s:
+    converged pairs per second})``; ``kwargs`` are ``polfed``'s (``vecs`` is
+    forced off).  Solves in flight together (a pool) share the device, so a
+    batch's best s is that of one solve only approximately."""
+    import time
+    import torch
+    op = as_operator(op)
+    kwargs = dict(kwargs, vecs=False)
+    kwargs.pop("produce_report", None)
+    rates = {}
+    for s in candidates:
+        if s < 1 or s > op.dim:
+            continue
+        x0 = np.random.default_rng(seed).random((op.dim, s))
+        polfed(op, x0, howmany, target, **kwargs)
+        torch.cuda.synchronize(op.device)
+        t = time.perf_counter()
+        vals, _ = polfed(op, x0, howmany, target, **kwargs)
+        torch.cuda.synchronize(op.device)
+        rates[s] = len(vals) / (time.perf_counter() - t)
+    if not rates:
+        raise ValueError("no candidate block size fits the operator")
+    return max(rates, key=rates.get), rates
+
+
 def _is_cuda_tensor(x) -> bool:
     try:
         import torch

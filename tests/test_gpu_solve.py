@@ -327,3 +327,24 @@ def test_block_breakdown_restarts_with_the_host_qr(pkg, orc, cuda):
     np.testing.assert_array_equal(v0, v1)
     np.testing.assert_array_equal(w0, w1)
     _check_pairs(H, v0, w0, 1e-9)
+
+
+def test_block_size_tuner(pkg, orc, cuda):
+    """tune_block_size times one complete solve per candidate block size and
+    returns the fastest; solves at every candidate return eigenvalues of H
+    (to 1e-10 against the dense spectrum)."""
+    rng = np.random.default_rng(41)
+    f, n, c, g = pkg.qsun_parameters(7, 3, 0.75, rng=rng)
+    op = pkg.QSunOperator(7, 3, 1.0, c, n, f, g)
+    kw = dict(dos=pkg.DoSConfig(N=96, R=24, seed=3), fact=pkg.FactorizationConfig(eigentol=1e-10))
+    best, rates = pkg.tune_block_size(op, 12, ("rescaled", 0.4), (2, 4), **kw)
+    assert best in (2, 4) and set(rates) == {2, 4} and all(r > 0 for r in rates.values())
+    assert rates[best] == max(rates.values())
+    H = orc.qsun_matrix(7, 3, 1.0, c, n, f, g)
+    vals = {}
+    for s in (2, 4):
+        x0 = np.random.default_rng(7).random((H.shape[0], s))
+        vals[s], _ = pkg.polfed(op, x0, 12, ("rescaled", 0.4), vecs=False, **kw)
+    for s in (2, 4):
+        assert len(vals[s]) >= 10
+        assert _vs_exact(H, vals[s]) < 1e-10
