@@ -20,10 +20,12 @@
 // Every CTA stages tiles of rows in shared memory (a tile is contiguous in
 // the RI layout, so the loads are coalesced).  A CTA's Gram partial is the
 // sum over its tiles, in order, of per-entry sums over a fixed split of the
-// tile's rows; the CTA that finishes last (a counter) adds the partials in
-// CTA order and runs the epilogue.  The grid size depends only on D and s,
-// and every product and sum is rounded on its own (fused multiply-adds where
-// written), so a pass gives the same bits in every run and in both QR paths:
+// tile's rows; the last CTA of each group of 32 to finish (a counter per
+// group) adds the group's partials in CTA order, and the last group to finish
+// adds the group sums in group order and runs the epilogue.  The grid size
+// depends only on D and s, and every product and sum is rounded on its own
+// (fused multiply-adds where written), so a pass gives the same bits in every
+// run and in both QR paths:
 // the host-QR path runs the same Gram and solve passes and only moves the
 // Cholesky to the host (host_cholesky's arithmetic, which the epilogue
 // repeats operation for operation).
@@ -39,6 +41,9 @@ namespace {
 constexpr int kBlkThreads = 256;
 constexpr int kBlkPhases = 16;   // at most this many row phases per Gram entry in a tile
 constexpr int kBlkRuns = 32;     // at most this many strided runs per entry over the CTA partials
+constexpr int kBlkGroup = 32;    // CTAs whose partials the last of them adds into a group partial
+constexpr int kBlkMaxGrid = 592;   // CTAs of a pass at most (4 per SM)
+constexpr int kBlkMaxGroups = 63;
 
 // row phases of a tile per Gram entry, and strided runs over the CTA
 // partials per entry, for E = s (s + 1) / 2 entries
@@ -64,6 +69,34 @@ __device__ inline void upper_entry(int e, int s, int *i, int *j) {
     (void)s;
     *j = jj;
     *i = e - base;
+}
+
+// out[e] = sum over rows b < n of src[b * E + e], in row order, by the calling
+// CTA: Q strided runs per entry (eight loads in flight each, added in row
+// order), then the runs added in run order.  runs: Q x E shared doubles.
+__device__ void cta_sum_rows(const double *src, int n, int E, int Q, double *runs, double *out) {
+    const int t = threadIdx.x;
+    for (int w = t; w < Q * E; w += blockDim.x) {
+        const int e = w % E, q = w / E;
+        double v = 0.0;
+        int b = q;
+        for (; b + 7 * Q < n; b += 8 * Q) {
+            double x[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) x[u] = __ldcg(src + (size_t)(b + u * Q) * E + e);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v = __dadd_rn(v, x[u]);
+        }
+        for (; b < n; b += Q) v = __dadd_rn(v, __ldcg(src + (size_t)b * E + e));
+        runs[q * E + e] = v;
+    }
+    __syncthreads();
+    for (int e = t; e < E; e += blockDim.x) {
+        double v = 0.0;
+        for (int q = 0; q < Q; ++q) v = __dadd_rn(v, runs[q * E + e]);
+        out[e] = v;
+    }
+    __syncthreads();
 }
 
 }  // namespace
@@ -232,45 +265,42 @@ __global__ void __launch_bounds__(kBlkThreads) k_blk_pass(const BlkPass p) {
     } else {
         for (int q = 0; q < ne; ++q) part[t + q * kBlkThreads] = acc[q];
     }
+    // two levels: the last CTA of each group of kBlkGroup CTAs adds the
+    // group's partials in CTA order; the last group to finish adds the group
+    // sums in group order
     __shared__ bool last;
     __shared__ int bad;
-    __threadfence();
-    __syncthreads();
-    if (t == 0) last = atomicAdd(p.counter, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    // the total: CTA partials of each entry in CTA order, split over Q
-    // strided runs that are then added in run order
     const int nb = gridDim.x;
+    const int grp = blockIdx.x / kBlkGroup, g0 = grp * kBlkGroup;
+    const int gn = nb - g0 < kBlkGroup ? nb - g0 : kBlkGroup;
+    const int ngrp = (nb + kBlkGroup - 1) / kBlkGroup;
+    double *gpart = p.partial + (size_t)nb * E;   // ngrp x E
     const int Q = blk_runs(E);
     double *g = smem;                 // s x s, reusing the tiles
     double *r = g + s * s;            // s x s
     double *rt = r + s * s;           // s x s
     double *runs = rt + s * s;        // Q x E
-    for (int w = t; w < Q * E; w += kBlkThreads) {
-        const int e = w % E, q = w / E;
-        // eight loads in flight, added in CTA order
-        double v = 0.0;
-        int b = q;
-        for (; b + 7 * Q < nb; b += 8 * Q) {
-            double x[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) x[u] = __ldcg(p.partial + (size_t)(b + u * Q) * E + e);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) v = __dadd_rn(v, x[u]);
-        }
-        for (; b < nb; b += Q) v = __dadd_rn(v, __ldcg(p.partial + (size_t)b * E + e));
-        runs[q * E + e] = v;
-    }
+    __threadfence();
     __syncthreads();
+    if (t == 0) last = atomicAdd(p.counter + 1 + grp, 1u) == (unsigned)gn - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    cta_sum_rows(p.partial + (size_t)g0 * E, gn, E, Q, runs, gpart + (size_t)grp * E);
+    if (t == 0) p.counter[1 + grp] = 0u;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(p.counter, 1u) == (unsigned)ngrp - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double *tot = runs + Q * E;       // E
+    cta_sum_rows(gpart, ngrp, E, Q, runs, tot);
     for (int e = t; e < E; e += kBlkThreads) {
-        double v = 0.0;
-        for (int q = 0; q < Q; ++q) v = __dadd_rn(v, runs[q * E + e]);
         int i, j;
         upper_entry(e, s, &i, &j);
-        g[i + j * s] = v;
-        g[j + i * s] = v;
+        g[i + j * s] = tot[e];
+        g[j + i * s] = tot[e];
     }
     __syncthreads();
     for (int i = t; i < s * s; i += kBlkThreads) p.G[i] = g[i];
@@ -374,21 +404,27 @@ __global__ void __launch_bounds__(kBlkThreads)
 
 int blk_grid(int64_t D, int s) {
     const int64_t tiles = (D + blk_rows(s) - 1) / blk_rows(s);
-    return (int)std::min<int64_t>(tiles, 592);
+    return (int)std::min<int64_t>(tiles, kBlkMaxGrid);
 }
 
-size_t blk_partial_doubles(int64_t D, int s) { return (size_t)blk_grid(D, s) * (size_t)(s * (s + 1) / 2); }
+int blk_counters() { return 1 + kBlkMaxGroups; }
+
+size_t blk_partial_doubles(int64_t D, int s) {
+    const int nb = blk_grid(D, s);
+    return (size_t)(nb + (nb + kBlkGroup - 1) / kBlkGroup) * (size_t)(s * (s + 1) / 2);
+}
 
 static size_t blk_smem(int s, bool two) {
     const int rows = blk_rows(s), pitch = blk_pitch(s), E = s * (s + 1) / 2;
     const int Q = blk_runs(E);
     const size_t pass = (size_t)rows * pitch * (two ? 2 : 1) + (size_t)s * s + kBlkThreads;
-    const size_t epi = 3 * (size_t)s * s + (size_t)Q * E;
+    const size_t epi = 3 * (size_t)s * s + (size_t)Q * E + E;
     return std::max(pass, epi) * sizeof(double);
 }
 
 void blk_pass(cudaStream_t st, const BlkPass &p) {
     PF_CHECK(p.s >= 1 && p.s <= kBlkMaxS, PF_ERR_INVALID, "fused block pass needs 1 <= s <= 32");
+    static_assert((kBlkMaxGrid + kBlkGroup - 1) / kBlkGroup <= kBlkMaxGroups, "group counters");
     const size_t smem = blk_smem(p.s, p.Y != nullptr);
     if (smem > 48 * 1024) PF_CUDA(cudaFuncSetAttribute(k_blk_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_blk_pass<<<blk_grid(p.D, p.s), kBlkThreads, smem, st>>>(p);

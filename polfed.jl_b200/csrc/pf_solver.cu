@@ -572,8 +572,8 @@ static void lanczos_pass(pf_op *op, int s, int howmany, int maxdim_req, double t
     // blocks of up to 32 columns take the fused block passes (pf_blocks.cu)
     const bool fused = s <= kBlkMaxS;
     DevArray<double> bpart(fused ? blk_partial_doubles(D, s) : 0);
-    DevArray<unsigned> bcount(fused ? 1 : 0);
-    if (fused) PF_CUDA(cudaMemsetAsync(bcount.p, 0, sizeof(unsigned), st));
+    DevArray<unsigned> bcount(fused ? blk_counters() : 0);
+    if (fused) PF_CUDA(cudaMemsetAsync(bcount.p, 0, blk_counters() * sizeof(unsigned), st));
     DevArray<int> dflag(1);
     PF_CUDA(cudaMemsetAsync(dflag.p, 0, sizeof(int), st));
     DevArray<double> Tfull((size_t)maxdim * maxdim);   // the projected matrix, column-major

@@ -75,7 +75,7 @@ struct BlkPass {
     int64_t ldb = 0;
     int col = 0;
     double *partial = nullptr;         // blk_partial_doubles(D, s)
-    unsigned *counter = nullptr;       // zero before the first pass (each pass leaves it zero)
+    unsigned *counter = nullptr;       // blk_counters() counters, zero before the first pass (each pass leaves them zero)
     double *G = nullptr;               // BLK_GRAM: the Gram matrix (full, column-major s x s)
     double *R = nullptr;               // EPI_CHOL*: this pass's Cholesky factor
     const double *rtot_in = nullptr;   // EPI_CHOL*: running product so far (null: I)
@@ -86,6 +86,7 @@ struct BlkPass {
     double *keep = nullptr;            // EPI_CHOL_BETA: beta; EPI_ALPHA: alpha (symmetric)
 };
 size_t blk_partial_doubles(int64_t D, int s);
+int blk_counters();   // the counters a pass needs (all zero before the first pass)
 void blk_pass(cudaStream_t st, const BlkPass &p);
 void blk_update(cudaStream_t st, int64_t D, int s, double *r, const double *V, const double *Vp, const double *alpha,
                 const double *beta);
